@@ -1,0 +1,237 @@
+/*
+ * symla_gpu.h -- C ABI of the B200 numeric factorize / solve path of symla.
+ *
+ * The reference library (alecjacobson/ma57, "symla") is a header-only C++
+ * template library; its numeric work happens behind two static template
+ * seams that SymLDLT<double> calls:
+ *
+ *   MultifrontalFactorizer<double>::factorize(sf, A, opts, mfOpts) -> NumericFactor
+ *       include/symla/multifrontal.hpp:299-300 (called from solver.hpp:158, :379)
+ *   MultifrontalSolver<double>::solve(nf, B, solveOpts) -> DenseMatrix
+ *       include/symla/solve.hpp:159 (called from solver.hpp:217)
+ *
+ * plus the residual of iterativeRefine (refine.hpp:97-144, called from
+ * solver.hpp:238). The entry points below replace those seams: plain pointers
+ * and sizes, int status codes, no C++ or torch types. The symbolic analysis
+ * (ordering, elimination tree, supernodes; symbolic.hpp:195-399) stays on the
+ * host; symla_analyze() is a restatement of it that produces the same
+ * structure, for callers that do not run the reference's own analysis.
+ *
+ * Conventions
+ *   - Matrices are CSC, 0-based, int32 indices (Eigen::SparseMatrix<double,
+ *     ColMajor, int> in compressed mode). Only the lower triangle (row >= col)
+ *     of the values is read (multifrontal.hpp:190-216, refine.hpp:88-92).
+ *   - Dense right-hand sides are column-major with a leading dimension.
+ *   - Every call that takes a `*_on_device` flag accepts host pointers (0) or
+ *     device pointers on the context's GPU (1).
+ *   - A context owns its device memory and one CUDA stream; it is not
+ *     thread-safe (same contract as the reference's SymLDLT).
+ *   - On error the status is returned and symla_last_error() holds a message
+ *     for the calling thread.
+ */
+#ifndef SYMLA_GPU_H_
+#define SYMLA_GPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The C++ wrapper maps them onto the reference's exceptions:
+ * NOT_ANALYZED/NOT_FACTORIZED/SINGULAR -> std::logic_error
+ * (solver.hpp:141-143, :199-206), BAD_SIZE/INVALID -> std::invalid_argument
+ * (solver.hpp:55, :207-209, :301-311), RETRY_EXHAUSTED -> std::runtime_error
+ * (solver.hpp:403-413). */
+enum {
+  SYMLA_OK = 0,
+  SYMLA_ERR_NOT_ANALYZED = 1,
+  SYMLA_ERR_NOT_FACTORIZED = 2,
+  SYMLA_ERR_SINGULAR = 3,
+  SYMLA_ERR_BAD_SIZE = 4,
+  SYMLA_ERR_RETRY_EXHAUSTED = 5,
+  SYMLA_ERR_OOM = 6,
+  SYMLA_ERR_TIMEOUT = 7,
+  SYMLA_ERR_CUDA = 8,
+  SYMLA_ERR_INVALID = 9,
+  SYMLA_ERR_NO_DEVICE = 10,
+  SYMLA_ERR_INTERNAL = 11
+};
+
+enum { SYMLA_ORDER_AMD = 0, SYMLA_ORDER_METIS = 1, SYMLA_ORDER_NATURAL = 2 };
+enum { SYMLA_MODE_THRESHOLD = 0, SYMLA_MODE_STATIC = 1 };
+/* Arithmetic of the Schur-complement (trailing) updates of large fronts.
+ * Pivot tests, D, 2x2 inversion, L, the solves and the refinement residual
+ * are FP64 in both. */
+enum { SYMLA_PREC_FP64 = 0, SYMLA_PREC_MIXED = 1 };
+
+/* Thread-local message for the most recent failing call on this thread. */
+const char* symla_last_error(void);
+
+/* ------------------------------------------------------------------ */
+/* Host symbolic analysis (replaces SymbolicFactor::analyze,           */
+/* symbolic.hpp:195-399, for callers without the reference's analysis) */
+/* ------------------------------------------------------------------ */
+typedef struct symla_symbolic symla_symbolic;
+
+typedef struct {
+  int n;
+  int num_supernodes;
+  int num_fundamental;
+  int64_t pattern_len;        /* sum of supernode rowPattern sizes */
+  int64_t fundamental_len;    /* sum of fundamental rowPattern sizes */
+  int64_t storage_nnz;        /* sum of Supernode::storageNnz() */
+} symla_symbolic_info;
+
+/* SymLDLT::analyzePattern (solver.hpp:133-137) with SymbolicFactorOptions
+ * {max_relax_size, max_relax_fill_fraction} (symbolic.hpp:161-184). */
+int symla_analyze(int n, const int* colptr, const int* rowind, int ordering, int max_relax_size,
+                  double max_relax_fill_fraction, symla_symbolic** out);
+void symla_symbolic_destroy(symla_symbolic* sym);
+int symla_symbolic_get_info(const symla_symbolic* sym, symla_symbolic_info* info);
+/* Any output pointer may be NULL. perm/etree_parent/etree_colcount: n.
+ * sn_first/sn_ncols: num_supernodes; sn_ptr: num_supernodes+1;
+ * sn_rows: pattern_len (supernode si's rowPattern is
+ * sn_rows[sn_ptr[si] .. sn_ptr[si+1])). */
+int symla_symbolic_get(const symla_symbolic* sym, int* perm, int* etree_parent, int* etree_colcount, int* sn_first,
+                       int* sn_ncols, int* sn_ptr, int* sn_rows);
+/* The fundamental (pre-amalgamation) supernodes (SymbolicFactor::
+ * fundamentalSupernodes), same layout, num_fundamental entries. */
+int symla_symbolic_get_fundamental(const symla_symbolic* sym, int* sn_first, int* sn_ncols, int* sn_ptr,
+                                   int* sn_rows);
+/* Build a symbolic handle from a caller's own analysis (for a maintainer
+ * whose SymLDLT keeps the reference's SymbolicFactor): perm, etree parent,
+ * and the final supernodes. */
+int symla_symbolic_import(int n, const int* perm, const int* etree_parent, int num_supernodes, const int* sn_first,
+                          const int* sn_ncols, const int* sn_ptr, const int* sn_rows, symla_symbolic** out);
+
+/* ------------------------------------------------------------------ */
+/* Device context                                                      */
+/* ------------------------------------------------------------------ */
+typedef struct symla_gpu_ctx symla_gpu_ctx;
+
+/* Uploads the symbolic structure and precomputes, once per pattern, the
+ * A-value -> front scatter map, child -> parent extend-add maps, the level
+ * schedule and the front arena layout. `colptr/rowind` is the pattern the
+ * values of later factorize calls will follow (refactorize reuses it). */
+int symla_gpu_create(const symla_symbolic* sym, int n, const int* colptr, const int* rowind, int device,
+                     symla_gpu_ctx** out);
+void symla_gpu_destroy(symla_gpu_ctx* ctx);
+
+typedef struct {
+  int mode;                     /* SYMLA_MODE_* */
+  int precision;                /* SYMLA_PREC_* */
+  double pivot_threshold;       /* u; accepted and ignored (dense_kernel.hpp:57-69) */
+  double zero_tolerance;        /* default 1e-300 (dense_kernel.hpp:77) */
+  double relative_pivot_floor;  /* default 1e-12 (dense_kernel.hpp:102) */
+  /* Mode::StaticRegularized, one attempt (dense_kernel.hpp:227-253) */
+  double static_delta;          /* <= 0: sqrt(eps) * front max, per front */
+  double static_rel_floor;      /* default 1e-8 */
+  double static_abs_floor;      /* default 1e-300 */
+  const int* expected_sign;     /* n entries in ORIGINAL index space, or NULL */
+  const double* front_delta;    /* optional per-supernode delta override (learned), or NULL */
+} symla_factor_opts;
+
+void symla_factor_opts_default(symla_factor_opts* o);
+
+typedef struct {
+  int n_pos, n_neg, n_zero;
+  int singular;                 /* NumericFactor::singular */
+  int n_singular;               /* size of singularCols */
+  int num_perturbed;
+  double total_perturbation;
+  int num_delayed;              /* columns that arrived as extras at some front */
+  int used_dynamic_path;        /* delays forced the re-planned (host-synchronised) path */
+  double max_growth;
+  float factor_ms;              /* device time of the factorization (CUDA events) */
+} symla_factor_info;
+
+/* MultifrontalFactorizer::factorize for one attempt (ThresholdPivot, or one
+ * StaticRegularized pass with a fixed delta). values: nnz entries in the
+ * CSC order given at create time. */
+int symla_gpu_factorize(symla_gpu_ctx* ctx, const double* values, int values_on_device, const symla_factor_opts* opts,
+                        symla_factor_info* info);
+
+/* SymLDLT::factorizeStaticRegularized's inertia-controlled retry loop
+ * (solver.hpp:328-417) driving symla_gpu_factorize. expected_sign (original
+ * index space, n entries) or kkt_n1/kkt_n2 (>= 0) describe the expectation;
+ * with neither, one pass and no check. Returns SYMLA_ERR_RETRY_EXHAUSTED
+ * when the budget runs out. */
+typedef struct {
+  double initial_delta;         /* <= 0: sqrt(eps) * max|A| */
+  int max_retries;              /* default 10 */
+  double growth;                /* default 10 */
+  double static_rel_floor;
+  double static_abs_floor;
+  const int* expected_sign;     /* original index space, or NULL */
+  int kkt_n1, kkt_n2;           /* used when expected_sign is NULL and kkt_n1 >= 0 */
+  int precision;
+  const double* front_delta;    /* optional per-supernode first-attempt deltas (learned) */
+} symla_regularize_opts;
+
+void symla_regularize_opts_default(symla_regularize_opts* o);
+
+typedef struct {
+  int retries_used;
+  double last_delta;
+  int attempts;
+  double attempt_delta[32];
+  int attempt_ok[32];
+} symla_regularize_info;
+
+int symla_gpu_factorize_regularized(symla_gpu_ctx* ctx, const double* values, int values_on_device,
+                                    const symla_regularize_opts* opts, symla_factor_info* info,
+                                    symla_regularize_info* rinfo);
+
+/* MultifrontalSolver::solve: X = A^{-1} B, B and X n x nrhs column-major.
+ * Fails with SYMLA_ERR_NOT_FACTORIZED / SYMLA_ERR_SINGULAR like
+ * SymLDLT::solve (solver.hpp:198-218). */
+int symla_gpu_solve(symla_gpu_ctx* ctx, const double* B, int ldb, int nrhs, double* X, int ldx, int on_device);
+
+typedef struct {
+  int iterations;
+  double initial_relative_residual;
+  double final_relative_residual;
+} symla_refine_info;
+
+/* solve + iterativeRefine (refine.hpp:97-144) against the values of the
+ * matrix (same pattern as at create time), FP64 residual on the device. */
+int symla_gpu_solve_refine(symla_gpu_ctx* ctx, const double* values, const double* B, int ldb, int nrhs, double* X,
+                           int ldx, int on_device, int max_iterations, double tolerance, symla_refine_info* info);
+
+/* Final-order indices of the columns that could not be pivoted anywhere
+ * (NumericFactor::singularCols, sorted). Returns the count; writes at most
+ * cap entries. */
+int symla_gpu_singular_cols(symla_gpu_ctx* ctx, int* cols, int cap);
+
+/* Per-front factor export (NumericFactor::fronts[si], multifrontal.hpp:118-135):
+ * sizes first, then contents. rowIndices: m; L: m x npiv column-major (the
+ * strictly lower part of the top npiv x npiv block and the rows below it are
+ * multipliers; the (k+1,k) slot of a 2x2 block holds d21); d_diag/d_off:
+ * npiv; piv_start/piv_kind: number of pivot blocks (returned). */
+int symla_gpu_num_fronts(symla_gpu_ctx* ctx);
+int symla_gpu_front_size(symla_gpu_ctx* ctx, int si, int* m, int* npiv);
+int symla_gpu_front_get(symla_gpu_ctx* ctx, int si, int* row_indices, double* L, double* d_diag, double* d_off,
+                        int* piv_start, int* piv_kind);
+
+/* The context's CUDA stream (cudaStream_t), for callers that time or order
+ * work around the library. */
+void* symla_gpu_stream(symla_gpu_ctx* ctx);
+
+/* Device time of the phases of the most recent factorize / solve calls
+ * (CUDA events): [0] assembly, [1] dense factorization, [2] trailing update,
+ * [3] forward+diagonal solve, [4] backward solve, [5] residual, [6] total
+ * factorize, [7] total solve. */
+int symla_gpu_phase_ms(symla_gpu_ctx* ctx, float* ms, int cap);
+
+/* Front-size statistics of the plan: [0] fronts, [1] levels, [2] max m,
+ * [3] sum m^2, [4] algorithmic factorization flops of the last factorize
+ * (lower-triangle convention), [5] nnz(L) entries, [6] arena doubles. */
+int symla_gpu_plan_stats(symla_gpu_ctx* ctx, double* out, int cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SYMLA_GPU_H_ */

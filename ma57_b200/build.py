@@ -1,0 +1,85 @@
+"""Build recipe for the native library ``ma57_b200/lib/libsymla_b200.so``.
+
+Compiles the host symbolic analysis (C++17, g++) and the sm_100a CUDA kernels
+plus the C ABI (nvcc, ``-gencode arch=compute_100a,code=sm_100a``), and links
+them with the CUDA toolkit's static METIS into one shared library. The built
+library stays in-tree so that it travels with the repository snapshot.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIBDIR = PKG / "lib"
+LIB = LIBDIR / "libsymla_b200.so"
+CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
+NVCC = str(CUDA_HOME / "bin" / "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+HOST_SRCS = ["host/symbolic.cpp", "host/amd.cpp", "host/metis_order.cpp"]
+CUDA_SRCS = ["gpu/capi.cu", "gpu/factor_kernels.cu", "gpu/solve_kernels.cu"]
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError(f"build step failed: {cmd[0]} {cmd[-1]}")
+
+
+def _stale(out: Path, deps: list[Path]) -> bool:
+    if not out.exists():
+        return True
+    t = out.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def _headers() -> list[Path]:
+    hs = list(CSRC.rglob("*.h")) + list(CSRC.rglob("*.hpp")) + list(CSRC.rglob("*.cuh"))
+    hs.append(PKG.parent / "include" / "symla_gpu.h")
+    return hs
+
+
+def build(verbose: bool = False, force: bool = False) -> Path:
+    """Compile every source that changed and link the shared library."""
+    BUILD.mkdir(exist_ok=True)
+    LIBDIR.mkdir(exist_ok=True)
+    hdrs = _headers()
+    objs: list[Path] = []
+    for src in HOST_SRCS:
+        s = CSRC / src
+        o = BUILD / (s.stem + ".o")
+        objs.append(o)
+        if force or _stale(o, [s] + hdrs):
+            _run(["g++", "-std=c++17", "-O3", "-fPIC", "-Wall", "-c", str(s), "-o", str(o)])
+    for src in CUDA_SRCS:
+        s = CSRC / src
+        o = BUILD / (s.stem + ".o")
+        objs.append(o)
+        if force or _stale(o, [s] + hdrs):
+            cmd = [NVCC, *ARCH, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC",
+                   "--expt-relaxed-constexpr", "-c", str(s), "-o", str(o)]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+            _run(cmd)
+    metis = CUDA_HOME / "lib64" / "libmetis_static.a"
+    if force or _stale(LIB, objs):
+        _run([NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), str(metis), "-lcudart_static"])
+    return LIB
+
+
+def clean() -> None:
+    shutil.rmtree(BUILD, ignore_errors=True)
+    if LIB.exists():
+        LIB.unlink()
+
+
+if __name__ == "__main__":
+    build(verbose="-v" in sys.argv, force="-f" in sys.argv)
+    print(LIB)

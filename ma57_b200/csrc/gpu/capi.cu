@@ -1,0 +1,1232 @@
+// C ABI implementation (include/symla_gpu.h): symbolic entry points, the
+// device plan, and the factorize / solve / refine drivers.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../../include/symla_gpu.h"
+#include "../host/symbolic.hpp"
+#include "context.hpp"
+#include "factor_kernels.h"
+
+using namespace symla_gpu;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+struct CudaError : std::runtime_error {
+  cudaError_t err;
+  CudaError(cudaError_t e, const char* what) : std::runtime_error(what), err(e) {}
+};
+struct SymlaError : std::runtime_error {
+  int code;
+  SymlaError(int c, const std::string& what) : std::runtime_error(what), code(c) {}
+};
+
+#define CK(call)                                                                                         \
+  do {                                                                                                   \
+    cudaError_t e_ = (call);                                                                             \
+    if (e_ != cudaSuccess) {                                                                             \
+      char buf_[512];                                                                                    \
+      snprintf(buf_, sizeof buf_, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+      throw CudaError(e_, buf_);                                                                         \
+    }                                                                                                    \
+  } while (0)
+
+template <typename F>
+int guarded(F&& body) {
+  try {
+    body();
+    return SYMLA_OK;
+  } catch (const SymlaError& e) {
+    return set_error(e.code, e.what());
+  } catch (const CudaError& e) {
+    if (e.err == cudaErrorMemoryAllocation) return set_error(SYMLA_ERR_OOM, e.what());
+    if (e.err == cudaErrorNoDevice || e.err == cudaErrorInsufficientDriver) return set_error(SYMLA_ERR_NO_DEVICE, e.what());
+    return set_error(SYMLA_ERR_CUDA, e.what());
+  } catch (const std::bad_alloc&) {
+    return set_error(SYMLA_ERR_OOM, "host allocation failed");
+  } catch (const std::invalid_argument& e) {
+    return set_error(SYMLA_ERR_INVALID, e.what());
+  } catch (const std::exception& e) {
+    return set_error(SYMLA_ERR_INTERNAL, e.what());
+  }
+}
+
+template <typename T>
+T* dalloc(size_t count) {
+  if (count == 0) count = 1;
+  void* p = nullptr;
+  CK(cudaMalloc(&p, count * sizeof(T)));
+  return static_cast<T*>(p);
+}
+
+template <typename T>
+T* dupload(const std::vector<T>& v, cudaStream_t s) {
+  T* p = dalloc<T>(v.size());
+  if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  return p;
+}
+
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+}  // namespace
+
+extern "C" const char* symla_last_error(void) { return g_last_error.c_str(); }
+
+// ---------------------------------------------------------------------------
+// Symbolic
+extern "C" int symla_analyze(int n, const int* colptr, const int* rowind, int ordering, int max_relax_size,
+                             double max_relax_fill_fraction, symla_symbolic** out) {
+  if (!out) return set_error(SYMLA_ERR_INVALID, "symla_analyze: out is NULL");
+  *out = nullptr;
+  if (n < 0 || (n > 0 && (!colptr || !rowind))) return set_error(SYMLA_ERR_BAD_SIZE, "symla_analyze: bad matrix");
+  if (ordering < 0 || ordering > 2) return set_error(SYMLA_ERR_INVALID, "symla::computeOrdering: unknown OrderingType");
+  return guarded([&] {
+    symla_host::SymbolicFactorOptions opt;
+    opt.max_relax_size = max_relax_size;
+    opt.max_relax_fill_fraction = max_relax_fill_fraction;
+    auto* s = new symla_symbolic();
+    try {
+      s->sf = symla_host::analyze(n, colptr, rowind, static_cast<symla_host::OrderingType>(ordering), opt);
+    } catch (const std::runtime_error& e) {
+      delete s;
+      throw SymlaError(SYMLA_ERR_INTERNAL, e.what());
+    } catch (...) {
+      delete s;
+      throw;
+    }
+    *out = s;
+  });
+}
+
+extern "C" void symla_symbolic_destroy(symla_symbolic* sym) { delete sym; }
+
+extern "C" int symla_symbolic_get_info(const symla_symbolic* sym, symla_symbolic_info* info) {
+  if (!sym || !info) return set_error(SYMLA_ERR_INVALID, "null argument");
+  const auto& sf = sym->sf;
+  info->n = sf.etree.n;
+  info->num_supernodes = static_cast<int>(sf.supernodes.size());
+  info->num_fundamental = static_cast<int>(sf.fundamentalSupernodes.size());
+  info->pattern_len = 0;
+  info->storage_nnz = 0;
+  for (const auto& s : sf.supernodes) {
+    info->pattern_len += static_cast<int64_t>(s.rowPattern.size());
+    info->storage_nnz += s.storageNnz();
+  }
+  info->fundamental_len = 0;
+  for (const auto& s : sf.fundamentalSupernodes) info->fundamental_len += static_cast<int64_t>(s.rowPattern.size());
+  return SYMLA_OK;
+}
+
+namespace {
+void export_sn(const std::vector<symla_host::Supernode>& v, int* first, int* ncols, int* ptr, int* rows) {
+  int64_t off = 0;
+  for (size_t i = 0; i < v.size(); ++i) {
+    if (first) first[i] = v[i].firstCol;
+    if (ncols) ncols[i] = v[i].ncols;
+    if (ptr) ptr[i] = static_cast<int>(off);
+    if (rows) std::copy(v[i].rowPattern.begin(), v[i].rowPattern.end(), rows + off);
+    off += static_cast<int64_t>(v[i].rowPattern.size());
+  }
+  if (ptr) ptr[v.size()] = static_cast<int>(off);
+}
+}  // namespace
+
+extern "C" int symla_symbolic_get(const symla_symbolic* sym, int* perm, int* etree_parent, int* etree_colcount,
+                                  int* sn_first, int* sn_ncols, int* sn_ptr, int* sn_rows) {
+  if (!sym) return set_error(SYMLA_ERR_INVALID, "null symbolic");
+  const auto& sf = sym->sf;
+  if (perm) std::copy(sf.perm.begin(), sf.perm.end(), perm);
+  if (etree_parent) std::copy(sf.etree.parent.begin(), sf.etree.parent.end(), etree_parent);
+  if (etree_colcount) std::copy(sf.etree.colCount.begin(), sf.etree.colCount.end(), etree_colcount);
+  export_sn(sf.supernodes, sn_first, sn_ncols, sn_ptr, sn_rows);
+  return SYMLA_OK;
+}
+
+extern "C" int symla_symbolic_get_fundamental(const symla_symbolic* sym, int* sn_first, int* sn_ncols, int* sn_ptr,
+                                              int* sn_rows) {
+  if (!sym) return set_error(SYMLA_ERR_INVALID, "null symbolic");
+  export_sn(sym->sf.fundamentalSupernodes, sn_first, sn_ncols, sn_ptr, sn_rows);
+  return SYMLA_OK;
+}
+
+extern "C" int symla_symbolic_import(int n, const int* perm, const int* etree_parent, int num_supernodes,
+                                     const int* sn_first, const int* sn_ncols, const int* sn_ptr, const int* sn_rows,
+                                     symla_symbolic** out) {
+  if (!out || n < 0 || num_supernodes < 0) return set_error(SYMLA_ERR_INVALID, "symla_symbolic_import: bad arguments");
+  return guarded([&] {
+    auto* s = new symla_symbolic();
+    s->sf.perm.assign(perm, perm + n);
+    s->sf.etree.n = n;
+    s->sf.etree.parent.assign(etree_parent, etree_parent + n);
+    s->sf.etree.colCount.assign(n, 0);
+    s->sf.supernodes.resize(num_supernodes);
+    for (int i = 0; i < num_supernodes; ++i) {
+      s->sf.supernodes[i].firstCol = sn_first[i];
+      s->sf.supernodes[i].ncols = sn_ncols[i];
+      s->sf.supernodes[i].rowPattern.assign(sn_rows + sn_ptr[i], sn_rows + sn_ptr[i + 1]);
+    }
+    *out = s;
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Plan construction
+namespace {
+
+int pad_ld(int m) { return m; }
+
+// Builds invmap (length m_parent) and relmap (length cb) for child c of a
+// parent whose local row order is given by parentLocal (global -> local).
+void build_maps(const std::vector<int>& cbRows, const std::unordered_map<int, int>* g2l,
+                const std::vector<int>* parentRows, int mParent, std::vector<int>& invmap, std::vector<int>& relmap) {
+  invmap.assign(mParent, -1);
+  relmap.resize(cbRows.size());
+  for (size_t t = 0; t < cbRows.size(); ++t) {
+    int loc;
+    if (g2l) {
+      auto it = g2l->find(cbRows[t]);
+      if (it == g2l->end()) throw SymlaError(SYMLA_ERR_INTERNAL, "extend-add map: child row missing in parent front");
+      loc = it->second;
+    } else {
+      auto it = std::lower_bound(parentRows->begin(), parentRows->end(), cbRows[t]);
+      if (it == parentRows->end() || *it != cbRows[t])
+        throw SymlaError(SYMLA_ERR_INTERNAL, "extend-add map: child row missing in parent pattern");
+      loc = static_cast<int>(it - parentRows->begin());
+    }
+    relmap[t] = loc;
+    invmap[loc] = static_cast<int>(t);
+  }
+}
+
+void build_level_lists(symla_gpu_ctx* c, const std::vector<int>& frontsOfLevel, LevelLists& L) {
+  L.small.clear();
+  L.large.clear();
+  L.tasks.clear();
+  L.all = frontsOfLevel;
+  L.small_max_m = L.large_max_m = 0;
+  L.panels = 0;
+  int tiles = 0;
+  for (int s : frontsOfLevel) {
+    const auto& f = c->fronts[s];
+    if (f.m <= kSmallFrontMax) {
+      L.small.push_back(s);
+      L.small_max_m = std::max(L.small_max_m, f.m);
+    } else {
+      L.large.push_back(s);
+      L.large_max_m = std::max(L.large_max_m, f.m);
+      L.panels = std::max(L.panels, (f.nelig + kPanelWidth - 1) / kPanelWidth);
+      for (int j0 = 0; j0 < f.m; j0 += 32) {
+        L.tasks.push_back(s);
+        L.tasks.push_back(j0);
+      }
+      const int mt = std::max(0, f.m - std::min(f.nelig, kPanelWidth));
+      const int nt = (mt + 63) / 64;
+      tiles = std::max(tiles, nt * (nt + 1) / 2);
+    }
+  }
+  if (!L.large.empty()) {
+    const int budget = std::max(1, 148 * 6 / static_cast<int>(L.large.size()));
+    L.trailing_grid = std::max(1, std::min(tiles, budget));
+  } else {
+    L.trailing_grid = 0;
+  }
+}
+
+void free_level_device(LevelLists& L) {
+  dfree(L.d_small);
+  dfree(L.d_large);
+  dfree(L.d_tasks);
+  dfree(L.d_all);
+  L.d_small = L.d_large = L.d_tasks = L.d_all = nullptr;
+}
+
+void upload_level_lists(LevelLists& L, cudaStream_t s) {
+  free_level_device(L);
+  L.d_small = dupload(L.small, s);
+  L.d_large = dupload(L.large, s);
+  L.d_tasks = dupload(L.tasks, s);
+  L.d_all = dupload(L.all, s);
+}
+
+void build_plan(symla_gpu_ctx* c, const symla_host::SymbolicFactor& sf, const int* colptr, const int* rowind) {
+  const int n = c->n;
+  const auto& sns = sf.supernodes;
+  const int numSN = static_cast<int>(sns.size());
+  c->numSN = numSN;
+  c->perm = sf.perm;
+  c->newIndexOf.assign(n, 0);
+  for (int k = 0; k < n; ++k) c->newIndexOf[sf.perm[k]] = k;
+  c->rowPatterns.resize(numSN);
+  for (int s = 0; s < numSN; ++s) c->rowPatterns[s] = sns[s].rowPattern;
+
+  // supernode tree (multifrontal.hpp:312-332): children in increasing index
+  std::vector<int> colToSN(n, -1);
+  for (int s = 0; s < numSN; ++s)
+    for (int j = sns[s].firstCol; j < sns[s].firstCol + sns[s].ncols; ++j) colToSN[j] = s;
+  c->fronts.assign(numSN, HostFront());
+  for (int s = 0; s < numSN; ++s) {
+    auto& f = c->fronts[s];
+    f.firstCol = sns[s].firstCol;
+    f.ncols = sns[s].ncols;
+    f.nelig = f.ncols;
+    f.nextra = 0;
+    f.m = static_cast<int>(sns[s].rowPattern.size());
+    f.ld = pad_ld(f.m);
+    f.rowPattern = &c->rowPatterns[s];
+    const int last = f.firstCol + f.ncols - 1;
+    const int p = sf.etree.parent[last];
+    f.parent = (p == -1) ? -1 : colToSN[p];
+  }
+  for (int s = 0; s < numSN; ++s)
+    if (c->fronts[s].parent >= 0) c->fronts[c->fronts[s].parent].children.push_back(s);
+  int numLevels = 0;
+  for (int s = 0; s < numSN; ++s) {
+    auto& f = c->fronts[s];
+    int lv = 0;
+    for (int ch : f.children) lv = std::max(lv, c->fronts[ch].level + 1);
+    f.level = lv;
+    numLevels = std::max(numLevels, lv + 1);
+  }
+  c->numLevels = numLevels;
+
+  // arena and pools
+  std::vector<long long> foff(numSN);
+  long long arena = 0, fidxTot = 0, dTot = 0;
+  c->fidx_off.assign(numSN, 0);
+  c->dpos.assign(numSN, 0);
+  c->plan_sum_m2 = 0.0;
+  c->plan_max_m = 0;
+  for (int s = 0; s < numSN; ++s) {
+    const auto& f = c->fronts[s];
+    foff[s] = arena;
+    arena += static_cast<long long>(f.ld) * f.m;
+    c->fidx_off[s] = fidxTot;
+    fidxTot += f.m;
+    c->dpos[s] = dTot;
+    dTot += f.ncols;
+    c->plan_sum_m2 += static_cast<double>(f.m) * f.m;
+    c->plan_max_m = std::max(c->plan_max_m, f.m);
+  }
+  c->arena_doubles = static_cast<size_t>(arena);
+  c->d_arena = dalloc<double>(arena);
+  c->fidx_static.assign(fidxTot, 0);
+  for (int s = 0; s < numSN; ++s)
+    std::copy(c->rowPatterns[s].begin(), c->rowPatterns[s].end(), c->fidx_static.begin() + c->fidx_off[s]);
+  c->d_fidx = dupload(c->fidx_static, c->stream);
+  c->d_lperm = dalloc<int>(fidxTot);
+  c->d_lpos = dalloc<int>(fidxTot);
+  c->d_Dd = dalloc<double>(dTot);
+  c->d_Do = dalloc<double>(dTot);
+  c->d_pk = dalloc<int8_t>(dTot);
+
+  // extend-add maps
+  std::vector<int> mapPool;
+  std::vector<std::pair<long long, long long>> linkOffsets;  // (invmap off, relmap off)
+  c->hlinks.clear();
+  c->link_begin_static.assign(numSN, 0);
+  c->link_end_static.assign(numSN, 0);
+  std::vector<int> inv, rel, cbRows;
+  struct LinkTmp {
+    int child;
+    long long inv, rel;
+    int cb;
+  };
+  std::vector<LinkTmp> ltmp;
+  for (int s = 0; s < numSN; ++s) {
+    const auto& f = c->fronts[s];
+    c->link_begin_static[s] = static_cast<int>(ltmp.size());
+    for (int ch : f.children) {
+      const auto& cf = c->fronts[ch];
+      cbRows.assign(c->rowPatterns[ch].begin() + cf.ncols, c->rowPatterns[ch].end());
+      build_maps(cbRows, nullptr, &c->rowPatterns[s], f.m, inv, rel);
+      LinkTmp lt{ch, static_cast<long long>(mapPool.size()), 0, static_cast<int>(cbRows.size())};
+      mapPool.insert(mapPool.end(), inv.begin(), inv.end());
+      lt.rel = static_cast<long long>(mapPool.size());
+      mapPool.insert(mapPool.end(), rel.begin(), rel.end());
+      ltmp.push_back(lt);
+    }
+    c->link_end_static[s] = static_cast<int>(ltmp.size());
+  }
+  c->d_maps = dupload(mapPool, c->stream);
+  c->hlinks.resize(ltmp.size());
+  for (size_t i = 0; i < ltmp.size(); ++i) {
+    c->hlinks[i].child = ltmp[i].child;
+    c->hlinks[i].invmap = c->d_maps + ltmp[i].inv;
+    c->hlinks[i].relmap = c->d_maps + ltmp[i].rel;
+    c->hlinks[i].cb = ltmp[i].cb;
+  }
+  c->hlinks_static = c->hlinks;
+  c->links_capacity = std::max<size_t>(64, c->hlinks.size() * 2 + 64);
+  c->d_links = dalloc<ChildLink>(c->links_capacity);
+  if (!c->hlinks.empty())
+    CK(cudaMemcpyAsync(c->d_links, c->hlinks.data(), c->hlinks.size() * sizeof(ChildLink), cudaMemcpyHostToDevice,
+                       c->stream));
+
+  // A entries: (final column lo, pattern position of hi) -> value index
+  struct AEnt {
+    int col, pos, j, idx;
+  };
+  std::vector<AEnt> ents;
+  ents.reserve(c->nnz);
+  for (int cc = 0; cc < n; ++cc) {
+    for (int p = colptr[cc]; p < colptr[cc + 1]; ++p) {
+      const int r = rowind[p];
+      if (r < cc) continue;
+      const int nr = c->newIndexOf[r], nc = c->newIndexOf[cc];
+      const int lo = std::min(nr, nc), hi = std::max(nr, nc);
+      const int s = colToSN[lo];
+      const auto& rp = c->rowPatterns[s];
+      auto it = std::lower_bound(rp.begin(), rp.end(), hi);
+      if (it == rp.end() || *it != hi) throw SymlaError(SYMLA_ERR_INTERNAL, "A entry outside the supernode pattern");
+      ents.push_back(AEnt{lo, static_cast<int>(it - rp.begin()), lo - c->fronts[s].firstCol, p});
+    }
+  }
+  std::sort(ents.begin(), ents.end(), [](const AEnt& a, const AEnt& b) {
+    if (a.col != b.col) return a.col < b.col;
+    return a.pos < b.pos;
+  });
+  std::vector<int> acolptr(n + 1, 0), aj(ents.size()), apos(ents.size()), aidx(ents.size());
+  for (const auto& e : ents) acolptr[e.col + 1]++;
+  for (int i = 0; i < n; ++i) acolptr[i + 1] += acolptr[i];
+  for (size_t t = 0; t < ents.size(); ++t) {
+    aj[t] = ents[t].j;
+    apos[t] = ents[t].pos;
+    aidx[t] = ents[t].idx;
+  }
+  c->d_a_colptr = dupload(acolptr, c->stream);
+  c->d_a_j = dupload(aj, c->stream);
+  c->d_a_pos = dupload(apos, c->stream);
+  c->d_a_idx = dupload(aidx, c->stream);
+
+  // descriptors
+  c->hdesc.assign(numSN, FrontDesc());
+  for (int s = 0; s < numSN; ++s) {
+    const auto& f = c->fronts[s];
+    FrontDesc& d = c->hdesc[s];
+    d.F = c->d_arena + foff[s];
+    d.fidx = c->d_fidx + c->fidx_off[s];
+    d.lperm = c->d_lperm + c->fidx_off[s];
+    d.lpos = c->d_lpos + c->fidx_off[s];
+    d.Dd = c->d_Dd + c->dpos[s];
+    d.Do = c->d_Do + c->dpos[s];
+    d.pk = c->d_pk + c->dpos[s];
+    d.W = nullptr;
+    d.m = f.m;
+    d.ld = f.ld;
+    d.ncols = f.ncols;
+    d.nelig = f.nelig;
+    d.nextra = 0;
+    d.parent = f.parent;
+    d.ch_begin = c->link_begin_static[s];
+    d.ch_end = c->link_end_static[s];
+    d.a_begin = f.firstCol;
+    d.a_end = f.firstCol + f.ncols;
+    d.level = f.level;
+    d.wld = f.m;
+  }
+  c->hdesc_static = c->hdesc;
+  c->d_desc = dupload(c->hdesc, c->stream);
+  c->d_state = dalloc<FrontState>(numSN);
+  c->d_glob = dalloc<FactorGlobals>(1);
+
+  // levels
+  std::vector<std::vector<int>> byLevel(numLevels);
+  for (int s = 0; s < numSN; ++s) byLevel[c->fronts[s].level].push_back(s);
+  c->levels.assign(numLevels, LevelLists());
+  for (int l = 0; l < numLevels; ++l) {
+    build_level_lists(c, byLevel[l], c->levels[l]);
+    upload_level_lists(c->levels[l], c->stream);
+  }
+
+  // residual: full symmetric CSR gathered from the stored lower triangle,
+  // columns sorted per row; and the stored-entry rows for ||A||
+  std::vector<std::vector<std::pair<int, int>>> rows(n);
+  std::vector<int> scount(n + 1, 0);
+  for (int cc = 0; cc < n; ++cc) {
+    for (int p = colptr[cc]; p < colptr[cc + 1]; ++p) {
+      const int r = rowind[p];
+      scount[r + 1]++;
+      if (r < cc) continue;
+      rows[r].push_back({cc, p});
+      if (r != cc) rows[cc].push_back({r, p});
+    }
+  }
+  std::vector<int> rowptr(n + 1, 0), colind, vidx;
+  for (int i = 0; i < n; ++i) {
+    std::sort(rows[i].begin(), rows[i].end());
+    rowptr[i + 1] = rowptr[i] + static_cast<int>(rows[i].size());
+    for (auto& pr : rows[i]) {
+      colind.push_back(pr.first);
+      vidx.push_back(pr.second);
+    }
+  }
+  for (int i = 0; i < n; ++i) scount[i + 1] += scount[i];
+  std::vector<int> svidx(c->nnz), fill(scount.begin(), scount.end() - 1);
+  for (int cc = 0; cc < n; ++cc)
+    for (int p = colptr[cc]; p < colptr[cc + 1]; ++p) svidx[fill[rowind[p]]++] = p;
+  c->d_rowptr = dupload(rowptr, c->stream);
+  c->d_colind = dupload(colind, c->stream);
+  c->d_vidx = dupload(vidx, c->stream);
+  c->d_srowptr = dupload(scount, c->stream);
+  c->d_svidx = dupload(svidx, c->stream);
+  c->d_perm = dupload(c->perm, c->stream);
+  c->d_values = dalloc<double>(c->nnz);
+  c->d_sign_final = dalloc<int>(n);
+  c->d_front_delta = dalloc<double>(numSN);
+  c->d_norms = dalloc<double>(8);
+  c->hstate.assign(numSN, FrontState());
+  for (int i = 0; i < 8; ++i) CK(cudaEventCreate(&c->ev[i]));
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+void free_dynamic(symla_gpu_ctx* c) {
+  for (void* p : c->dyn_allocs) dfree(p);
+  c->dyn_allocs.clear();
+}
+
+// Reset descriptors / links to the static plan (start of every factorize).
+void reset_to_static(symla_gpu_ctx* c) {
+  bool changed = false;
+  for (int s = 0; s < c->numSN; ++s)
+    if (c->fronts[s].replanned) {
+      auto& f = c->fronts[s];
+      f.replanned = false;
+      f.nextra = 0;
+      f.nelig = f.ncols;
+      f.m = static_cast<int>(c->rowPatterns[s].size());
+      f.ld = pad_ld(f.m);
+      changed = true;
+    }
+  if (changed || c->hdesc.size() != c->hdesc_static.size()) {
+    c->hdesc = c->hdesc_static;
+    c->hlinks = c->hlinks_static;
+    CK(cudaMemcpyAsync(c->d_desc, c->hdesc.data(), c->hdesc.size() * sizeof(FrontDesc), cudaMemcpyHostToDevice,
+                       c->stream));
+    if (!c->hlinks.empty())
+      CK(cudaMemcpyAsync(c->d_links, c->hlinks.data(), c->hlinks.size() * sizeof(ChildLink), cudaMemcpyHostToDevice,
+                         c->stream));
+    c->w_dirty = true;
+  }
+  // row-index pool back to the symbolic order (pivoting permutes it)
+  CK(cudaMemcpyAsync(c->d_fidx, c->fidx_static.data(), c->fidx_static.size() * sizeof(int), cudaMemcpyHostToDevice,
+                     c->stream));
+  free_dynamic(c);
+}
+
+KernelOpts make_kernel_opts(symla_gpu_ctx* c, const symla_factor_opts* o) {
+  KernelOpts k{};
+  k.mode = o->mode;
+  k.precision = o->precision;
+  k.zero_tol = o->zero_tolerance;
+  k.rel_floor = o->relative_pivot_floor;
+  k.static_delta = o->static_delta;
+  k.static_rel_floor = o->static_rel_floor;
+  k.static_abs_floor = o->static_abs_floor;
+  k.sign_final = (o->mode == SYMLA_MODE_STATIC && o->expected_sign) ? c->d_sign_final : nullptr;
+  k.front_delta = (o->mode == SYMLA_MODE_STATIC && o->front_delta) ? c->d_front_delta : nullptr;
+  k.values = c->d_values;
+  k.a_j = c->d_a_j;
+  k.a_pos = c->d_a_pos;
+  k.a_idx = c->d_a_idx;
+  return k;
+}
+
+void launch_level(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
+                  const int* d_small, const int* d_large, const int* d_tasks) {
+  cudaStream_t st = c->stream;
+  if (!L.small.empty())
+    launch_factor_small(c->d_desc, c->d_links, c->d_state, d_small, static_cast<int>(L.small.size()), L.small_max_m,
+                        c->d_a_colptr, ko, c->d_glob, level, dynamic, st);
+  if (!L.large.empty()) {
+    launch_assemble(c->d_desc, c->d_links, c->d_state, d_tasks, static_cast<int>(L.tasks.size() / 2), c->d_a_colptr,
+                    ko, c->d_glob, level, dynamic, st);
+    for (int it = 0; it < L.panels; ++it) {
+      launch_panel(c->d_desc, c->d_state, d_large, static_cast<int>(L.large.size()), L.large_max_m, kPanelWidth, ko,
+                   c->d_glob, level, dynamic, st);
+      launch_trailing(c->d_desc, c->d_state, d_large, static_cast<int>(L.large.size()), L.trailing_grid, c->d_glob,
+                      level, dynamic, st);
+    }
+  }
+  CK(cudaGetLastError());
+}
+
+// Re-plan front s whose children delayed columns (multifrontal.hpp:453-479)
+// and upload its new descriptor and extend-add maps.
+void replan_front(symla_gpu_ctx* c, int s) {
+  auto& f = c->fronts[s];
+  const auto& rp = c->rowPatterns[s];
+  // children's contribution-block row indices, in their current order
+  std::vector<std::vector<int>> cbRowsOf(f.children.size());
+  std::vector<int> extras;
+  for (size_t t = 0; t < f.children.size(); ++t) {
+    const int ch = f.children[t];
+    const auto& cd = c->hdesc[ch];
+    const int np = c->hstate[ch].npiv;
+    std::vector<int> rowsAll(cd.m);
+    CK(cudaMemcpyAsync(rowsAll.data(), cd.fidx, cd.m * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    cbRowsOf[t].assign(rowsAll.begin() + np, rowsAll.end());
+    for (int g : cbRowsOf[t])
+      if (!std::binary_search(rp.begin(), rp.end(), g)) extras.push_back(g);
+  }
+  std::sort(extras.begin(), extras.end());
+  extras.erase(std::unique(extras.begin(), extras.end()), extras.end());
+  const int nExtra = static_cast<int>(extras.size());
+  f.nextra = nExtra;
+  f.nelig = f.ncols + nExtra;
+  f.m = static_cast<int>(rp.size()) + nExtra;
+  f.ld = pad_ld(f.m);
+  f.replanned = true;
+  std::vector<int> frontIdx(f.m);
+  for (int j = 0; j < f.ncols; ++j) frontIdx[j] = f.firstCol + j;
+  for (int j = 0; j < nExtra; ++j) frontIdx[f.ncols + j] = extras[j];
+  for (int j = f.ncols; j < static_cast<int>(rp.size()); ++j) frontIdx[f.nelig + (j - f.ncols)] = rp[j];
+  std::unordered_map<int, int> g2l;
+  g2l.reserve(f.m * 2);
+  for (int t = 0; t < f.m; ++t) g2l[frontIdx[t]] = t;
+
+  FrontDesc d = c->hdesc[s];
+  double* F = dalloc<double>(static_cast<size_t>(f.ld) * f.m);
+  c->dyn_allocs.push_back(F);
+  int* fidx = dupload(frontIdx, c->stream);
+  c->dyn_allocs.push_back(fidx);
+  int* lperm = dalloc<int>(f.m);
+  int* lpos = dalloc<int>(f.m);
+  c->dyn_allocs.push_back(lperm);
+  c->dyn_allocs.push_back(lpos);
+  double* Dd = dalloc<double>(f.nelig);
+  double* Do = dalloc<double>(f.nelig);
+  int8_t* pk = dalloc<int8_t>(f.nelig);
+  c->dyn_allocs.push_back(Dd);
+  c->dyn_allocs.push_back(Do);
+  c->dyn_allocs.push_back(pk);
+  d.F = F;
+  d.fidx = fidx;
+  d.lperm = lperm;
+  d.lpos = lpos;
+  d.Dd = Dd;
+  d.Do = Do;
+  d.pk = pk;
+  d.m = f.m;
+  d.ld = f.ld;
+  d.nelig = f.nelig;
+  d.nextra = nExtra;
+  d.wld = f.m;
+
+  // maps for every child
+  std::vector<int> pool, inv, rel;
+  std::vector<std::pair<size_t, size_t>> offs;
+  for (size_t t = 0; t < f.children.size(); ++t) {
+    build_maps(cbRowsOf[t], &g2l, nullptr, f.m, inv, rel);
+    offs.push_back({pool.size(), pool.size() + inv.size()});
+    pool.insert(pool.end(), inv.begin(), inv.end());
+    pool.insert(pool.end(), rel.begin(), rel.end());
+  }
+  int* dmaps = dupload(pool, c->stream);
+  c->dyn_allocs.push_back(dmaps);
+  const int begin = static_cast<int>(c->hlinks.size());
+  for (size_t t = 0; t < f.children.size(); ++t) {
+    ChildLink L;
+    L.child = f.children[t];
+    L.invmap = dmaps + offs[t].first;
+    L.relmap = dmaps + offs[t].second;
+    L.cb = static_cast<int>(cbRowsOf[t].size());
+    c->hlinks.push_back(L);
+  }
+  d.ch_begin = begin;
+  d.ch_end = static_cast<int>(c->hlinks.size());
+  if (c->hlinks.size() > c->links_capacity) {
+    size_t cap = c->hlinks.size() * 2;
+    ChildLink* nl = dalloc<ChildLink>(cap);
+    dfree(c->d_links);
+    c->d_links = nl;
+    c->links_capacity = cap;
+    CK(cudaMemcpyAsync(c->d_links, c->hlinks.data(), c->hlinks.size() * sizeof(ChildLink), cudaMemcpyHostToDevice,
+                       c->stream));
+  } else {
+    CK(cudaMemcpyAsync(c->d_links + begin, c->hlinks.data() + begin, f.children.size() * sizeof(ChildLink),
+                       cudaMemcpyHostToDevice, c->stream));
+  }
+  c->hdesc[s] = d;
+  CK(cudaMemcpyAsync(c->d_desc + s, &c->hdesc[s], sizeof(FrontDesc), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->w_dirty = true;
+}
+
+void read_states(symla_gpu_ctx* c) {
+  CK(cudaMemcpyAsync(c->hstate.data(), c->d_state, c->numSN * sizeof(FrontState), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_factor_info* info) {
+  cudaStream_t st = c->stream;
+  reset_to_static(c);
+  const KernelOpts ko = make_kernel_opts(c, o);
+  CK(cudaMemsetAsync(c->d_state, 0, c->numSN * sizeof(FrontState), st));
+  FactorGlobals g0{INT_MAX, 0, -1, 0};
+  CK(cudaMemcpyAsync(c->d_glob, &g0, sizeof g0, cudaMemcpyHostToDevice, st));
+  CK(cudaEventRecord(c->ev[0], st));
+  for (int l = 0; l < c->numLevels; ++l) {
+    const LevelLists& L = c->levels[l];
+    launch_level(c, L, l, ko, 0, L.d_small, L.d_large, L.d_tasks);
+  }
+  FactorGlobals g;
+  CK(cudaMemcpyAsync(&g, c->d_glob, sizeof g, cudaMemcpyDeviceToHost, st));
+  read_states(c);
+  bool dynamic = false;
+  if (g.delay_level != INT_MAX) {
+    // Delayed pivots: fronts above the delaying level were skipped; re-plan
+    // and run them level by level with the actual contribution blocks.
+    dynamic = true;
+    for (int l = g.delay_level + 1; l < c->numLevels; ++l) {
+      const LevelLists& Ls = c->levels[l];
+      for (int s : Ls.all) {
+        bool childDelayed = false;
+        for (int ch : c->fronts[s].children)
+          if (c->hstate[ch].npiv < c->hdesc[ch].nelig) childDelayed = true;
+        if (childDelayed) replan_front(c, s);
+      }
+      LevelLists L;
+      build_level_lists(c, Ls.all, L);
+      upload_level_lists(L, st);
+      launch_level(c, L, l, ko, 1, L.d_small, L.d_large, L.d_tasks);
+      read_states(c);
+      free_level_device(L);
+    }
+  }
+  CK(cudaEventRecord(c->ev[1], st));
+  CK(cudaEventSynchronize(c->ev[1]));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+  if (!dynamic) read_states(c);
+
+  // reductions (multifrontal.hpp:795-803)
+  symla_factor_info r{};
+  c->singular = false;
+  c->singularCols.clear();
+  double maxGrowth = 1.0;
+  for (int s = 0; s < c->numSN; ++s) {
+    const FrontState& S = c->hstate[s];
+    r.n_pos += S.n_pos;
+    r.n_neg += S.n_neg;
+    r.n_zero += S.n_zero;
+    r.num_perturbed += S.num_perturbed;
+    r.total_perturbation += S.perturb;
+    r.num_delayed += c->fronts[s].nextra;
+    if (S.orig_max > 0) maxGrowth = std::max(maxGrowth, S.running_max / S.orig_max);
+    if (S.flags & kFlagSingularRoot) {
+      c->singular = true;
+      const auto& d = c->hdesc[s];
+      std::vector<int> rows(d.m);
+      CK(cudaMemcpy(rows.data(), d.fidx, d.m * sizeof(int), cudaMemcpyDeviceToHost));
+      for (int i = S.npiv; i < d.m; ++i) c->singularCols.push_back(rows[i]);
+    }
+  }
+  std::sort(c->singularCols.begin(), c->singularCols.end());
+  r.singular = c->singular ? 1 : 0;
+  r.n_singular = static_cast<int>(c->singularCols.size());
+  r.used_dynamic_path = dynamic ? 1 : 0;
+  r.max_growth = maxGrowth;
+  r.factor_ms = ms;
+  c->phase_ms[6] = ms;
+  c->last_info = r;
+  c->last_precision = o->precision;
+  if (info) *info = r;
+  c->factorized = true;
+}
+
+void ensure_vectors(symla_gpu_ctx* c, int nrhs) {
+  if (nrhs <= c->vec_nrhs) return;
+  dfree(c->d_Bp);
+  dfree(c->d_Z);
+  dfree(c->d_Xf);
+  dfree(c->d_B);
+  dfree(c->d_X);
+  dfree(c->d_R);
+  dfree(c->d_dX);
+  dfree(c->d_Xn);
+  dfree(c->d_Rn);
+  const size_t len = static_cast<size_t>(c->n) * nrhs;
+  c->d_Bp = dalloc<double>(len);
+  c->d_Z = dalloc<double>(len);
+  c->d_Xf = dalloc<double>(len);
+  c->d_B = dalloc<double>(len);
+  c->d_X = dalloc<double>(len);
+  c->d_R = dalloc<double>(len);
+  c->d_dX = dalloc<double>(len);
+  c->d_Xn = dalloc<double>(len);
+  c->d_Rn = dalloc<double>(len);
+  c->vec_nrhs = nrhs;
+}
+
+void ensure_workspace(symla_gpu_ctx* c, int nrhs) {
+  if (!c->w_dirty && nrhs <= c->w_nrhs) return;
+  const int cap = std::max(nrhs, c->w_nrhs);
+  long long total = 0;
+  for (int s = 0; s < c->numSN; ++s) total += static_cast<long long>(c->hdesc[s].m) * cap;
+  dfree(c->d_W);
+  c->d_W = dalloc<double>(total);
+  long long off = 0;
+  for (int s = 0; s < c->numSN; ++s) {
+    c->hdesc[s].W = c->d_W + off;
+    c->hdesc[s].wld = c->hdesc[s].m;
+    off += static_cast<long long>(c->hdesc[s].m) * cap;
+  }
+  CK(cudaMemcpyAsync(c->d_desc, c->hdesc.data(), c->hdesc.size() * sizeof(FrontDesc), cudaMemcpyHostToDevice,
+                     c->stream));
+  // keep the static copies' W consistent for fronts that were not re-planned
+  for (int s = 0; s < c->numSN; ++s)
+    if (!c->fronts[s].replanned) c->hdesc_static[s].W = c->hdesc[s].W;
+  c->w_nrhs = cap;
+  c->w_dirty = false;
+}
+
+// X(final order scratch) := A^{-1} B for device B (ldb) into device X (ldx),
+// both in the original index space.
+void device_solve(symla_gpu_ctx* c, const double* dB, int ldb, int nrhs, double* dX, int ldx) {
+  cudaStream_t st = c->stream;
+  ensure_vectors(c, nrhs);
+  ensure_workspace(c, nrhs);
+  const int n = c->n;
+  launch_permute_in(n, nrhs, c->d_perm, dB, ldb, c->d_Bp, st);
+  CK(cudaEventRecord(c->ev[2], st));
+  for (int l = 0; l < c->numLevels; ++l) {
+    const auto& L = c->levels[l];
+    launch_forward(c->d_desc, c->d_links, c->d_state, L.d_all, static_cast<int>(L.all.size()), nrhs, c->d_Bp, c->d_Z,
+                   n, st);
+  }
+  CK(cudaEventRecord(c->ev[3], st));
+  for (int l = c->numLevels - 1; l >= 0; --l) {
+    const auto& L = c->levels[l];
+    launch_backward(c->d_desc, c->d_state, L.d_all, static_cast<int>(L.all.size()), nrhs, c->d_Z, c->d_Xf, n, st);
+  }
+  CK(cudaEventRecord(c->ev[4], st));
+  launch_permute_out(n, nrhs, c->d_perm, c->d_Xf, dX, ldx, st);
+  CK(cudaGetLastError());
+}
+
+void check_solvable(symla_gpu_ctx* c) {
+  if (!c->factorized)
+    throw SymlaError(SYMLA_ERR_NOT_FACTORIZED, "symla::SymLDLT::solve: factorize() must be called before solve()");
+  if (c->singular)
+    throw SymlaError(SYMLA_ERR_SINGULAR,
+                     "symla::SymLDLT::solve: factorization is numerically singular (see isSingular()/"
+                     "singularColumns()); refusing to solve");
+}
+
+void upload_values(symla_gpu_ctx* c, const double* values, int on_device) {
+  if (c->nnz == 0) return;
+  if (on_device)
+    CK(cudaMemcpyAsync(c->d_values, values, c->nnz * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  else
+    CK(cudaMemcpyAsync(c->d_values, values, c->nnz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+extern "C" int symla_gpu_create(const symla_symbolic* sym, int n, const int* colptr, const int* rowind, int device,
+                                symla_gpu_ctx** out) {
+  if (!out) return set_error(SYMLA_ERR_INVALID, "symla_gpu_create: out is NULL");
+  *out = nullptr;
+  if (!sym) return set_error(SYMLA_ERR_NOT_ANALYZED, "symla::SymLDLT::factorize: analyzePattern must be called first");
+  if (n != sym->sf.etree.n) return set_error(SYMLA_ERR_BAD_SIZE, "symla_gpu_create: matrix size differs from the analysis");
+  symla_gpu_ctx* c = new symla_gpu_ctx();
+  const int rc = guarded([&] {
+    int count = 0;
+    CK(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) throw SymlaError(SYMLA_ERR_NO_DEVICE, "symla_gpu_create: no such CUDA device");
+    c->device = device;
+    CK(cudaSetDevice(device));
+    static bool configured[64] = {};
+    if (!configured[device]) {
+      CK(configure_factor_kernels());
+      configured[device] = true;
+    }
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->n = n;
+    c->nnz = n > 0 ? colptr[n] : 0;
+    build_plan(c, sym->sf, colptr, rowind);
+  });
+  if (rc != SYMLA_OK) {
+    symla_gpu_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return SYMLA_OK;
+}
+
+extern "C" void symla_gpu_destroy(symla_gpu_ctx* c) {
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_dynamic(c);
+  for (auto& L : c->levels) free_level_device(L);
+  void* ptrs[] = {c->d_arena, c->d_fidx, c->d_lperm, c->d_lpos, c->d_Dd, c->d_Do, c->d_pk, c->d_maps, c->d_desc, c->d_links, c->d_state,
+                  c->d_glob, c->d_a_colptr, c->d_a_j, c->d_a_pos, c->d_a_idx, c->d_values, c->d_sign_final,
+                  c->d_front_delta, c->d_perm, c->d_rowptr, c->d_colind, c->d_vidx, c->d_srowptr, c->d_svidx, c->d_W,
+                  c->d_Bp, c->d_Z, c->d_Xf, c->d_B, c->d_X, c->d_R, c->d_dX, c->d_Xn, c->d_Rn, c->d_norms,
+                  c->d_scratch_int};
+  for (void* p : ptrs) dfree(p);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+extern "C" void symla_factor_opts_default(symla_factor_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->mode = SYMLA_MODE_THRESHOLD;
+  o->precision = SYMLA_PREC_FP64;
+  o->pivot_threshold = 0.01;
+  o->zero_tolerance = 1e-300;
+  o->relative_pivot_floor = 1e-12;
+  o->static_delta = 0.0;
+  o->static_rel_floor = 1e-8;
+  o->static_abs_floor = 1e-300;
+}
+
+extern "C" int symla_gpu_factorize(symla_gpu_ctx* c, const double* values, int values_on_device,
+                                   const symla_factor_opts* opts, symla_factor_info* info) {
+  if (!c) return set_error(SYMLA_ERR_NOT_ANALYZED, "symla::SymLDLT::factorize: analyzePattern must be called first");
+  symla_factor_opts def;
+  symla_factor_opts_default(&def);
+  if (!opts) opts = &def;
+  if (c->nnz > 0 && !values) return set_error(SYMLA_ERR_INVALID, "symla_gpu_factorize: values is NULL");
+  return guarded([&] {
+    CK(cudaSetDevice(c->device));
+    c->factorized = false;
+    upload_values(c, values, values_on_device);
+    if (opts->mode == SYMLA_MODE_STATIC) {
+      if (opts->expected_sign) {
+        std::vector<int> sf(c->n);
+        for (int t = 0; t < c->n; ++t) sf[t] = opts->expected_sign[c->perm[t]];
+        CK(cudaMemcpyAsync(c->d_sign_final, sf.data(), c->n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+      }
+      if (opts->front_delta) {
+        CK(cudaMemcpyAsync(c->d_front_delta, opts->front_delta, c->numSN * sizeof(double), cudaMemcpyHostToDevice,
+                           c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+      }
+    }
+    run_factorization(c, opts, info);
+  });
+}
+
+extern "C" void symla_regularize_opts_default(symla_regularize_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->initial_delta = 0.0;
+  o->max_retries = 10;
+  o->growth = 10.0;
+  o->static_rel_floor = 1e-8;
+  o->static_abs_floor = 1e-300;
+  o->expected_sign = nullptr;
+  o->kkt_n1 = -1;
+  o->kkt_n2 = -1;
+  o->precision = SYMLA_PREC_FP64;
+  o->front_delta = nullptr;
+}
+
+extern "C" int symla_gpu_factorize_regularized(symla_gpu_ctx* c, const double* values, int values_on_device,
+                                               const symla_regularize_opts* ro, symla_factor_info* info,
+                                               symla_regularize_info* rinfo) {
+  if (!c) return set_error(SYMLA_ERR_NOT_ANALYZED, "symla::SymLDLT::factorize: analyzePattern must be called first");
+  symla_regularize_opts def;
+  symla_regularize_opts_default(&def);
+  if (!ro) ro = &def;
+  const int n = c->n;
+  // solver.hpp:299-317: expected signs in the original index space
+  std::vector<int> signs(n, 0);
+  bool haveExpectation = false;
+  if (ro->expected_sign) {
+    signs.assign(ro->expected_sign, ro->expected_sign + n);
+    haveExpectation = true;
+  } else if (ro->kkt_n1 >= 0) {
+    if (ro->kkt_n1 + ro->kkt_n2 != n)
+      return set_error(SYMLA_ERR_BAD_SIZE,
+                       "symla::SymLDLT::factorize: setKKTBlockSizes(n1, n2) sizes do not sum to the matrix size");
+    for (int i = 0; i < ro->kkt_n1; ++i) signs[i] = -1;
+    for (int i = ro->kkt_n1; i < n; ++i) signs[i] = +1;
+    haveExpectation = true;
+  }
+  int expectedPos = 0, expectedNeg = 0;
+  for (int sgn : signs) {
+    if (sgn > 0)
+      ++expectedPos;
+    else if (sgn < 0)
+      ++expectedNeg;
+  }
+  double delta = ro->initial_delta;
+  if (delta <= 0.0) {
+    // solver.hpp:346-359: sqrt(eps) * max|A|
+    double maxAbs = 0.0;
+    if (c->nnz > 0) {
+      if (values_on_device) {
+        std::vector<double> hv(c->nnz);
+        cudaMemcpy(hv.data(), values, c->nnz * sizeof(double), cudaMemcpyDeviceToHost);
+        for (double v : hv) maxAbs = std::max(maxAbs, std::fabs(v));
+      } else {
+        for (int i = 0; i < c->nnz; ++i) maxAbs = std::max(maxAbs, std::fabs(values[i]));
+      }
+    }
+    if (maxAbs <= 0.0) maxAbs = 1.0;
+    delta = std::sqrt(std::numeric_limits<double>::epsilon()) * maxAbs;
+  }
+  symla_factor_opts fo;
+  symla_factor_opts_default(&fo);
+  fo.mode = SYMLA_MODE_STATIC;
+  fo.precision = ro->precision;
+  fo.static_rel_floor = ro->static_rel_floor;
+  fo.static_abs_floor = ro->static_abs_floor;
+  fo.expected_sign = signs.data();
+  const int maxAttempts = std::max(1, ro->max_retries + 1);
+  symla_regularize_info ri{};
+  symla_factor_info fi{};
+  for (int attempt = 0; attempt < maxAttempts; ++attempt) {
+    fo.static_delta = delta;
+    fo.front_delta = (attempt == 0) ? ro->front_delta : nullptr;
+    const int rc = symla_gpu_factorize(c, values, values_on_device, &fo, &fi);
+    if (rc != SYMLA_OK) return rc;
+    ri.retries_used = attempt;
+    ri.last_delta = delta;
+    const bool fullCoverage = (expectedPos + expectedNeg == n);
+    const bool ok = !haveExpectation || (fi.n_zero == 0 && !fi.singular &&
+                                         (!fullCoverage || (fi.n_pos == expectedPos && fi.n_neg == expectedNeg)));
+    if (ri.attempts < 32) {
+      ri.attempt_delta[ri.attempts] = delta;
+      ri.attempt_ok[ri.attempts] = ok ? 1 : 0;
+    }
+    ri.attempts++;
+    if (ok) {
+      if (info) *info = fi;
+      if (rinfo) *rinfo = ri;
+      return SYMLA_OK;
+    }
+    if (attempt + 1 >= maxAttempts) {
+      c->factorized = false;
+      if (info) *info = fi;
+      if (rinfo) *rinfo = ri;
+      char buf[640];
+      snprintf(buf, sizeof buf,
+               "symla::SymLDLT::factorize (Mode::StaticRegularized): inertia-controlled regularization retry budget "
+               "(%d retries) exhausted without matching the expected inertia. expected (n_pos=%d, n_neg=%d, "
+               "n_zero=0), got (n_pos=%d, n_neg=%d, n_zero=%d, singular=%s) at delta=%g. Refusing to report a "
+               "wrong-inertia factorization as successful.",
+               ro->max_retries, expectedPos, expectedNeg, fi.n_pos, fi.n_neg, fi.n_zero, fi.singular ? "true" : "false",
+               delta);
+      return set_error(SYMLA_ERR_RETRY_EXHAUSTED, buf);
+    }
+    delta *= ro->growth;
+  }
+  return SYMLA_OK;
+}
+
+extern "C" int symla_gpu_solve(symla_gpu_ctx* c, const double* B, int ldb, int nrhs, double* X, int ldx,
+                               int on_device) {
+  if (!c) return set_error(SYMLA_ERR_NOT_FACTORIZED, "symla::SymLDLT::solve: factorize() must be called before solve()");
+  return guarded([&] {
+    check_solvable(c);
+    if (nrhs < 0 || ldb < c->n || ldx < c->n)
+      throw SymlaError(SYMLA_ERR_BAD_SIZE, "symla::SymLDLT::solve: B.rows() must match the factorized matrix size");
+    if (nrhs == 0 || c->n == 0) return;
+    CK(cudaSetDevice(c->device));
+    const int n = c->n;
+    ensure_vectors(c, nrhs);
+    CK(cudaEventRecord(c->ev[5], c->stream));
+    if (on_device) {
+      device_solve(c, B, ldb, nrhs, X, ldx);
+    } else {
+      CK(cudaMemcpy2DAsync(c->d_B, n * sizeof(double), B, static_cast<size_t>(ldb) * sizeof(double),
+                           n * sizeof(double), nrhs, cudaMemcpyHostToDevice, c->stream));
+      device_solve(c, c->d_B, n, nrhs, c->d_X, n);
+      CK(cudaMemcpy2DAsync(X, static_cast<size_t>(ldx) * sizeof(double), c->d_X, n * sizeof(double),
+                           n * sizeof(double), nrhs, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaEventRecord(c->ev[6], c->stream));
+    CK(cudaEventSynchronize(c->ev[6]));
+    float a = 0, b = 0, t = 0;
+    cudaEventElapsedTime(&a, c->ev[2], c->ev[3]);
+    cudaEventElapsedTime(&b, c->ev[3], c->ev[4]);
+    cudaEventElapsedTime(&t, c->ev[5], c->ev[6]);
+    c->phase_ms[3] = a;
+    c->phase_ms[4] = b;
+    c->phase_ms[7] = t;
+  });
+}
+
+extern "C" int symla_gpu_solve_refine(symla_gpu_ctx* c, const double* values, const double* B, int ldb, int nrhs,
+                                      double* X, int ldx, int on_device, int max_iterations, double tolerance,
+                                      symla_refine_info* info) {
+  if (!c) return set_error(SYMLA_ERR_NOT_FACTORIZED, "symla::SymLDLT::solve: factorize() must be called before solve()");
+  return guarded([&] {
+    check_solvable(c);
+    if (nrhs < 0 || ldb < c->n || ldx < c->n)
+      throw SymlaError(SYMLA_ERR_BAD_SIZE, "symla::SymLDLT::solve: B.rows() must match the factorized matrix size");
+    CK(cudaSetDevice(c->device));
+    const int n = c->n;
+    symla_refine_info ri{};
+    if (nrhs == 0 || n == 0) {
+      if (info) *info = ri;
+      return;
+    }
+    cudaStream_t st = c->stream;
+    ensure_vectors(c, nrhs);
+    const long long len = static_cast<long long>(n) * nrhs;
+    // B -> d_B (compact n x nrhs), values -> d_values
+    if (on_device)
+      launch_copy2d(n, nrhs, B, ldb, c->d_B, n, st);
+    else
+      CK(cudaMemcpy2DAsync(c->d_B, n * sizeof(double), B, static_cast<size_t>(ldb) * sizeof(double),
+                           n * sizeof(double), nrhs, cudaMemcpyHostToDevice, st));
+    if (values) upload_values(c, values, on_device);
+    // refine.hpp:106-107
+    CK(cudaMemsetAsync(c->d_norms, 0, 8 * sizeof(double), st));
+    launch_rowsum_max(n, c->d_srowptr, c->d_svidx, c->d_values, c->d_norms + 0, st);
+    launch_absmax(c->d_B, len, c->d_norms + 1, st);
+    device_solve(c, c->d_B, n, nrhs, c->d_X, n);
+    auto residual_of = [&](const double* Xd, double* Rd, double* out2) {
+      CK(cudaMemsetAsync(c->d_norms + 2, 0, 2 * sizeof(double), st));
+      launch_residual(n, nrhs, c->d_rowptr, c->d_colind, c->d_vidx, c->d_values, Xd, n, c->d_B, n, Rd, st);
+      launch_absmax(Rd, len, c->d_norms + 2, st);
+      launch_absmax(Xd, len, c->d_norms + 3, st);
+      double h[4];
+      CK(cudaMemcpyAsync(h, c->d_norms, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      out2[0] = h[2];
+      out2[1] = h[3];
+      const double denom = h[0] * h[3] + h[1];
+      return denom > 0.0 ? h[2] / denom : h[2];
+    };
+    double nr[2];
+    double res = residual_of(c->d_X, c->d_R, nr);
+    ri.initial_relative_residual = res;
+    ri.final_relative_residual = res;
+    for (int it = 0; it < max_iterations; ++it) {
+      if (res <= tolerance) break;
+      device_solve(c, c->d_R, n, nrhs, c->d_dX, n);
+      CK(cudaMemcpyAsync(c->d_Xn, c->d_X, len * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      launch_axpy(len, c->d_dX, c->d_Xn, st);
+      const double resNew = residual_of(c->d_Xn, c->d_Rn, nr);
+      if (!(resNew < res)) break;
+      std::swap(c->d_X, c->d_Xn);
+      std::swap(c->d_R, c->d_Rn);
+      res = resNew;
+      ri.iterations = it + 1;
+      ri.final_relative_residual = res;
+    }
+    if (on_device)
+      launch_copy2d(n, nrhs, c->d_X, n, X, ldx, st);
+    else
+      CK(cudaMemcpy2DAsync(X, static_cast<size_t>(ldx) * sizeof(double), c->d_X, n * sizeof(double),
+                           n * sizeof(double), nrhs, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (info) *info = ri;
+  });
+}
+
+extern "C" int symla_gpu_singular_cols(symla_gpu_ctx* c, int* cols, int cap) {
+  if (!c) return 0;
+  const int k = static_cast<int>(c->singularCols.size());
+  for (int i = 0; i < k && i < cap; ++i) cols[i] = c->singularCols[i];
+  return k;
+}
+
+extern "C" int symla_gpu_num_fronts(symla_gpu_ctx* c) { return c ? c->numSN : 0; }
+
+extern "C" int symla_gpu_front_size(symla_gpu_ctx* c, int si, int* m, int* npiv) {
+  if (!c || si < 0 || si >= c->numSN) return set_error(SYMLA_ERR_INVALID, "front index out of range");
+  if (m) *m = c->hdesc[si].m;
+  if (npiv) *npiv = c->factorized ? c->hstate[si].npiv : 0;
+  return SYMLA_OK;
+}
+
+extern "C" int symla_gpu_front_get(symla_gpu_ctx* c, int si, int* row_indices, double* L, double* d_diag,
+                                   double* d_off, int* piv_start, int* piv_kind) {
+  if (!c || si < 0 || si >= c->numSN) return set_error(SYMLA_ERR_INVALID, "front index out of range");
+  int nblocks = 0;
+  const int rc = guarded([&] {
+    if (!c->factorized) throw SymlaError(SYMLA_ERR_NOT_FACTORIZED, "not factorized");
+    const FrontDesc& d = c->hdesc[si];
+    const int m = d.m, np = c->hstate[si].npiv;
+    if (row_indices) CK(cudaMemcpy(row_indices, d.fidx, m * sizeof(int), cudaMemcpyDeviceToHost));
+    if (L && np > 0) {
+      std::vector<double> F(static_cast<size_t>(d.ld) * np);
+      CK(cudaMemcpy(F.data(), d.F, F.size() * sizeof(double), cudaMemcpyDeviceToHost));
+      for (int j = 0; j < np; ++j)
+        for (int i = 0; i < m; ++i) L[i + static_cast<size_t>(j) * m] = (i >= j) ? F[i + static_cast<size_t>(j) * d.ld] : 0.0;
+    }
+    std::vector<int8_t> pk(np);
+    if (np > 0) CK(cudaMemcpy(pk.data(), d.pk, np, cudaMemcpyDeviceToHost));
+    if (d_diag && np > 0) CK(cudaMemcpy(d_diag, d.Dd, np * sizeof(double), cudaMemcpyDeviceToHost));
+    if (d_off && np > 0) CK(cudaMemcpy(d_off, d.Do, np * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < np; ++k) {
+      if (pk[k] == 2) continue;
+      if (piv_start) piv_start[nblocks] = k;
+      if (piv_kind) piv_kind[nblocks] = (pk[k] == 1) ? 1 : 0;
+      ++nblocks;
+    }
+  });
+  return rc == SYMLA_OK ? nblocks : -rc;
+}
+
+extern "C" void* symla_gpu_stream(symla_gpu_ctx* c) { return c ? c->stream : nullptr; }
+
+extern "C" int symla_gpu_phase_ms(symla_gpu_ctx* c, float* ms, int cap) {
+  if (!c) return 0;
+  for (int i = 0; i < cap && i < 8; ++i) ms[i] = c->phase_ms[i];
+  return 8;
+}
+
+extern "C" int symla_gpu_plan_stats(symla_gpu_ctx* c, double* out, int cap) {
+  if (!c) return 0;
+  double v[7] = {0};
+  v[0] = c->numSN;
+  v[1] = c->numLevels;
+  v[2] = c->plan_max_m;
+  v[3] = c->plan_sum_m2;
+  if (c->factorized) {
+    double flops = 0.0, nnzL = 0.0;
+    for (int s = 0; s < c->numSN; ++s) {
+      const FrontDesc& d = c->hdesc[s];
+      const int np = c->hstate[s].npiv, m = d.m;
+      std::vector<int8_t> pk(np);
+      if (np > 0) cudaMemcpy(pk.data(), d.pk, np, cudaMemcpyDeviceToHost);
+      for (int k = 0; k < np;) {
+        if (pk[k] == 1) {
+          const double r = m - k - 2;
+          flops += 3 * r + 2 * r * (r + 1);
+          k += 2;
+        } else {
+          const double r = m - k - 1;
+          flops += r + r * (r + 1);
+          k += 1;
+        }
+      }
+      nnzL += static_cast<double>(m) * np - static_cast<double>(np) * (np - 1) / 2.0;
+    }
+    v[4] = flops;
+    v[5] = nnzL;
+  }
+  v[6] = static_cast<double>(c->arena_doubles);
+  for (int i = 0; i < cap && i < 7; ++i) out[i] = v[i];
+  return 7;
+}

@@ -1,0 +1,79 @@
+// Shared device-side types for the B200 numeric factorize / solve path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace symla_gpu {
+
+// One frontal matrix (supernode) as the kernels see it. All pointers are
+// device pointers; a front's storage may live in the static arena or, after
+// delayed pivots re-planned it, in a per-level allocation.
+struct FrontDesc {
+  double* F;          // m x m column-major, leading dimension ld; lower triangle authoritative
+  int* fidx;          // m final-order row indices (permuted in place by pivoting swaps)
+  double* Dd;         // nelig: D diagonal
+  double* Do;         // nelig: D(k+1,k) of a 2x2 block starting at k, else 0
+  int8_t* pk;         // nelig: 0 = 1x1, 1 = first of 2x2, 2 = second of 2x2
+  double* W;          // solve workspace, m x nrhs (column stride wld)
+  int* lperm;         // m: pre-pivot local index now at each position (pivoting swaps)
+  int* lpos;          // m: inverse of lperm, written when the front is finished
+  int m, ld;
+  int ncols, nelig, nextra;
+  int parent;         // parent front or -1
+  int ch_begin, ch_end;  // children, into the ChildLink array
+  int a_begin, a_end;    // original-A entries of the own columns
+  int level;
+  int wld;            // leading dimension of W (>= m)
+};
+
+// Child -> parent extend-add maps.
+struct ChildLink {
+  int child;
+  const int* invmap;  // m_parent entries: parent local row -> child CB index, -1 if none
+  const int* relmap;  // cb_child entries: child CB index -> parent local row
+  int cb;             // contribution block size of the child
+};
+
+// Per-front results written by the factor kernels.
+struct FrontState {
+  int npiv;        // pivots finalized at this front
+  int flags;       // bit0 done, bit1 delayed to parent, bit2 leftover at a root (singular)
+  int n_pos, n_neg, n_zero;
+  int num_perturbed;
+  int k;           // next column (panel driver progress)
+  int panel_start; // first column of the panel in flight
+  double perturb;
+  double orig_max;
+  double running_max;
+  double delta;    // static pivoting delta used for this front
+};
+
+enum : int { kFlagDone = 1, kFlagDelayed = 2, kFlagSingularRoot = 4 };
+
+// Global counters for one factorization (device, zeroed per call).
+struct FactorGlobals {
+  int delay_level;     // lowest level that produced a delayed column, or INT_MAX
+  int error;           // nonzero: internal error code
+  int err_front;
+  int pad;
+};
+
+// Options visible to kernels.
+struct KernelOpts {
+  int mode;            // 0 threshold, 1 static
+  int precision;       // 0 fp64, 1 mixed
+  double zero_tol;
+  double rel_floor;
+  double static_delta;
+  double static_rel_floor;
+  double static_abs_floor;
+  const int* sign_final;        // n, expected sign in final order (static mode) or nullptr
+  const double* front_delta;    // per front delta override or nullptr
+  const double* values;         // A values (device), CSC order
+  const int* a_j;               // A entry: local column
+  const int* a_pos;             // A entry: rowPattern position
+  const int* a_idx;             // A entry: index into values
+};
+
+}  // namespace symla_gpu

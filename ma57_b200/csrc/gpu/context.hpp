@@ -1,0 +1,136 @@
+// Device context behind the C ABI (include/symla_gpu.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../host/symbolic.hpp"
+#include "common.cuh"
+
+struct symla_symbolic {
+  symla_host::SymbolicFactor sf;
+};
+
+namespace symla_gpu {
+
+// Host mirror of one front's current layout.
+struct HostFront {
+  int firstCol = 0, ncols = 0, nelig = 0, nextra = 0;
+  int m = 0, ld = 0;
+  int parent = -1, level = 0;
+  std::vector<int> children;
+  const std::vector<int>* rowPattern = nullptr;
+  bool replanned = false;
+};
+
+struct LevelLists {
+  std::vector<int> small;      // fronts with m <= kSmallFrontMax
+  int small_max_m = 0;
+  std::vector<int> large;      // other fronts
+  int large_max_m = 0;
+  int panels = 0;              // panel iterations needed
+  int trailing_grid = 0;
+  std::vector<int> tasks;      // assembly tasks (front, column block) for large fronts
+  std::vector<int> all;        // every front of the level (solve)
+  // device copies (static plan)
+  int* d_small = nullptr;
+  int* d_large = nullptr;
+  int* d_tasks = nullptr;
+  int* d_all = nullptr;
+};
+
+struct DeviceBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace symla_gpu
+
+struct symla_gpu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int n = 0;
+  int nnz = 0;
+  int numSN = 0;
+  int numLevels = 0;
+
+  std::vector<int> perm;  // final -> original
+  std::vector<int> newIndexOf;
+  std::vector<symla_gpu::HostFront> fronts;
+  std::vector<std::vector<int>> rowPatterns;  // owned copy of supernode patterns
+  std::vector<symla_gpu::LevelLists> levels;
+  std::vector<symla_gpu::FrontDesc> hdesc;
+  std::vector<symla_gpu::FrontDesc> hdesc_static;
+  std::vector<symla_gpu::ChildLink> hlinks;
+  std::vector<symla_gpu::ChildLink> hlinks_static;
+  std::vector<int> link_begin_static, link_end_static;
+
+  // device: static plan
+  double* d_arena = nullptr;
+  size_t arena_doubles = 0;
+  int* d_fidx = nullptr;       // per-front row index pool (static layout)
+  int* d_lperm = nullptr;      // per-front local pivot permutation pool
+  int* d_lpos = nullptr;       // and its inverse
+  std::vector<int> fidx_static;  // host copy of the static frontIdx pool
+  std::vector<long long> fidx_off;
+  double* d_Dd = nullptr;
+  double* d_Do = nullptr;
+  int8_t* d_pk = nullptr;
+  std::vector<long long> dpos;
+  int* d_maps = nullptr;       // invmap / relmap pool
+  symla_gpu::FrontDesc* d_desc = nullptr;
+  symla_gpu::ChildLink* d_links = nullptr;
+  size_t links_capacity = 0;
+  symla_gpu::FrontState* d_state = nullptr;
+  symla_gpu::FactorGlobals* d_glob = nullptr;
+  int* d_a_colptr = nullptr;
+  int* d_a_j = nullptr;
+  int* d_a_pos = nullptr;
+  int* d_a_idx = nullptr;
+  double* d_values = nullptr;
+  int* d_sign_final = nullptr;
+  double* d_front_delta = nullptr;
+  int* d_perm = nullptr;
+  // residual
+  int* d_rowptr = nullptr;
+  int* d_colind = nullptr;
+  int* d_vidx = nullptr;
+  int* d_srowptr = nullptr;
+  int* d_svidx = nullptr;
+  // solve workspace
+  double* d_W = nullptr;
+  int w_nrhs = 0;
+  bool w_dirty = true;
+  double* d_Bp = nullptr;
+  double* d_Z = nullptr;
+  double* d_Xf = nullptr;
+  double* d_B = nullptr;
+  double* d_X = nullptr;
+  double* d_R = nullptr;
+  double* d_dX = nullptr;
+  double* d_Xn = nullptr;
+  double* d_Rn = nullptr;
+  double* d_norms = nullptr;
+  int vec_nrhs = 0;
+  double* d_hostvals_tmp = nullptr;
+  int* d_scratch_int = nullptr;
+  size_t scratch_int_cap = 0;
+
+  // dynamic (delayed-pivot) allocations for the current factorization
+  std::vector<void*> dyn_allocs;
+
+  // state
+  bool factorized = false;
+  bool singular = false;
+  std::vector<int> singularCols;
+  std::vector<symla_gpu::FrontState> hstate;
+  symla_factor_info last_info{};
+  float phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  cudaEvent_t ev[8] = {};
+  double plan_sum_m2 = 0.0;
+  int plan_max_m = 0;
+  long long nnzL = 0;
+  int last_precision = 0;
+};

@@ -1,0 +1,898 @@
+// Numeric factorization kernels: front assembly (extend + extend-add), dense
+// partial LDL^T with threshold Bunch-Kaufman or static pivoting, and the
+// Schur-complement (trailing) update. sm_100a.
+//
+// Reference behaviour followed (include/symla/...):
+//   multifrontal.hpp:498-535  F = 0; extend (A entries of own columns);
+//                             extend-add of each child's generated element
+//   dense_kernel.hpp:576-793  pivot search and 1x1 / swap / 2x2 / delay
+//                             decisions, restricted to the eligible rows
+//   dense_kernel.hpp:919-1059 static pivoting with sign-matched perturbation
+//   dense_kernel.hpp:806-821  trailing update with the panel's L D L^T
+//
+// Fronts keep only their lower triangle (row >= column); the reference keeps
+// both triangles and re-averages them after every update
+// (dense_kernel.hpp:269-297), which is a no-op for a computation that forms
+// each symmetric entry once.
+#include <cfloat>
+#include <climits>
+#include <cmath>
+
+#include "common.cuh"
+#include "factor_kernels.h"
+#include "reduce.cuh"
+
+namespace symla_gpu {
+
+namespace {
+
+constexpr double kAlpha = 0.64038820320220756;  // (1 + sqrt(17)) / 8
+
+__device__ __forceinline__ bool level_aborted(const FactorGlobals* g, int level, int dynamic) {
+  return !dynamic && g->delay_level < level;
+}
+
+// Child contribution to parent entry (i, j) (i >= j in the parent's local
+// order), summed over children in their fixed order.
+__device__ __forceinline__ double gather_children(const FrontDesc* fronts, const ChildLink* links,
+                                                  const FrontState* st, int ch_begin, int ch_end, int i, int j) {
+  double v = 0.0;
+  for (int c = ch_begin; c < ch_end; ++c) {
+    const ChildLink L = links[c];
+    const int b = L.invmap[j];
+    if (b < 0) continue;
+    const int a = L.invmap[i];
+    if (a < 0) continue;
+    const FrontDesc& cf = fronts[L.child];
+    const int np = st[L.child].npiv;
+    const int r = a > b ? a : b, cc = a > b ? b : a;
+    v += cf.F[static_cast<int64_t>(np + cc) * cf.ld + np + r];
+  }
+  return v;
+}
+
+__device__ __forceinline__ int a_local_row(int pos, int ncols, int nextra) {
+  return pos < ncols ? pos : pos + nextra;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Assembly of large fronts in global memory: one CTA per (front, 32-column
+// block). Every parent entry is written exactly once (gather form), so no
+// separate zero fill and no atomics; then the A entries of the block's own
+// columns are added.
+__global__ void __launch_bounds__(256) assemble_kernel(const FrontDesc* __restrict__ fronts,
+                                                       const ChildLink* __restrict__ links,
+                                                       const FrontState* __restrict__ st, const int* __restrict__ tasks,
+                                                       const int* __restrict__ a_colptr, KernelOpts o,
+                                                       const FactorGlobals* __restrict__ g, int level, int dynamic) {
+  if (level_aborted(g, level, dynamic)) return;
+  const int s = tasks[2 * blockIdx.x];
+  const int j0 = tasks[2 * blockIdx.x + 1];
+  const FrontDesc f = fronts[s];
+  const int j1 = min(j0 + 32, f.m);
+  if (threadIdx.x < j1 - j0) f.lperm[j0 + threadIdx.x] = j0 + threadIdx.x;
+  for (int j = j0; j < j1; ++j) {
+    double* col = f.F + static_cast<int64_t>(j) * f.ld;
+    for (int i = j + threadIdx.x; i < f.m; i += blockDim.x)
+      col[i] = gather_children(fronts, links, st, f.ch_begin, f.ch_end, i, j);
+  }
+  __syncthreads();
+  if (j0 < f.ncols) {
+    const int jend = min(j1, f.ncols);
+    const int e0 = a_colptr[f.a_begin + j0], e1 = a_colptr[f.a_begin + jend];
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+      const int j = o.a_j[e];
+      const int i = a_local_row(o.a_pos[e], f.ncols, f.nextra);
+      f.F[static_cast<int64_t>(j) * f.ld + i] += o.values[o.a_idx[e]];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Small fronts: one CTA per front, the whole front in shared memory
+// (assembly, factorization and write-back in one launch).
+namespace {
+
+template <int NT>
+struct SmallFront {
+  double* S;
+  int lds;
+  int m;
+  __device__ double& at(int i, int j) { return S[j * lds + i]; }
+  // symmetric read from lower storage
+  __device__ double sym(int i, int j) { return i >= j ? S[j * lds + i] : S[i * lds + j]; }
+};
+
+// Symmetric swap of positions i < j in lower storage over the whole front.
+template <int NT>
+__device__ void smem_swap(SmallFront<NT>& F, int* fi, int* lp, int i, int j) {
+  const int m = F.m;
+  for (int t = threadIdx.x; t < m - 1; t += NT) {
+    if (t < i) {  // row swap in columns c < i
+      const int c = t;
+      double a = F.at(i, c);
+      F.at(i, c) = F.at(j, c);
+      F.at(j, c) = a;
+    } else if (t < j - 1) {  // c in (i, j): (c, i) <-> (j, c)
+      const int c = t + 1;
+      double a = F.at(c, i);
+      F.at(c, i) = F.at(j, c);
+      F.at(j, c) = a;
+    } else if (t == j - 1) {  // diagonal
+      double a = F.at(i, i);
+      F.at(i, i) = F.at(j, j);
+      F.at(j, j) = a;
+    } else {  // rows r > j
+      const int r = t + 1;
+      double a = F.at(r, i);
+      F.at(r, i) = F.at(r, j);
+      F.at(r, j) = a;
+    }
+  }
+  if (threadIdx.x == 0) {
+    int a = fi[i];
+    fi[i] = fi[j];
+    fi[j] = a;
+    a = lp[i];
+    lp[i] = lp[j];
+    lp[j] = a;
+  }
+  __syncthreads();
+}
+
+}  // namespace
+
+template <int NT>
+__global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __restrict__ fronts,
+                                                          const ChildLink* __restrict__ links, FrontState* st,
+                                                          const int* __restrict__ front_list,
+                                                          const int* __restrict__ a_colptr, KernelOpts o,
+                                                          FactorGlobals* g, int level, int dynamic) {
+  if (level_aborted(g, level, dynamic)) return;
+  extern __shared__ double smem[];
+  __shared__ double red_v[NT / 32];
+  __shared__ int red_i[NT / 32];
+  __shared__ int s_np;
+
+  const int s = front_list[blockIdx.x];
+  const FrontDesc f = fronts[s];
+  const int m = f.m;
+  SmallFront<NT> F{smem, m | 1, m};
+  int* fi = reinterpret_cast<int*>(smem + static_cast<size_t>(F.lds) * m);
+  int* lp = fi + m;  // local pivot permutation
+
+  // ---- assembly (multifrontal.hpp:498-535), children summed in fixed order
+  for (int t = threadIdx.x; t < m * m; t += NT) {
+    const int i = t % m, j = t / m;
+    if (i < j) continue;
+    F.at(i, j) = gather_children(fronts, links, st, f.ch_begin, f.ch_end, i, j);
+  }
+  for (int t = threadIdx.x; t < m; t += NT) {
+    fi[t] = f.fidx[t];
+    lp[t] = t;
+  }
+  __syncthreads();
+  {
+    const int e0 = a_colptr[f.a_begin], e1 = a_colptr[f.a_begin + f.ncols];
+    for (int e = e0 + threadIdx.x; e < e1; e += NT) {
+      const int j = o.a_j[e];
+      const int i = a_local_row(o.a_pos[e], f.ncols, f.nextra);
+      F.at(i, j) += o.values[o.a_idx[e]];
+    }
+  }
+  __syncthreads();
+
+  // ---- orig_max over the whole front (dense_kernel.hpp:413, :934)
+  double tmax = 0.0;
+  for (int t = threadIdx.x; t < m * m; t += NT) {
+    const int i = t % m, j = t / m;
+    if (i >= j) tmax = fmax(tmax, fabs(F.at(i, j)));
+  }
+  double orig_max = block_max<NT>(tmax, red_v);
+  const bool isStatic = (o.mode == 1);
+  if (isStatic) {
+    if (orig_max < o.static_abs_floor) orig_max = 1.0;
+  } else {
+    if (orig_max < o.zero_tol) orig_max = 1.0;
+  }
+  double thread_rmax = 0.0;  // cumulative max of values this thread wrote
+
+  const int effEnd = f.nelig;
+  int n_pos = 0, n_neg = 0, n_zero = 0, nPert = 0;
+  double pert = 0.0;
+  double delta = 0.0;
+  int k = 0;
+
+  if (isStatic) {
+    // dense_kernel.hpp:919-1059, unblocked (panel_size 1 for small fronts)
+    delta = o.front_delta ? o.front_delta[s] : (o.static_delta > 0.0 ? o.static_delta : 1.4901161193847656e-08 * orig_max);
+    const double floorv = fmax(o.static_abs_floor, o.static_rel_floor * orig_max);
+    for (k = 0; k < effEnd; ++k) {
+      const double akk = F.at(k, k);
+      const int sign = o.sign_final ? o.sign_final[fi[k]] : 0;
+      bool need;
+      if (sign > 0)
+        need = akk < floorv;
+      else if (sign < 0)
+        need = akk > -floorv;
+      else
+        need = fabs(akk) < floorv;
+      double d = akk;
+      if (need) {
+        const double sg = (sign != 0) ? static_cast<double>(sign) : (akk >= 0.0 ? 1.0 : -1.0);
+        d = akk + sg * delta;
+        const double applied = d - akk;
+        if (applied != 0.0) {
+          pert += fabs(applied);
+          ++nPert;
+        }
+      }
+      if (d > 0)
+        ++n_pos;
+      else if (d < 0)
+        ++n_neg;
+      else
+        ++n_zero;
+      __syncthreads();
+      if (threadIdx.x == 0) F.at(k, k) = d;
+      thread_rmax = fmax(thread_rmax, fabs(d));
+      for (int i = k + 1 + threadIdx.x; i < m; i += NT) {
+        const double a = F.at(i, k);
+        thread_rmax = fmax(thread_rmax, fabs(a));
+        F.at(i, k) = a / d;
+      }
+      __syncthreads();
+      const int mt = m - k - 1;
+      for (int t = threadIdx.x; t < mt * mt; t += NT) {
+        const int ii = t % mt, jj = t / mt;
+        if (ii < jj) continue;
+        const int i = k + 1 + ii, j = k + 1 + jj;
+        const double v = F.at(i, j) - (F.at(i, k) * d) * F.at(j, k);
+        F.at(i, j) = v;
+        thread_rmax = fmax(thread_rmax, fabs(v));
+      }
+      __syncthreads();
+    }
+    for (int t = threadIdx.x; t < effEnd; t += NT) {
+        f.Dd[t] = F.at(t, t);
+        f.Do[t] = 0.0;
+        f.pk[t] = 0;
+      }
+  } else {
+    // dense_kernel.hpp:576-793, unblocked
+    while (k < effEnd) {
+      ArgMax am{0.0, -1};
+      for (int i = k + 1 + threadIdx.x; i < effEnd; i += NT) {
+        const double v = fabs(F.at(i, k));
+        am = argmax_combine(am, ArgMax{v, i});
+      }
+      am = block_argmax<NT>(am, red_v, red_i);
+      const double lambda = am.v;
+      const int r = am.i;
+      const double akk = F.at(k, k);
+      int dec;  // 0: 1x1 at k, 1: swap k<->r then 1x1, 2: 2x2 (k, r), 3: stop
+      if (lambda <= o.zero_tol) {
+        const double isolatedFloor = fmax(o.zero_tol, o.rel_floor * orig_max);
+        dec = (fabs(akk) <= isolatedFloor) ? 3 : 0;
+      } else if (fabs(akk) >= kAlpha * lambda) {
+        dec = 0;
+      } else {
+        double sm = 0.0;
+        for (int i = k + threadIdx.x; i < effEnd; i += NT)
+          if (i != r) sm = fmax(sm, fabs(F.sym(i, r)));
+        const double sigma = block_max<NT>(sm, red_v);
+        if (fabs(akk) * sigma >= kAlpha * lambda * lambda)
+          dec = 0;
+        else if (fabs(F.at(r, r)) >= kAlpha * sigma)
+          dec = 1;
+        else
+          dec = 2;
+      }
+      if (dec == 3) break;
+      __syncthreads();
+      if (dec == 1) smem_swap<NT>(F, fi, lp, k, r);
+      if (dec == 0 || dec == 1) {
+        const double d = F.at(k, k);
+        if (d > 0)
+          ++n_pos;
+        else if (d < 0)
+          ++n_neg;
+        else
+          ++n_zero;
+        thread_rmax = fmax(thread_rmax, fabs(d));
+        for (int i = k + 1 + threadIdx.x; i < m; i += NT) {
+          const double a = F.at(i, k);
+          thread_rmax = fmax(thread_rmax, fabs(a));
+          F.at(i, k) = a / d;
+        }
+        if (threadIdx.x == 0) {
+          f.Dd[k] = d;
+          f.Do[k] = 0.0;
+          f.pk[k] = 0;
+        }
+        __syncthreads();
+        const int mt = m - k - 1;
+        for (int t = threadIdx.x; t < mt * mt; t += NT) {
+          const int ii = t % mt, jj = t / mt;
+          if (ii < jj) continue;
+          const int i = k + 1 + ii, j = k + 1 + jj;
+          const double v = F.at(i, j) - (F.at(i, k) * d) * F.at(j, k);
+          F.at(i, j) = v;
+          thread_rmax = fmax(thread_rmax, fabs(v));
+        }
+        __syncthreads();
+        k += 1;
+        continue;
+      }
+      // 2x2 pivot
+      if (r != k + 1) smem_swap<NT>(F, fi, lp, k + 1, r);
+      const double d11 = F.at(k, k), d21 = F.at(k + 1, k), d22 = F.at(k + 1, k + 1);
+      const double det = d11 * d22 - d21 * d21;
+      const double rm = fmax(orig_max, block_max<NT>(thread_rmax, red_v));
+      const double rm1 = fmax(1.0, rm);
+      if (fabs(det) <= o.zero_tol * rm1 * rm1) break;
+      thread_rmax = fmax(thread_rmax, fmax(fabs(d11), fmax(fabs(d21), fabs(d22))));
+      if (det < 0) {
+        ++n_pos;
+        ++n_neg;
+      } else {
+        const double tr = d11 + d22;
+        if (tr > 0)
+          n_pos += 2;
+        else if (tr < 0)
+          n_neg += 2;
+        else {
+          ++n_pos;
+          ++n_neg;
+        }
+      }
+      const double inv11 = d22 / det, inv21 = -d21 / det, inv22 = d11 / det;
+      for (int i = k + 2 + threadIdx.x; i < m; i += NT) {
+        const double a0 = F.at(i, k), a1 = F.at(i, k + 1);
+        thread_rmax = fmax(thread_rmax, fmax(fabs(a0), fabs(a1)));
+        F.at(i, k) = a0 * inv11 + a1 * inv21;
+        F.at(i, k + 1) = a0 * inv21 + a1 * inv22;
+      }
+      if (threadIdx.x == 0) {
+        f.Dd[k] = d11;
+        f.Dd[k + 1] = d22;
+        f.Do[k] = d21;
+        f.Do[k + 1] = 0.0;
+        f.pk[k] = 1;
+        f.pk[k + 1] = 2;
+      }
+      __syncthreads();
+      const int mt = m - k - 2;
+      for (int t = threadIdx.x; t < mt * mt; t += NT) {
+        const int ii = t % mt, jj = t / mt;
+        if (ii < jj) continue;
+        const int i = k + 2 + ii, j = k + 2 + jj;
+        const double l0i = F.at(i, k), l1i = F.at(i, k + 1);
+        const double w0 = l0i * d11 + l1i * d21;
+        const double w1 = l0i * d21 + l1i * d22;
+        const double v = F.at(i, j) - (w0 * F.at(j, k) + w1 * F.at(j, k + 1));
+        F.at(i, j) = v;
+        thread_rmax = fmax(thread_rmax, fabs(v));
+      }
+      __syncthreads();
+      k += 2;
+    }
+  }
+
+  // ---- write back (lower triangle of the whole front, permuted indices)
+  __syncthreads();
+  for (int t = threadIdx.x; t < m * m; t += NT) {
+    const int i = t % m, j = t / m;
+    if (i >= j) f.F[static_cast<int64_t>(j) * f.ld + i] = F.at(i, j);
+  }
+  for (int t = threadIdx.x; t < m; t += NT) {
+    f.fidx[t] = fi[t];
+    f.lpos[lp[t]] = t;
+  }
+  const double rmax = block_max<NT>(thread_rmax, red_v);
+  if (threadIdx.x == 0) s_np = k;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    FrontState& S = st[s];
+    S.npiv = k;
+    S.n_pos = n_pos;
+    S.n_neg = n_neg;
+    S.n_zero = n_zero;
+    S.num_perturbed = nPert;
+    S.perturb = pert;
+    S.orig_max = orig_max;
+    S.running_max = fmax(orig_max, rmax);
+    S.delta = delta;
+    S.k = k;
+    int flags = kFlagDone;
+    if (k < effEnd) {
+      if (f.parent >= 0) {
+        flags |= kFlagDelayed;
+        atomicMin(&g->delay_level, f.level);
+      } else {
+        flags |= kFlagSingularRoot;
+      }
+    } else if (k < m && f.parent < 0) {
+      flags |= kFlagSingularRoot;
+    }
+    S.flags = flags;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Large fronts: panel of up to NB pivots by one CTA, lazily bringing the
+// candidate columns up to date from the front (which holds the panel-start
+// state for every non-pivoted column) and the panel's L and D
+// (dense_kernel.hpp:516-559). The trailing update follows in
+// trailing_update_kernel.
+namespace {
+
+constexpr int kPanelThreads = 512;
+
+// Compute current column `col` over rows [k, m) into vec:
+// vec[i] = raw(i, col) - sum_q L(i, ps+q) * (D L(col, ps+:))_q
+__device__ void panel_current_column(const FrontDesc& f, int ps, int p, int k, int col, double* vec, double* wbuf) {
+  // w = D * L(col, ps:ps+p)^T (block diagonal D, 2x2 aware)
+  if (threadIdx.x < p) {
+    const int q = threadIdx.x;
+    const int pq = ps + q;
+    const int8_t kind = f.pk[pq];
+    const double lq = f.F[static_cast<int64_t>(pq) * f.ld + col];
+    double w;
+    if (kind == 0) {
+      w = f.Dd[pq] * lq;
+    } else if (kind == 1) {
+      const double l1 = f.F[static_cast<int64_t>(pq + 1) * f.ld + col];
+      w = f.Dd[pq] * lq + f.Do[pq] * l1;
+    } else {
+      const double l0 = f.F[static_cast<int64_t>(pq - 1) * f.ld + col];
+      w = f.Do[pq - 1] * l0 + f.Dd[pq] * lq;
+    }
+    wbuf[q] = w;
+  }
+  __syncthreads();
+  for (int i = k + threadIdx.x; i < f.m; i += blockDim.x) {
+    double raw = (i >= col) ? f.F[static_cast<int64_t>(col) * f.ld + i] : f.F[static_cast<int64_t>(i) * f.ld + col];
+    double corr = 0.0;
+    for (int q = 0; q < p; ++q) corr += f.F[static_cast<int64_t>(ps + q) * f.ld + i] * wbuf[q];
+    vec[i] = raw - corr;
+  }
+  __syncthreads();
+}
+
+// Symmetric swap of positions i < j in lower storage over the whole front
+// (global memory).
+__device__ void global_swap(const FrontDesc& f, int i, int j) {
+  const int m = f.m;
+  double* F = f.F;
+  const int64_t ld = f.ld;
+  for (int t = threadIdx.x; t < m - 1; t += blockDim.x) {
+    if (t < i) {
+      const int c = t;
+      double a = F[c * ld + i];
+      F[c * ld + i] = F[c * ld + j];
+      F[c * ld + j] = a;
+    } else if (t < j - 1) {
+      const int c = t + 1;
+      double a = F[i * ld + c];
+      F[i * ld + c] = F[c * ld + j];
+      F[c * ld + j] = a;
+    } else if (t == j - 1) {
+      double a = F[i * ld + i];
+      F[i * ld + i] = F[j * ld + j];
+      F[j * ld + j] = a;
+    } else {
+      const int r = t + 1;
+      double a = F[i * ld + r];
+      F[i * ld + r] = F[j * ld + r];
+      F[j * ld + r] = a;
+    }
+  }
+  if (threadIdx.x == 0) {
+    int a = f.fidx[i];
+    f.fidx[i] = f.fidx[j];
+    f.fidx[j] = a;
+    a = f.lperm[i];
+    f.lperm[i] = f.lperm[j];
+    f.lperm[j] = a;
+  }
+  __syncthreads();
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
+                                                              const int* __restrict__ front_list, int nb, KernelOpts o,
+                                                              FactorGlobals* g, int level, int dynamic) {
+  if (level_aborted(g, level, dynamic)) return;
+  constexpr int NT = kPanelThreads;
+  extern __shared__ double smem[];
+  __shared__ double red_v[NT / 32];
+  __shared__ int red_i[NT / 32];
+  __shared__ double wbuf[72];
+
+  const int s = front_list[blockIdx.x];
+  const FrontDesc f = fronts[s];
+  FrontState S = st[s];
+  if (S.flags & kFlagDone) {
+    // no panel this round: the trailing update that follows must do nothing
+    if (threadIdx.x == 0) st[s].panel_start = S.k;
+    return;
+  }
+  const int m = f.m;
+  const int effEnd = f.nelig;
+  double* colk = smem;
+  double* colr = smem + m;
+
+  // First panel: orig_max over the assembled front.
+  if (S.k == 0) {
+    double tmax = 0.0;
+    for (int j = 0; j < m; ++j)
+      for (int i = j + threadIdx.x; i < m; i += NT) tmax = fmax(tmax, fabs(f.F[static_cast<int64_t>(j) * f.ld + i]));
+    double om = block_max<NT>(tmax, red_v);
+    if (o.mode == 1) {
+      if (om < o.static_abs_floor) om = 1.0;
+    } else {
+      if (om < o.zero_tol) om = 1.0;
+    }
+    S.orig_max = om;
+    S.running_max = om;
+    S.n_pos = S.n_neg = S.n_zero = 0;
+    S.num_perturbed = 0;
+    S.perturb = 0.0;
+    S.delta = o.front_delta ? o.front_delta[s] : (o.static_delta > 0.0 ? o.static_delta : 1.4901161193847656e-08 * om);
+  }
+  const double orig_max = S.orig_max;
+  int k = S.k;
+  const int ps = k;
+  const int pe = ps + min(nb, effEnd - ps);
+  double thread_rmax = 0.0;
+  bool stopped = false;
+  int n_pos = S.n_pos, n_neg = S.n_neg, n_zero = S.n_zero, nPert = S.num_perturbed;
+  double pert = S.perturb;
+
+  while (k < pe) {
+    const int p = k - ps;
+    panel_current_column(f, ps, p, k, k, colk, wbuf);
+    if (o.mode == 1) {
+      const double akk = colk[k];
+      const int sign = o.sign_final ? o.sign_final[f.fidx[k]] : 0;
+      const double floorv = fmax(o.static_abs_floor, o.static_rel_floor * orig_max);
+      bool need;
+      if (sign > 0)
+        need = akk < floorv;
+      else if (sign < 0)
+        need = akk > -floorv;
+      else
+        need = fabs(akk) < floorv;
+      double d = akk;
+      if (need) {
+        const double sg = (sign != 0) ? static_cast<double>(sign) : (akk >= 0.0 ? 1.0 : -1.0);
+        d = akk + sg * S.delta;
+        const double applied = d - akk;
+        if (applied != 0.0) {
+          pert += fabs(applied);
+          ++nPert;
+        }
+      }
+      if (d > 0)
+        ++n_pos;
+      else if (d < 0)
+        ++n_neg;
+      else
+        ++n_zero;
+      thread_rmax = fmax(thread_rmax, fabs(d));
+      for (int i = k + 1 + threadIdx.x; i < m; i += NT) {
+        const double a = colk[i];
+        thread_rmax = fmax(thread_rmax, fabs(a));
+        f.F[static_cast<int64_t>(k) * f.ld + i] = a / d;
+      }
+      if (threadIdx.x == 0) {
+        f.F[static_cast<int64_t>(k) * f.ld + k] = d;
+        f.Dd[k] = d;
+        f.Do[k] = 0.0;
+        f.pk[k] = 0;
+      }
+      __syncthreads();
+      ++k;
+      continue;
+    }
+    ArgMax am{0.0, -1};
+    for (int i = k + 1 + threadIdx.x; i < effEnd; i += NT) am = argmax_combine(am, ArgMax{fabs(colk[i]), i});
+    am = block_argmax<NT>(am, red_v, red_i);
+    const double lambda = am.v;
+    const int r = am.i;
+    const double akk = colk[k];
+    int dec;
+    if (lambda <= o.zero_tol) {
+      const double isolatedFloor = fmax(o.zero_tol, o.rel_floor * orig_max);
+      dec = (fabs(akk) <= isolatedFloor) ? 3 : 0;
+    } else if (fabs(akk) >= kAlpha * lambda) {
+      dec = 0;
+    } else {
+      panel_current_column(f, ps, p, k, r, colr, wbuf);
+      double sm = 0.0;
+      for (int i = k + threadIdx.x; i < effEnd; i += NT)
+        if (i != r) sm = fmax(sm, fabs(colr[i]));
+      const double sigma = block_max<NT>(sm, red_v);
+      if (fabs(akk) * sigma >= kAlpha * lambda * lambda)
+        dec = 0;
+      else if (fabs(colr[r]) >= kAlpha * sigma)
+        dec = 1;
+      else
+        dec = 2;
+    }
+    if (dec == 3) {
+      stopped = true;
+      break;
+    }
+    __syncthreads();
+    if (dec == 0 || dec == 1) {
+      double* col = colk;
+      if (dec == 1) {
+        global_swap(f, k, r);
+        // new column k = old column r with rows k and r exchanged
+        if (threadIdx.x == 0) {
+          const double a = colr[k];
+          colr[k] = colr[r];
+          colr[r] = a;
+        }
+        __syncthreads();
+        col = colr;
+      }
+      const double d = col[k];
+      if (d > 0)
+        ++n_pos;
+      else if (d < 0)
+        ++n_neg;
+      else
+        ++n_zero;
+      thread_rmax = fmax(thread_rmax, fabs(d));
+      for (int i = k + 1 + threadIdx.x; i < m; i += NT) {
+        const double a = col[i];
+        thread_rmax = fmax(thread_rmax, fabs(a));
+        f.F[static_cast<int64_t>(k) * f.ld + i] = a / d;
+      }
+      if (threadIdx.x == 0) {
+        f.F[static_cast<int64_t>(k) * f.ld + k] = d;
+        f.Dd[k] = d;
+        f.Do[k] = 0.0;
+        f.pk[k] = 0;
+      }
+      __syncthreads();
+      k += 1;
+      continue;
+    }
+    // 2x2: bring r to k+1
+    if (r != k + 1) {
+      global_swap(f, k + 1, r);
+      if (threadIdx.x == 0) {
+        double a = colk[k + 1];
+        colk[k + 1] = colk[r];
+        colk[r] = a;
+        a = colr[k + 1];
+        colr[k + 1] = colr[r];
+        colr[r] = a;
+      }
+      __syncthreads();
+    }
+    const double d11 = colk[k], d21 = colk[k + 1], d22 = colr[k + 1];
+    const double det = d11 * d22 - d21 * d21;
+    const double rm = fmax(S.running_max, block_max<NT>(thread_rmax, red_v));
+    const double rm1 = fmax(1.0, rm);
+    if (fabs(det) <= o.zero_tol * rm1 * rm1) {
+      stopped = true;
+      break;
+    }
+    thread_rmax = fmax(thread_rmax, fmax(fabs(d11), fmax(fabs(d21), fabs(d22))));
+    if (det < 0) {
+      ++n_pos;
+      ++n_neg;
+    } else {
+      const double tr = d11 + d22;
+      if (tr > 0)
+        n_pos += 2;
+      else if (tr < 0)
+        n_neg += 2;
+      else {
+        ++n_pos;
+        ++n_neg;
+      }
+    }
+    const double inv11 = d22 / det, inv21 = -d21 / det, inv22 = d11 / det;
+    for (int i = k + 2 + threadIdx.x; i < m; i += NT) {
+      const double a0 = colk[i], a1 = colr[i];
+      thread_rmax = fmax(thread_rmax, fmax(fabs(a0), fabs(a1)));
+      f.F[static_cast<int64_t>(k) * f.ld + i] = a0 * inv11 + a1 * inv21;
+      f.F[static_cast<int64_t>(k + 1) * f.ld + i] = a0 * inv21 + a1 * inv22;
+    }
+    if (threadIdx.x == 0) {
+      f.F[static_cast<int64_t>(k) * f.ld + k] = d11;
+      f.F[static_cast<int64_t>(k) * f.ld + k + 1] = d21;
+      f.F[static_cast<int64_t>(k + 1) * f.ld + k + 1] = d22;
+      f.Dd[k] = d11;
+      f.Dd[k + 1] = d22;
+      f.Do[k] = d21;
+      f.Do[k + 1] = 0.0;
+      f.pk[k] = 1;
+      f.pk[k + 1] = 2;
+    }
+    __syncthreads();
+    k += 2;
+  }
+
+  const double rmax = block_max<NT>(thread_rmax, red_v);
+  if (stopped || k >= effEnd)
+    for (int t = threadIdx.x; t < m; t += NT) f.lpos[f.lperm[t]] = t;
+  if (threadIdx.x == 0) {
+    FrontState& W = st[s];
+    W.orig_max = orig_max;
+    W.delta = S.delta;
+    W.running_max = fmax(S.running_max, rmax);
+    W.n_pos = n_pos;
+    W.n_neg = n_neg;
+    W.n_zero = n_zero;
+    W.num_perturbed = nPert;
+    W.perturb = pert;
+    W.panel_start = ps;
+    W.k = k;
+    W.npiv = k;
+    int flags = 0;
+    if (stopped || k >= effEnd) {
+      flags |= kFlagDone;
+      if (k < effEnd) {
+        if (f.parent >= 0) {
+          flags |= kFlagDelayed;
+          atomicMin(&g->delay_level, f.level);
+        } else {
+          flags |= kFlagSingularRoot;
+        }
+      } else if (k < m && f.parent < 0) {
+        flags |= kFlagSingularRoot;
+      }
+    }
+    W.flags = flags;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Trailing update T(k1:m, k1:m) -= L(k1:m, ps:k1) * (L D)(k1:m, ps:k1)^T on
+// the lower triangle, FP64, 64x64 tiles, K = panel width (<= NB+1).
+namespace {
+constexpr int kTT = 64;        // tile edge
+constexpr int kTThreads = 256;  // 16 x 16 threads, 4 x 4 outputs each
+constexpr int kKMax = 40;  // panel width + 1 (2x2 straddle) <= 40
+}  // namespace
+
+__global__ void __launch_bounds__(kTThreads) trailing_update_kernel(const FrontDesc* __restrict__ fronts,
+                                                                    FrontState* st,
+                                                                    const int* __restrict__ front_list,
+                                                                    const FactorGlobals* __restrict__ g, int level,
+                                                                    int dynamic) {
+  if (level_aborted(g, level, dynamic)) return;
+  __shared__ double Li[kKMax][kTT + 1];
+  __shared__ double Wj[kKMax][kTT + 1];
+  const int s = front_list[blockIdx.y];
+  const FrontDesc f = fronts[s];
+  const FrontState S = st[s];
+  const int ps = S.panel_start, k1 = S.k;
+  const int p = k1 - ps;
+  if (p <= 0) return;
+  const int mt = f.m - k1;
+  if (mt <= 0) return;
+  const int nt = (mt + kTT - 1) / kTT;
+  const int ntiles = nt * (nt + 1) / 2;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double tmax = 0.0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    // tile -> (ti, tj), ti >= tj, column-major over the lower triangle
+    int tj = 0, rem = tile;
+    while (rem >= nt - tj) {
+      rem -= nt - tj;
+      ++tj;
+    }
+    const int ti = tj + rem;
+    const int i0 = k1 + ti * kTT, j0 = k1 + tj * kTT;
+    __syncthreads();
+    for (int t = threadIdx.x; t < p * kTT; t += kTThreads) {
+      const int q = t / kTT, r = t % kTT;
+      const int pq = ps + q;
+      const int gi = i0 + r, gj = j0 + r;
+      Li[q][r] = (gi < f.m) ? f.F[static_cast<int64_t>(pq) * f.ld + gi] : 0.0;
+      double w = 0.0;
+      if (gj < f.m) {
+        const int8_t kind = f.pk[pq];
+        const double lq = f.F[static_cast<int64_t>(pq) * f.ld + gj];
+        if (kind == 0)
+          w = f.Dd[pq] * lq;
+        else if (kind == 1)
+          w = f.Dd[pq] * lq + f.Do[pq] * f.F[static_cast<int64_t>(pq + 1) * f.ld + gj];
+        else
+          w = f.Do[pq - 1] * f.F[static_cast<int64_t>(pq - 1) * f.ld + gj] + f.Dd[pq] * lq;
+      }
+      Wj[q][r] = w;
+    }
+    __syncthreads();
+    double acc[4][4] = {};
+    for (int q = 0; q < p; ++q) {
+      double a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        a[u] = Li[q][ty + 16 * u];
+        b[u] = Wj[q][tx + 16 * u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int gi = i0 + ty + 16 * u, gj = j0 + tx + 16 * v;
+        if (gi < f.m && gj < f.m && gi >= gj) {
+          double* c = f.F + static_cast<int64_t>(gj) * f.ld + gi;
+          const double nv = *c - acc[u][v];
+          *c = nv;
+          tmax = fmax(tmax, fabs(nv));
+        }
+      }
+  }
+  tmax = warp_max(tmax);
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&st[s].running_max, tmax);
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+
+void launch_assemble(const FrontDesc* fronts, const ChildLink* links, const FrontState* st, const int* tasks,
+                     int ntasks, const int* a_colptr, const KernelOpts& o, const FactorGlobals* g, int level,
+                     int dynamic, cudaStream_t stream) {
+  if (ntasks <= 0) return;
+  assemble_kernel<<<ntasks, 256, 0, stream>>>(fronts, links, st, tasks, a_colptr, o, g, level, dynamic);
+}
+
+size_t small_front_smem(int m) {
+  return static_cast<size_t>(m | 1) * m * sizeof(double) + 2 * static_cast<size_t>(m) * sizeof(int) + 16;
+}
+
+void launch_factor_small(const FrontDesc* fronts, const ChildLink* links, FrontState* st, const int* list, int count,
+                         int max_m, const int* a_colptr, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
+                         cudaStream_t stream) {
+  if (count <= 0) return;
+  const size_t sm = small_front_smem(max_m);
+  if (max_m <= 48) {
+    factor_small_kernel<128><<<count, 128, sm, stream>>>(fronts, links, st, list, a_colptr, o, g, level, dynamic);
+  } else {
+    factor_small_kernel<256><<<count, 256, sm, stream>>>(fronts, links, st, list, a_colptr, o, g, level, dynamic);
+  }
+}
+
+void launch_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m, int nb,
+                  const KernelOpts& o, FactorGlobals* g, int level, int dynamic, cudaStream_t stream) {
+  if (count <= 0) return;
+  const size_t sm = 2 * static_cast<size_t>(max_m) * sizeof(double);
+  panel_kernel<<<count, kPanelThreads, sm, stream>>>(fronts, st, list, nb, o, g, level, dynamic);
+}
+
+void launch_trailing(const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
+                     const FactorGlobals* g, int level, int dynamic, cudaStream_t stream) {
+  if (count <= 0 || grid_x <= 0) return;
+  dim3 grid(grid_x, count);
+  trailing_update_kernel<<<grid, kTThreads, 0, stream>>>(fronts, st, list, g, level, dynamic);
+}
+
+cudaError_t configure_factor_kernels() {
+  cudaError_t e;
+  e = cudaFuncSetAttribute(factor_small_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(factor_small_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  return e;
+}
+
+}  // namespace symla_gpu

@@ -1,0 +1,50 @@
+// Host launchers for the factorization and solve kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace symla_gpu {
+
+// Fronts whose m is at most this go through the one-CTA shared-memory kernel.
+constexpr int kSmallFrontMax = 128;
+// Panel width of the large-front path.
+constexpr int kPanelWidth = 32;
+
+cudaError_t configure_factor_kernels();
+size_t small_front_smem(int m);
+
+void launch_assemble(const FrontDesc* fronts, const ChildLink* links, const FrontState* st, const int* tasks,
+                     int ntasks, const int* a_colptr, const KernelOpts& o, const FactorGlobals* g, int level,
+                     int dynamic, cudaStream_t stream);
+void launch_factor_small(const FrontDesc* fronts, const ChildLink* links, FrontState* st, const int* list, int count,
+                         int max_m, const int* a_colptr, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
+                         cudaStream_t stream);
+void launch_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m, int nb,
+                  const KernelOpts& o, FactorGlobals* g, int level, int dynamic, cudaStream_t stream);
+void launch_trailing(const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
+                     const FactorGlobals* g, int level, int dynamic, cudaStream_t stream);
+
+// Solve
+void launch_permute_in(int n, int nrhs, const int* perm, const double* B, int ldb, double* Bp, cudaStream_t stream);
+void launch_permute_out(int n, int nrhs, const int* perm, const double* X, double* Xout, int ldx, cudaStream_t stream);
+void launch_forward(const FrontDesc* fronts, const ChildLink* links, const FrontState* st, const int* list, int count,
+                    int nrhs, const double* Bp, double* Z, int n, cudaStream_t stream);
+void launch_backward(const FrontDesc* fronts, const FrontState* st, const int* list, int count, int nrhs,
+                     const double* Z, double* X, int n, cudaStream_t stream);
+
+// Residual R = B - sym(A) X in the original index space (full symmetric CSR
+// gathered from the stored lower triangle); rowptr/colind/vidx describe it.
+void launch_residual(int n, int nrhs, const int* rowptr, const int* colind, const int* vidx, const double* vals,
+                     const double* X, int ldx, const double* B, int ldb, double* R, cudaStream_t stream);
+// out[slot] = max(out[slot], max |v|) over len entries (out pre-zeroed).
+void launch_absmax(const double* v, long long len, double* out, cudaStream_t stream);
+// Max absolute row sum over the stored entries (refine.hpp:69-81).
+void launch_rowsum_max(int n, const int* srowptr, const int* svidx, const double* vals, double* out,
+                       cudaStream_t stream);
+// X += dX (len entries)
+void launch_axpy(long long len, const double* dx, double* x, cudaStream_t stream);
+void launch_copy2d(int rows, int cols, const double* src, int lds, double* dst, int ldd, cudaStream_t stream);
+
+}  // namespace symla_gpu

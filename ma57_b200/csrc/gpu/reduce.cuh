@@ -1,0 +1,74 @@
+// Block-level reductions used by the dense kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace symla_gpu {
+
+// (value, index) argmax with the reference's scan semantics: the larger value
+// wins; among equal values the smaller index wins (dense_kernel.hpp:588-596
+// scans rows upward with a strict '>').
+struct ArgMax {
+  double v;
+  int i;
+};
+
+__device__ __forceinline__ ArgMax argmax_combine(ArgMax a, ArgMax b) {
+  if (b.v > a.v || (b.v == a.v && b.i < a.i && b.i >= 0)) return b;
+  return a;
+}
+
+__device__ __forceinline__ ArgMax warp_argmax(ArgMax a) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    ArgMax o;
+    o.v = __shfl_xor_sync(0xffffffffu, a.v, off);
+    o.i = __shfl_xor_sync(0xffffffffu, a.i, off);
+    a = argmax_combine(a, o);
+  }
+  return a;
+}
+
+// Block argmax; every thread returns the result. Scratch: NT/32 entries each.
+template <int NT>
+__device__ __forceinline__ ArgMax block_argmax(ArgMax a, double* sv, int* si) {
+  a = warp_argmax(a);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) {
+    sv[wid] = a.v;
+    si[wid] = a.i;
+  }
+  __syncthreads();
+  ArgMax r{sv[0], si[0]};
+#pragma unroll
+  for (int w = 1; w < NT / 32; ++w) r = argmax_combine(r, ArgMax{sv[w], si[w]});
+  return r;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+  return v;
+}
+
+template <int NT>
+__device__ __forceinline__ double block_max(double v, double* sv) {
+  v = warp_max(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sv[wid] = v;
+  __syncthreads();
+  double r = sv[0];
+#pragma unroll
+  for (int w = 1; w < NT / 32; ++w) r = fmax(r, sv[w]);
+  return r;
+}
+
+// atomicMax for non-negative doubles (IEEE order == integer order there).
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+  if (!(v >= 0.0)) return;
+  atomicMax(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+}  // namespace symla_gpu
