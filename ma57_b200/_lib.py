@@ -94,7 +94,13 @@ _SIGS = {
     "symla_gpu_stream": (_p, [_p]),
     "symla_gpu_phase_ms": (_i, [_p, _pf, _i]),
     "symla_gpu_plan_stats": (_i, [_p, _pd, _i]),
+    "symla_gpu_set_profiling": (_i, [_p, _i]),
+    "symla_gpu_kernel_stats": (_i, [_p, _i, _pd]),
+    "symla_gpu_reset_kernel_stats": (None, [_p]),
+    "symla_gpu_launch_count": (C.c_longlong, [_p]),
 }
+
+KERNEL_KINDS = ["trailing", "panel", "small", "assemble", "forward", "backward", "residual"]
 
 # Every symbol declared in include/symla_gpu.h that is a function.
 EXPORTED = tuple(_SIGS.keys())

@@ -222,20 +222,50 @@ void build_level_lists(symla_gpu_ctx* c, const std::vector<int>& frontsOfLevel, 
   L.all = frontsOfLevel;
   L.small_max_m = L.large_max_m = 0;
   L.panels = 0;
+  L.small_flops = 0.0;
+  L.assemble_bytes = 0.0;
+  L.trailing_flops.clear();
+  L.solve_bytes_per_rhs = 0.0;
+  L.solve_bytes_fixed = 0.0;
   int tiles = 0;
   for (int s : frontsOfLevel) {
     const auto& f = c->fronts[s];
+    // algorithmic factorization flops of the front's nelig 1x1 pivots
+    // (lower-triangle convention: r + r(r+1) for trailing size r)
+    double ff = 0.0;
+    for (int k = 0; k < f.nelig; ++k) {
+      const double r = f.m - k - 1;
+      ff += r + r * (r + 1);
+    }
+    const double np = f.nelig;
+    L.solve_bytes_fixed += 8.0 * (f.m * np - np * (np - 1) / 2.0) + 4.0 * f.m;
+    L.solve_bytes_per_rhs += 8.0 * 2.0 * f.m;
     if (f.m <= kSmallFrontMax) {
       L.small.push_back(s);
       L.small_max_m = std::max(L.small_max_m, f.m);
+      L.small_flops += ff;
     } else {
       L.large.push_back(s);
       L.large_max_m = std::max(L.large_max_m, f.m);
-      L.panels = std::max(L.panels, (f.nelig + kPanelWidth - 1) / kPanelWidth);
+      const int panels = (f.nelig + kPanelWidth - 1) / kPanelWidth;
+      L.panels = std::max(L.panels, panels);
+      if (static_cast<int>(L.trailing_flops.size()) < panels) L.trailing_flops.resize(panels, 0.0);
+      for (int it = 0; it < panels; ++it) {
+        const int ps = it * kPanelWidth;
+        const int p = std::min(kPanelWidth, f.nelig - ps);
+        const double mt = f.m - (ps + p);
+        L.trailing_flops[it] += static_cast<double>(p) * mt * (mt + 1.0);
+      }
       for (int j0 = 0; j0 < f.m; j0 += 32) {
         L.tasks.push_back(s);
         L.tasks.push_back(j0);
       }
+      double cbsum = 0.0;
+      for (int ch : f.children) {
+        const double cb = c->fronts[ch].m - c->fronts[ch].nelig;
+        cbsum += cb * (cb + 1) / 2.0;
+      }
+      L.assemble_bytes += 8.0 * (cbsum + static_cast<double>(f.m) * (f.m + 1) / 2.0);
       const int mt = std::max(0, f.m - std::min(f.nelig, kPanelWidth));
       const int nt = (mt + 63) / 64;
       tiles = std::max(tiles, nt * (nt + 1) / 2);
@@ -254,7 +284,10 @@ void free_level_device(LevelLists& L) {
   dfree(L.d_large);
   dfree(L.d_tasks);
   dfree(L.d_all);
+  dfree(L.d_fwd_tasks);
+  dfree(L.d_bwd_tasks);
   L.d_small = L.d_large = L.d_tasks = L.d_all = nullptr;
+  L.d_fwd_tasks = L.d_bwd_tasks = nullptr;
 }
 
 void upload_level_lists(LevelLists& L, cudaStream_t s) {
@@ -481,6 +514,7 @@ void build_plan(symla_gpu_ctx* c, const symla_host::SymbolicFactor& sf, const in
   std::vector<int> svidx(c->nnz), fill(scount.begin(), scount.end() - 1);
   for (int cc = 0; cc < n; ++cc)
     for (int p = colptr[cc]; p < colptr[cc + 1]; ++p) svidx[fill[rowind[p]]++] = p;
+  c->nnz_full = static_cast<long long>(colind.size());
   c->d_rowptr = dupload(rowptr, c->stream);
   c->d_colind = dupload(colind, c->stream);
   c->d_vidx = dupload(vidx, c->stream);
@@ -530,6 +564,10 @@ void reset_to_static(symla_gpu_ctx* c) {
   free_dynamic(c);
 }
 
+template <typename F>
+void timed(symla_gpu_ctx* c, int kind, double flops, double bytes, F&& launch);
+void collect_pending(symla_gpu_ctx* c);
+
 KernelOpts make_kernel_opts(symla_gpu_ctx* c, const symla_factor_opts* o) {
   KernelOpts k{};
   k.mode = o->mode;
@@ -552,16 +590,25 @@ void launch_level(symla_gpu_ctx* c, const LevelLists& L, int level, const Kernel
                   const int* d_small, const int* d_large, const int* d_tasks) {
   cudaStream_t st = c->stream;
   if (!L.small.empty())
-    launch_factor_small(c->d_desc, c->d_links, c->d_state, d_small, static_cast<int>(L.small.size()), L.small_max_m,
-                        c->d_a_colptr, ko, c->d_glob, level, dynamic, st);
+    timed(c, SYMLA_KERNEL_SMALL, L.small_flops, 0.0, [&] {
+      launch_factor_small(c->d_desc, c->d_links, c->d_state, d_small, static_cast<int>(L.small.size()),
+                          L.small_max_m, c->d_a_colptr, ko, c->d_glob, level, dynamic, st);
+    });
   if (!L.large.empty()) {
-    launch_assemble(c->d_desc, c->d_links, c->d_state, d_tasks, static_cast<int>(L.tasks.size() / 2), c->d_a_colptr,
-                    ko, c->d_glob, level, dynamic, st);
+    timed(c, SYMLA_KERNEL_ASSEMBLE, 0.0, L.assemble_bytes, [&] {
+      launch_assemble(c->d_desc, c->d_links, c->d_state, d_tasks, static_cast<int>(L.tasks.size() / 2),
+                      c->d_a_colptr, ko, c->d_glob, level, dynamic, st);
+    });
     for (int it = 0; it < L.panels; ++it) {
-      launch_panel(c->d_desc, c->d_state, d_large, static_cast<int>(L.large.size()), L.large_max_m, kPanelWidth, ko,
-                   c->d_glob, level, dynamic, st);
-      launch_trailing(c->d_desc, c->d_state, d_large, static_cast<int>(L.large.size()), L.trailing_grid, c->d_glob,
-                      level, dynamic, st);
+      timed(c, SYMLA_KERNEL_PANEL, 0.0, 0.0, [&] {
+        launch_panel(c->d_desc, c->d_state, d_large, static_cast<int>(L.large.size()), L.large_max_m, kPanelWidth,
+                     ko, c->d_glob, level, dynamic, st);
+      });
+      const double tf = it < static_cast<int>(L.trailing_flops.size()) ? L.trailing_flops[it] : 0.0;
+      timed(c, SYMLA_KERNEL_TRAILING, tf, 0.0, [&] {
+        launch_trailing(c->d_desc, c->d_state, d_large, static_cast<int>(L.large.size()), L.trailing_grid, c->d_glob,
+                        level, dynamic, st);
+      });
     }
   }
   CK(cudaGetLastError());
@@ -713,6 +760,7 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
   }
   CK(cudaEventRecord(c->ev[1], st));
   CK(cudaEventSynchronize(c->ev[1]));
+  collect_pending(c);
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
   if (!dynamic) read_states(c);
@@ -798,28 +846,95 @@ void ensure_workspace(symla_gpu_ctx* c, int nrhs) {
   c->w_dirty = false;
 }
 
-// X(final order scratch) := A^{-1} B for device B (ldb) into device X (ldx),
-// both in the original index space.
+// (Re)build the pipelined solve task lists when the fronts' sizes or pivot
+// counts differ from the ones the lists were built for.
+void ensure_solve_tasks(symla_gpu_ctx* c) {
+  std::vector<int> np(c->numSN);
+  for (int s = 0; s < c->numSN; ++s) np[s] = c->hstate[s].npiv;
+  bool same = (np == c->solve_np) && c->d_flags != nullptr && !c->w_dirty;
+  if (same) return;
+  const int RB = solve_block_rows();
+  std::vector<int> fbase(c->numSN);
+  int total = 0;
+  for (int s = 0; s < c->numSN; ++s) {
+    fbase[s] = total;
+    total += (c->hdesc[s].m + RB - 1) / RB;
+  }
+  if (total > c->flag_count || !c->d_flags) {
+    dfree(c->d_flags);
+    c->d_flags = dalloc<int>(std::max(1, total));
+    CK(cudaMemsetAsync(c->d_flags, 0, std::max(1, total) * sizeof(int), c->stream));
+    c->flag_count = total;
+    c->solve_epoch = 0;
+  }
+  dfree(c->d_flag_base);
+  c->d_flag_base = dupload(fbase, c->stream);
+  for (auto& L : c->levels) {
+    L.fwd_tasks.clear();
+    L.bwd_tasks.clear();
+    for (int s : L.all) {
+      const int m = c->hdesc[s].m;
+      for (int rb = 0; rb * RB < m; ++rb) L.fwd_tasks.push_back(make_int2(s, rb));
+      const int nbp = (np[s] + RB - 1) / RB;
+      for (int cb = nbp - 1; cb >= 0; --cb) L.bwd_tasks.push_back(make_int2(s, cb));
+    }
+    dfree(L.d_fwd_tasks);
+    dfree(L.d_bwd_tasks);
+    L.d_fwd_tasks = dupload(L.fwd_tasks, c->stream);
+    L.d_bwd_tasks = dupload(L.bwd_tasks, c->stream);
+  }
+  c->solve_np = np;
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+// X := A^{-1} B for device B (ldb) into device X (ldx), both in the
+// original index space.
 void device_solve(symla_gpu_ctx* c, const double* dB, int ldb, int nrhs, double* dX, int ldx) {
   cudaStream_t st = c->stream;
   ensure_vectors(c, nrhs);
   ensure_workspace(c, nrhs);
+  ensure_solve_tasks(c);
   const int n = c->n;
   launch_permute_in(n, nrhs, c->d_perm, dB, ldb, c->d_Bp, st);
   CK(cudaEventRecord(c->ev[2], st));
-  for (int l = 0; l < c->numLevels; ++l) {
-    const auto& L = c->levels[l];
-    launch_forward(c->d_desc, c->d_links, c->d_state, L.d_all, static_cast<int>(L.all.size()), nrhs, c->d_Bp, c->d_Z,
-                   n, st);
-  }
-  CK(cudaEventRecord(c->ev[3], st));
-  for (int l = c->numLevels - 1; l >= 0; --l) {
-    const auto& L = c->levels[l];
-    launch_backward(c->d_desc, c->d_state, L.d_all, static_cast<int>(L.all.size()), nrhs, c->d_Z, c->d_Xf, n, st);
+  const int chunk = solve_rhs_chunk();
+  for (int c0 = 0; c0 < nrhs; c0 += chunk) {
+    const int nc = std::min(chunk, nrhs - c0);
+    const int ef = ++c->solve_epoch;
+    for (int l = 0; l < c->numLevels; ++l) {
+      const auto& L = c->levels[l];
+      const int nt = static_cast<int>(L.fwd_tasks.size());
+      const int grid = std::min(nt, c->fwd_resident);
+      timed(c, SYMLA_KERNEL_FORWARD, 0.0, L.solve_bytes_fixed + nc * L.solve_bytes_per_rhs, [&] {
+        CK(launch_forward_pipelined(c->d_desc, c->d_links, c->d_state, L.d_fwd_tasks, nt, grid, c->d_flag_base,
+                                    c->d_flags, ef, c->d_solve_err, nrhs, c0, c->d_Bp, n, st));
+      });
+    }
+    if (c0 == 0) CK(cudaEventRecord(c->ev[3], st));
+    const int eb = ++c->solve_epoch;
+    for (int l = c->numLevels - 1; l >= 0; --l) {
+      const auto& L = c->levels[l];
+      const int nt = static_cast<int>(L.bwd_tasks.size());
+      const int grid = std::min(nt, c->bwd_resident);
+      timed(c, SYMLA_KERNEL_BACKWARD, 0.0, L.solve_bytes_fixed + nc * L.solve_bytes_per_rhs, [&] {
+        CK(launch_backward_pipelined(c->d_desc, c->d_state, L.d_bwd_tasks, nt, grid, c->d_flag_base, c->d_flags, eb,
+                                     c->d_solve_err, nrhs, c0, c->d_Xf, n, st));
+      });
+    }
   }
   CK(cudaEventRecord(c->ev[4], st));
   launch_permute_out(n, nrhs, c->d_perm, c->d_Xf, dX, ldx, st);
   CK(cudaGetLastError());
+}
+
+void check_solve_error(symla_gpu_ctx* c) {
+  int err = 0;
+  CK(cudaMemcpyAsync(&err, c->d_solve_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (err != 0) {
+    CK(cudaMemsetAsync(c->d_solve_err, 0, sizeof(int), c->stream));
+    throw SymlaError(SYMLA_ERR_TIMEOUT, "solve: a pipelined block wait timed out");
+  }
 }
 
 void check_solvable(symla_gpu_ctx* c) {
@@ -839,6 +954,49 @@ void upload_values(symla_gpu_ctx* c, const double* values, int on_device) {
     CK(cudaMemcpyAsync(c->d_values, values, c->nnz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
 }
 
+
+cudaEvent_t pool_event(symla_gpu_ctx* c) {
+  if (!c->evpool.empty()) {
+    cudaEvent_t e = c->evpool.back();
+    c->evpool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  CK(cudaEventCreate(&e));
+  return e;
+}
+
+// Brackets a launch with events when profiling; always counts the launch.
+template <typename F>
+void timed(symla_gpu_ctx* c, int kind, double flops, double bytes, F&& launch) {
+  c->launches++;
+  if (!c->profiling) {
+    launch();
+    return;
+  }
+  cudaEvent_t a = pool_event(c), b = pool_event(c);
+  CK(cudaEventRecord(a, c->stream));
+  launch();
+  CK(cudaEventRecord(b, c->stream));
+  c->pending.push_back({a, b, kind, flops, bytes});
+}
+
+void collect_pending(symla_gpu_ctx* c) {
+  if (c->pending.empty()) return;
+  CK(cudaStreamSynchronize(c->stream));
+  for (auto& p : c->pending) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, p.a, p.b));
+    auto& k = c->kstat[p.kind];
+    k.launches++;
+    k.ms += ms;
+    k.flops += p.flops;
+    k.bytes += p.bytes;
+    c->evpool.push_back(p.a);
+    c->evpool.push_back(p.b);
+  }
+  c->pending.clear();
+}
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -863,6 +1021,9 @@ extern "C" int symla_gpu_create(const symla_symbolic* sym, int n, const int* col
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     c->n = n;
     c->nnz = n > 0 ? colptr[n] : 0;
+    CK(solve_max_resident(device, &c->fwd_resident, &c->bwd_resident));
+    c->d_solve_err = dalloc<int>(1);
+    CK(cudaMemsetAsync(c->d_solve_err, 0, sizeof(int), c->stream));
     build_plan(c, sym->sf, colptr, rowind);
   });
   if (rc != SYMLA_OK) {
@@ -882,10 +1043,15 @@ extern "C" void symla_gpu_destroy(symla_gpu_ctx* c) {
                   c->d_glob, c->d_a_colptr, c->d_a_j, c->d_a_pos, c->d_a_idx, c->d_values, c->d_sign_final,
                   c->d_front_delta, c->d_perm, c->d_rowptr, c->d_colind, c->d_vidx, c->d_srowptr, c->d_svidx, c->d_W,
                   c->d_Bp, c->d_Z, c->d_Xf, c->d_B, c->d_X, c->d_R, c->d_dX, c->d_Xn, c->d_Rn, c->d_norms,
-                  c->d_scratch_int};
+                  c->d_scratch_int, c->d_flag_base, c->d_flags, c->d_solve_err};
   for (void* p : ptrs) dfree(p);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& p : c->pending) {
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  for (auto e : c->evpool) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -1063,6 +1229,8 @@ extern "C" int symla_gpu_solve(symla_gpu_ctx* c, const double* B, int ldb, int n
     }
     CK(cudaEventRecord(c->ev[6], c->stream));
     CK(cudaEventSynchronize(c->ev[6]));
+    collect_pending(c);
+    check_solve_error(c);
     float a = 0, b = 0, t = 0;
     cudaEventElapsedTime(&a, c->ev[2], c->ev[3]);
     cudaEventElapsedTime(&b, c->ev[3], c->ev[4]);
@@ -1105,7 +1273,9 @@ extern "C" int symla_gpu_solve_refine(symla_gpu_ctx* c, const double* values, co
     device_solve(c, c->d_B, n, nrhs, c->d_X, n);
     auto residual_of = [&](const double* Xd, double* Rd, double* out2) {
       CK(cudaMemsetAsync(c->d_norms + 2, 0, 2 * sizeof(double), st));
-      launch_residual(n, nrhs, c->d_rowptr, c->d_colind, c->d_vidx, c->d_values, Xd, n, c->d_B, n, Rd, st);
+      timed(c, SYMLA_KERNEL_RESIDUAL, 2.0 * c->nnz_full * nrhs, 12.0 * c->nnz_full + 16.0 * n * nrhs, [&] {
+        launch_residual(n, nrhs, c->d_rowptr, c->d_colind, c->d_vidx, c->d_values, Xd, n, c->d_B, n, Rd, st);
+      });
       launch_absmax(Rd, len, c->d_norms + 2, st);
       launch_absmax(Xd, len, c->d_norms + 3, st);
       double h[4];
@@ -1139,6 +1309,8 @@ extern "C" int symla_gpu_solve_refine(symla_gpu_ctx* c, const double* values, co
       CK(cudaMemcpy2DAsync(X, static_cast<size_t>(ldx) * sizeof(double), c->d_X, n * sizeof(double),
                            n * sizeof(double), nrhs, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    collect_pending(c);
+    check_solve_error(c);
     if (info) *info = ri;
   });
 }
@@ -1230,3 +1402,27 @@ extern "C" int symla_gpu_plan_stats(symla_gpu_ctx* c, double* out, int cap) {
   for (int i = 0; i < cap && i < 7; ++i) out[i] = v[i];
   return 7;
 }
+
+extern "C" int symla_gpu_set_profiling(symla_gpu_ctx* c, int enable) {
+  if (!c) return set_error(SYMLA_ERR_INVALID, "null context");
+  c->profiling = enable != 0;
+  return SYMLA_OK;
+}
+
+extern "C" int symla_gpu_kernel_stats(symla_gpu_ctx* c, int kind, double* out4) {
+  if (!c || kind < 0 || kind >= SYMLA_KERNEL_KINDS || !out4) return set_error(SYMLA_ERR_INVALID, "bad arguments");
+  const auto& k = c->kstat[kind];
+  out4[0] = static_cast<double>(k.launches);
+  out4[1] = k.ms;
+  out4[2] = k.flops;
+  out4[3] = k.bytes;
+  return SYMLA_OK;
+}
+
+extern "C" void symla_gpu_reset_kernel_stats(symla_gpu_ctx* c) {
+  if (!c) return;
+  for (auto& k : c->kstat) k = symla_gpu_ctx::KStat();
+  c->launches = 0;
+}
+
+extern "C" long long symla_gpu_launch_count(symla_gpu_ctx* c) { return c ? c->launches : 0; }

@@ -51,6 +51,9 @@ struct FrontState {
 
 enum : int { kFlagDone = 1, kFlagDelayed = 2, kFlagSingularRoot = 4 };
 
+// Error word of the pipelined solve kernels.
+constexpr int kSolveErrTimeout = 1;
+
 // Global counters for one factorization (device, zeroed per call).
 struct FactorGlobals {
   int delay_level;     // lowest level that produced a delayed column, or INT_MAX

@@ -34,6 +34,16 @@ struct LevelLists {
   int trailing_grid = 0;
   std::vector<int> tasks;      // assembly tasks (front, column block) for large fronts
   std::vector<int> all;        // every front of the level (solve)
+  // algorithmic work estimates (instrumentation)
+  double small_flops = 0.0;
+  double assemble_bytes = 0.0;
+  std::vector<double> trailing_flops;  // per panel iteration
+  double solve_bytes_fixed = 0.0;
+  double solve_bytes_per_rhs = 0.0;
+  // pipelined solve tasks {front, block}
+  std::vector<int2> fwd_tasks, bwd_tasks;
+  int2* d_fwd_tasks = nullptr;
+  int2* d_bwd_tasks = nullptr;
   // device copies (static plan)
   int* d_small = nullptr;
   int* d_large = nullptr;
@@ -53,6 +63,7 @@ struct symla_gpu_ctx {
   cudaStream_t stream = nullptr;
   int n = 0;
   int nnz = 0;
+  long long nnz_full = 0;
   int numSN = 0;
   int numLevels = 0;
 
@@ -118,6 +129,15 @@ struct symla_gpu_ctx {
   int* d_scratch_int = nullptr;
   size_t scratch_int_cap = 0;
 
+  // pipelined solve
+  int* d_flag_base = nullptr;
+  int* d_flags = nullptr;
+  int* d_solve_err = nullptr;
+  int flag_count = 0;
+  int solve_epoch = 0;
+  int fwd_resident = 0, bwd_resident = 0;
+  std::vector<int> solve_np;  // npiv per front the task lists were built for
+
   // dynamic (delayed-pivot) allocations for the current factorization
   std::vector<void*> dyn_allocs;
 
@@ -133,4 +153,19 @@ struct symla_gpu_ctx {
   int plan_max_m = 0;
   long long nnzL = 0;
   int last_precision = 0;
+
+  // instrumentation
+  bool profiling = false;
+  long long launches = 0;
+  struct KStat {
+    long long launches = 0;
+    double ms = 0.0, flops = 0.0, bytes = 0.0;
+  } kstat[7];
+  struct PendingEv {
+    cudaEvent_t a, b;
+    int kind;
+    double flops, bytes;
+  };
+  std::vector<PendingEv> pending;
+  std::vector<cudaEvent_t> evpool;
 };

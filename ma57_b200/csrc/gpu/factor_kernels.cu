@@ -389,6 +389,7 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
   }
   for (int t = threadIdx.x; t < m; t += NT) {
     f.fidx[t] = fi[t];
+    f.lperm[t] = lp[t];
     f.lpos[lp[t]] = t;
   }
   const double rmax = block_max<NT>(thread_rmax, red_v);

@@ -12,9 +12,20 @@
 //                      L_bottom^T x, transposed unit-lower solve
 //   refine.hpp:116     R = B - A.selfadjointView<Lower>() * X
 //
-// Sign convention: a front's workspace rows for its own pivots hold
-// Bp - (children's deltas) - L y, i.e. y after the solve; its remaining rows
-// hold the negated forwarded delta, so the parent adds them.
+// Work decomposition: every front is cut into 64-row blocks (forward) or
+// 64-column blocks of its pivot range (backward). One cooperative launch per
+// tree level runs all blocks of all fronts of that level; a block that needs
+// the solution of an earlier block of the same front waits for that block's
+// flag (release/acquire), so the triangular solve of a large front is
+// pipelined across many SMs instead of running in one CTA. Each CTA walks its
+// blocks in increasing task order and a block only waits on blocks with a
+// smaller task index, and the launch is cooperative (all CTAs resident), so
+// the waits always end; every wait is still bounded and reports a timeout
+// through the error word instead of spinning forever.
+//
+// Sign convention: a front's workspace rows for its own pivots hold y after
+// the forward pass; its remaining rows hold the negated forwarded delta
+// (sum of the children's minus L_bottom * y), so the parent adds them.
 #include <cmath>
 
 #include "common.cuh"
@@ -24,8 +35,53 @@
 namespace symla_gpu {
 
 namespace {
-constexpr int kSolveThreads = 256;
-constexpr int kBlk = 32;
+constexpr int kRB = 64;        // rows (forward) / columns (backward) per block
+constexpr int kST = 256;       // threads per CTA
+constexpr int kRhsChunk = 16;  // right-hand sides per pass
+constexpr long long kSpinLimit = 40000000;  // a few seconds with the sleep below
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Wait until flags[idx] >= epoch; false on timeout or a raised error.
+__device__ bool wait_flag(const int* flags, int idx, int epoch, int* err) {
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    long long it = 0;
+    int ok = 1;
+    while (ld_acquire(flags + idx) < epoch) {
+      if (ld_acquire(err) != 0) {
+        ok = 0;
+        break;
+      }
+      if (++it > kSpinLimit) {
+        atomicCAS(err, 0, kSolveErrTimeout);
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  const bool ok = s_ok != 0;
+  __syncthreads();
+  return ok;
+}
+
+__device__ __forceinline__ void publish(int* flags, int idx, int epoch) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    st_release(flags + idx, epoch);
+  }
+}
 }  // namespace
 
 __global__ void permute_in_kernel(int n, int nrhs, const int* __restrict__ perm, const double* __restrict__ B, int ldb,
@@ -44,145 +100,227 @@ __global__ void permute_out_kernel(int n, int nrhs, const int* __restrict__ perm
   Xout[perm[i] + static_cast<long long>(c) * ldx] = X[t];
 }
 
-__global__ void __launch_bounds__(kSolveThreads) forward_kernel(const FrontDesc* __restrict__ fronts,
-                                                                const ChildLink* __restrict__ links,
-                                                                const FrontState* __restrict__ st,
-                                                                const int* __restrict__ list, int nrhs,
-                                                                const double* __restrict__ Bp, double* __restrict__ Z,
-                                                                int n) {
-  const int s = list[blockIdx.x];
-  const FrontDesc f = fronts[s];
-  const int m = f.m;
-  const int np = st[s].npiv;
-  double* W = f.W;
-  const int wld = f.wld;
-  const int64_t ld = f.ld;
-  for (int t = threadIdx.x; t < m * nrhs; t += blockDim.x) {
-    const int i = t % m, c = t / m;
-    W[i + static_cast<int64_t>(c) * wld] = (i < np) ? Bp[f.fidx[i] + static_cast<int64_t>(c) * n] : 0.0;
-  }
-  __syncthreads();
-  for (int ch = f.ch_begin; ch < f.ch_end; ++ch) {
-    const ChildLink L = links[ch];
-    const FrontDesc cf = fronts[L.child];
-    const int cnp = st[L.child].npiv;
-    const int cb = cf.m - cnp;
-    for (int t = threadIdx.x; t < cb * nrhs; t += blockDim.x) {
-      const int a = t % cb, c = t / cb;
-      // relmap gives the parent's pre-pivot position; lpos maps it through
-      // the parent's pivoting swaps
-      W[f.lpos[L.relmap[a]] + static_cast<int64_t>(c) * wld] += cf.W[cnp + a + static_cast<int64_t>(c) * cf.wld];
-    }
-    __syncthreads();
-  }
-  // blocked forward substitution over the pivot columns; rows below each
-  // block (own rows and forwarded rows alike) are updated as we go
-  for (int j0 = 0; j0 < np; j0 += kBlk) {
-    const int j1 = min(j0 + kBlk, np);
-    for (int c = threadIdx.x; c < nrhs; c += blockDim.x) {
-      double* w = W + static_cast<int64_t>(c) * wld;
-      for (int j = j0; j < j1; ++j) {
-        const double yj = w[j];
-        const double* Lj = f.F + j * ld;
-        const int skip = (f.pk[j] == 1) ? j + 1 : -1;
-        for (int i = j + 1; i < j1; ++i)
-          if (i != skip) w[i] -= Lj[i] * yj;
+// Forward task = (front, row block); flag of a pivot row block at
+// flag_base[front] + row block.
+__global__ void __launch_bounds__(kST) forward_pipelined_kernel(
+    const FrontDesc* __restrict__ fronts, const ChildLink* __restrict__ links, const FrontState* __restrict__ st,
+    const int2* __restrict__ tasks, int ntasks, const int* __restrict__ flag_base, int* flags, int epoch, int* err,
+    int nrhs, int c0, const double* __restrict__ Bp, int n) {
+  __shared__ double acc[kRB][kRhsChunk + 1];
+  // the staged y block (step 2) and the diagonal L block (step 3) are never
+  // live at the same time
+  __shared__ double stage[kRB * (kRB + 1)];
+  double(*yb)[kRhsChunk + 1] = reinterpret_cast<double(*)[kRhsChunk + 1]>(stage);
+  double(*Ld)[kRB + 1] = reinterpret_cast<double(*)[kRB + 1]>(stage);
+  const int nc = min(kRhsChunk, nrhs - c0);
+  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
+    if (ld_acquire(err) != 0) return;
+    const int s = tasks[task].x, rb = tasks[task].y;
+    const FrontDesc f = fronts[s];
+    const int m = f.m, np = st[s].npiv;
+    const int r0 = rb * kRB, r1 = min(r0 + kRB, m), nr = r1 - r0;
+    const int64_t ld = f.ld;
+    double* W = f.W;
+    const int wld = f.wld;
+    // 1. Bp for pivot rows plus the children's forwarded rows, gathered
+    //    through each row's pre-pivot position
+    for (int t = threadIdx.x; t < nr * nc; t += kST) {
+      const int ii = t % nr, c = t / nr;
+      const int i = r0 + ii;
+      double v = (i < np) ? Bp[f.fidx[i] + static_cast<int64_t>(c0 + c) * n] : 0.0;
+      const int pre = f.lperm[i];
+      for (int ch = f.ch_begin; ch < f.ch_end; ++ch) {
+        const ChildLink L = links[ch];
+        const int a = L.invmap[pre];
+        if (a < 0) continue;
+        const FrontDesc& cf = fronts[L.child];
+        const int cnp = st[L.child].npiv;
+        v += cf.W[cnp + a + static_cast<int64_t>(c0 + c) * cf.wld];
       }
+      acc[ii][c] = v;
     }
     __syncthreads();
-    const int rows = m - j1;
-    for (int t = threadIdx.x; t < rows * nrhs; t += blockDim.x) {
-      const int i = j1 + t % rows, c = t / rows;
-      double* w = W + static_cast<int64_t>(c) * wld;
-      double acc = 0.0;
-      for (int j = j0; j < j1; ++j) {
-        if (i == j + 1 && f.pk[j] == 1) continue;
-        acc += f.F[j * ld + i] * w[j];
+    // 2. contributions of the finished pivot blocks before this row block
+    const int nbp = (np + kRB - 1) / kRB;
+    const int jend = min(rb, nbp);
+    for (int j = 0; j < jend; ++j) {
+      if (!wait_flag(flags, flag_base[s] + j, epoch, err)) return;
+      const int j0 = j * kRB, j1 = min(j0 + kRB, np), nj = j1 - j0;
+      for (int t = threadIdx.x; t < nj * nc; t += kST) {
+        const int jj = t % nj, c = t / nj;
+        yb[jj][c] = W[j0 + jj + static_cast<int64_t>(c0 + c) * wld];
       }
-      w[i] -= acc;
-    }
-    __syncthreads();
-  }
-  // D^{-1}
-  for (int t = threadIdx.x; t < np * nrhs; t += blockDim.x) {
-    const int q = t % np, c = t / np;
-    const double* w = W + static_cast<int64_t>(c) * wld;
-    const int8_t kind = f.pk[q];
-    if (kind == 0) {
-      Z[f.fidx[q] + static_cast<int64_t>(c) * n] = w[q] / f.Dd[q];
-    } else if (kind == 1) {
-      const double d11 = f.Dd[q], d21 = f.Do[q], d22 = f.Dd[q + 1];
-      const double det = d11 * d22 - d21 * d21;
-      const double y0 = w[q], y1 = w[q + 1];
-      Z[f.fidx[q] + static_cast<int64_t>(c) * n] = (d22 * y0 - d21 * y1) / det;
-      Z[f.fidx[q + 1] + static_cast<int64_t>(c) * n] = (-d21 * y0 + d11 * y1) / det;
-    }
-  }
-}
-
-__global__ void __launch_bounds__(kSolveThreads) backward_kernel(const FrontDesc* __restrict__ fronts,
-                                                                 const FrontState* __restrict__ st,
-                                                                 const int* __restrict__ list, int nrhs,
-                                                                 const double* __restrict__ Z, double* __restrict__ X,
-                                                                 int n) {
-  const int s = list[blockIdx.x];
-  const FrontDesc f = fronts[s];
-  const int m = f.m;
-  const int np = st[s].npiv;
-  if (np == 0) return;
-  double* W = f.W;
-  const int wld = f.wld;
-  const int64_t ld = f.ld;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  // x_own = z_own - L_bottom^T x_ext   (warp per pivot column)
-  for (int q = warp; q < np; q += nwarps) {
-    const double* Lq = f.F + q * ld;
-    for (int c = 0; c < nrhs; ++c) {
-      double acc = 0.0;
-      for (int t = np + lane; t < m; t += 32) acc += Lq[t] * X[f.fidx[t] + static_cast<int64_t>(c) * n];
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-      if (lane == 0) W[q + static_cast<int64_t>(c) * wld] = Z[f.fidx[q] + static_cast<int64_t>(c) * n] - acc;
-    }
-  }
-  __syncthreads();
-  // blocked backward substitution with Ltop^T
-  for (int j1 = np; j1 > 0; j1 -= kBlk) {
-    const int j0 = max(0, j1 - kBlk);
-    // contributions of rows i >= j1 to x[j], j in [j0, j1)
-    if (j1 < np) {
-      for (int j = j0 + warp; j < j1; j += nwarps) {
-        const double* Lj = f.F + j * ld;
-        for (int c = 0; c < nrhs; ++c) {
-          const double* w = W + static_cast<int64_t>(c) * wld;
-          double acc = 0.0;
-          for (int i = j1 + lane; i < np; i += 32) {
-            if (i == j + 1 && f.pk[j] == 1) continue;
-            acc += Lj[i] * w[i];
-          }
-#pragma unroll
-          for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-          if (lane == 0) W[j + static_cast<int64_t>(c) * wld] -= acc;
+      __syncthreads();
+      for (int t = threadIdx.x; t < nr * nc; t += kST) {
+        const int ii = t % nr, c = t / nr;
+        const int i = r0 + ii;
+        double sacc = 0.0;
+        for (int jj = 0; jj < nj; ++jj) {
+          const int jc = j0 + jj;
+          if (i == jc + 1 && f.pk[jc] == 1) continue;
+          sacc += f.F[jc * ld + i] * yb[jj][c];
         }
+        acc[ii][c] -= sacc;
       }
       __syncthreads();
     }
-    for (int c = threadIdx.x; c < nrhs; c += blockDim.x) {
-      double* w = W + static_cast<int64_t>(c) * wld;
-      for (int j = j1 - 1; j >= j0; --j) {
-        const double* Lj = f.F + j * ld;
-        const int skip = (f.pk[j] == 1) ? j + 1 : -1;
-        double acc = 0.0;
-        for (int i = j + 1; i < j1; ++i)
-          if (i != skip) acc += Lj[i] * w[i];
-        w[j] -= acc;
+    // 3. the block's own pivot columns: unit-lower solve for its pivot rows
+    //    and the matching update of its non-pivot rows
+    if (r0 < np) {
+      const int npv = min(r1, np) - r0;
+      for (int t = threadIdx.x; t < kRB * kRB; t += kST) {
+        const int ii = t % kRB, jj = t / kRB;
+        const int i = r0 + ii, jc = r0 + jj;
+        double l = 0.0;
+        if (ii < nr && jj < npv && i > jc) l = f.F[jc * ld + i];
+        if (ii < nr && jj < npv && i == jc + 1 && f.pk[jc] == 1) l = 0.0;
+        Ld[ii][jj] = l;
       }
+      __syncthreads();
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      for (int c = warp; c < nc; c += kST / 32) {
+        double y0 = (lane < nr) ? acc[lane][c] : 0.0;
+        double y1 = (lane + 32 < nr) ? acc[lane + 32][c] : 0.0;
+        for (int jj = 0; jj < npv; ++jj) {
+          const double yj = __shfl_sync(0xffffffffu, jj < 32 ? y0 : y1, jj & 31);
+          if (lane > jj) y0 -= Ld[lane][jj] * yj;
+          if (lane + 32 > jj) y1 -= Ld[lane + 32][jj] * yj;
+        }
+        if (lane < nr) acc[lane][c] = y0;
+        if (lane + 32 < nr) acc[lane + 32][c] = y1;
+      }
+      __syncthreads();
     }
+    for (int t = threadIdx.x; t < nr * nc; t += kST) {
+      const int ii = t % nr, c = t / nr;
+      W[r0 + ii + static_cast<int64_t>(c0 + c) * wld] = acc[ii][c];
+    }
+    if (r0 < np) publish(flags, flag_base[s] + rb, epoch);
     __syncthreads();
   }
-  for (int t = threadIdx.x; t < np * nrhs; t += blockDim.x) {
-    const int q = t % np, c = t / np;
-    X[f.fidx[q] + static_cast<int64_t>(c) * n] = W[q + static_cast<int64_t>(c) * wld];
+}
+
+// Backward task = (front, pivot column block), a front's blocks listed from
+// the last to the first; flag at flag_base[front] + column block.
+__global__ void __launch_bounds__(kST) backward_pipelined_kernel(
+    const FrontDesc* __restrict__ fronts, const FrontState* __restrict__ st, const int2* __restrict__ tasks,
+    int ntasks, const int* __restrict__ flag_base, int* flags, int epoch, int* err, int nrhs, int c0,
+    double* __restrict__ X, int n) {
+  __shared__ double acc[kRB][kRhsChunk + 1];
+  // staged x rows (step 2) and the diagonal L block (step 3) share storage
+  __shared__ double stage[kRB * (kRB + 1)];
+  double(*xb)[kRhsChunk + 1] = reinterpret_cast<double(*)[kRhsChunk + 1]>(stage);
+  double(*Ld)[kRB + 1] = reinterpret_cast<double(*)[kRB + 1]>(stage);
+  const int nc = min(kRhsChunk, nrhs - c0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int NW = kST / 32;
+  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
+    if (ld_acquire(err) != 0) return;
+    const int s = tasks[task].x, cb = tasks[task].y;
+    const FrontDesc f = fronts[s];
+    const int m = f.m, np = st[s].npiv;
+    const int q0 = cb * kRB, q1 = min(q0 + kRB, np), nq = q1 - q0;
+    const int64_t ld = f.ld;
+    const double* W = f.W;
+    const int wld = f.wld;
+    // 1. z = D^{-1} y for the block's pivots (a 2x2 partner may sit in the
+    //    neighbouring block; y is complete in W after the forward pass)
+    for (int t = threadIdx.x; t < nq * nc; t += kST) {
+      const int qq = t % nq, c = t / nq;
+      const int q = q0 + qq;
+      const double* w = W + static_cast<int64_t>(c0 + c) * wld;
+      const int8_t kind = f.pk[q];
+      double z;
+      if (kind == 0) {
+        z = w[q] / f.Dd[q];
+      } else if (kind == 1) {
+        const double d11 = f.Dd[q], d21 = f.Do[q], d22 = f.Dd[q + 1];
+        const double det = d11 * d22 - d21 * d21;
+        z = (d22 * w[q] - d21 * w[q + 1]) / det;
+      } else {
+        const double d11 = f.Dd[q - 1], d21 = f.Do[q - 1], d22 = f.Dd[q];
+        const double det = d11 * d22 - d21 * d21;
+        z = (-d21 * w[q - 1] + d11 * w[q]) / det;
+      }
+      acc[qq][c] = z;
+    }
+    __syncthreads();
+    // 2. minus L(rows below, block)^T x(rows below): the ancestor rows
+    //    [np, m) are final from earlier levels; later pivot blocks of this
+    //    front are waited for.
+    const int nbp = (np + kRB - 1) / kRB;
+    for (int j = nbp; j > cb; --j) {
+      int i0, i1;
+      if (j == nbp) {
+        i0 = np;
+        i1 = m;
+      } else {
+        if (!wait_flag(flags, flag_base[s] + j, epoch, err)) return;
+        i0 = j * kRB;
+        i1 = min(i0 + kRB, np);
+      }
+      for (int base = i0; base < i1; base += kRB) {
+        const int ni = min(kRB, i1 - base);
+        for (int t = threadIdx.x; t < ni * nc; t += kST) {
+          const int ii = t % ni, c = t / ni;
+          xb[ii][c] = X[f.fidx[base + ii] + static_cast<int64_t>(c0 + c) * n];
+        }
+        __syncthreads();
+        for (int qq = warp; qq < nq; qq += NW) {  // warp per column, lanes over rows
+          const int q = q0 + qq;
+          const double* Lq = f.F + q * ld;
+          double part[kRhsChunk];
+#pragma unroll
+          for (int c = 0; c < kRhsChunk; ++c) part[c] = 0.0;
+          for (int ii = lane; ii < ni; ii += 32) {
+            const int i = base + ii;
+            double l = Lq[i];
+            if (i == q + 1 && f.pk[q] == 1) l = 0.0;
+#pragma unroll
+            for (int c = 0; c < kRhsChunk; ++c)
+              if (c < nc) part[c] += l * xb[ii][c];
+          }
+#pragma unroll
+          for (int c = 0; c < kRhsChunk; ++c) {
+            double v = part[c];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+            if (lane == 0 && c < nc) acc[qq][c] -= v;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    // 3. transposed unit-lower solve on the diagonal block
+    for (int t = threadIdx.x; t < kRB * kRB; t += kST) {
+      const int ii = t % kRB, jj = t / kRB;
+      const int i = q0 + ii, jc = q0 + jj;
+      double l = 0.0;
+      if (ii < nq && jj < nq && i > jc) l = f.F[jc * ld + i];
+      if (ii < nq && jj < nq && i == jc + 1 && f.pk[jc] == 1) l = 0.0;
+      Ld[ii][jj] = l;
+    }
+    __syncthreads();
+    for (int c = warp; c < nc; c += NW) {
+      double x0 = (lane < nq) ? acc[lane][c] : 0.0;
+      double x1 = (lane + 32 < nq) ? acc[lane + 32][c] : 0.0;
+      for (int jj = nq - 1; jj >= 0; --jj) {
+        // x[jj] is final once every row below it has been applied; row jj of
+        // Ltop then updates the unknowns above it
+        const double xj = __shfl_sync(0xffffffffu, jj < 32 ? x0 : x1, jj & 31);
+        if (lane < jj) x0 -= Ld[jj][lane] * xj;
+        if (lane + 32 < jj) x1 -= Ld[jj][lane + 32] * xj;
+      }
+      if (lane < nq) acc[lane][c] = x0;
+      if (lane + 32 < nq) acc[lane + 32][c] = x1;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nq * nc; t += kST) {
+      const int qq = t % nq, c = t / nq;
+      X[f.fidx[q0 + qq] + static_cast<int64_t>(c0 + c) * n] = acc[qq][c];
+    }
+    publish(flags, flag_base[s] + cb, epoch);
+    __syncthreads();
   }
 }
 
@@ -238,21 +376,49 @@ inline unsigned grid_for(long long work, int threads) {
 }
 }  // namespace
 
+int solve_block_rows() { return kRB; }
+int solve_rhs_chunk() { return kRhsChunk; }
+
+cudaError_t solve_max_resident(int device, int* fwd_ctas, int* bwd_ctas) {
+  int sms = 0, a = 0, b = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, forward_pipelined_kernel, kST, 0);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, backward_pipelined_kernel, kST, 0);
+  if (e != cudaSuccess) return e;
+  *fwd_ctas = a * sms;
+  *bwd_ctas = b * sms;
+  return cudaSuccess;
+}
+
+cudaError_t launch_forward_pipelined(const FrontDesc* fronts, const ChildLink* links, const FrontState* st,
+                                     const int2* tasks, int ntasks, int grid, const int* flag_base, int* flags,
+                                     int epoch, int* err, int nrhs, int c0, const double* Bp, int n,
+                                     cudaStream_t stream) {
+  if (ntasks <= 0) return cudaSuccess;
+  void* args[] = {(void*)&fronts, (void*)&links, (void*)&st,  (void*)&tasks, (void*)&ntasks,
+                  (void*)&flag_base, (void*)&flags, (void*)&epoch, (void*)&err, (void*)&nrhs,
+                  (void*)&c0,     (void*)&Bp,    (void*)&n};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(forward_pipelined_kernel), dim3(grid), dim3(kST),
+                                     args, 0, stream);
+}
+
+cudaError_t launch_backward_pipelined(const FrontDesc* fronts, const FrontState* st, const int2* tasks, int ntasks,
+                                      int grid, const int* flag_base, int* flags, int epoch, int* err, int nrhs,
+                                      int c0, double* X, int n, cudaStream_t stream) {
+  if (ntasks <= 0) return cudaSuccess;
+  void* args[] = {(void*)&fronts, (void*)&st,  (void*)&tasks, (void*)&ntasks, (void*)&flag_base, (void*)&flags,
+                  (void*)&epoch,  (void*)&err, (void*)&nrhs,  (void*)&c0,     (void*)&X,         (void*)&n};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(backward_pipelined_kernel), dim3(grid), dim3(kST),
+                                     args, 0, stream);
+}
+
 void launch_permute_in(int n, int nrhs, const int* perm, const double* B, int ldb, double* Bp, cudaStream_t stream) {
   permute_in_kernel<<<grid_for(static_cast<long long>(n) * nrhs, 256), 256, 0, stream>>>(n, nrhs, perm, B, ldb, Bp);
 }
 void launch_permute_out(int n, int nrhs, const int* perm, const double* X, double* Xout, int ldx, cudaStream_t stream) {
   permute_out_kernel<<<grid_for(static_cast<long long>(n) * nrhs, 256), 256, 0, stream>>>(n, nrhs, perm, X, Xout, ldx);
-}
-void launch_forward(const FrontDesc* fronts, const ChildLink* links, const FrontState* st, const int* list, int count,
-                    int nrhs, const double* Bp, double* Z, int n, cudaStream_t stream) {
-  if (count <= 0) return;
-  forward_kernel<<<count, kSolveThreads, 0, stream>>>(fronts, links, st, list, nrhs, Bp, Z, n);
-}
-void launch_backward(const FrontDesc* fronts, const FrontState* st, const int* list, int count, int nrhs,
-                     const double* Z, double* X, int n, cudaStream_t stream) {
-  if (count <= 0) return;
-  backward_kernel<<<count, kSolveThreads, 0, stream>>>(fronts, st, list, nrhs, Z, X, n);
 }
 void launch_residual(int n, int nrhs, const int* rowptr, const int* colind, const int* vidx, const double* vals,
                      const double* X, int ldx, const double* B, int ldb, double* R, cudaStream_t stream) {
