@@ -4,6 +4,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <stdexcept>
@@ -601,8 +602,13 @@ void launch_level(symla_gpu_ctx* c, const LevelLists& L, int level, const Kernel
     });
     for (int it = 0; it < L.panels; ++it) {
       timed(c, SYMLA_KERNEL_PANEL, 0.0, 0.0, [&] {
-        launch_panel(c->d_desc, c->d_state, d_large, static_cast<int>(L.large.size()), L.large_max_m, kPanelWidth,
-                     ko, c->d_glob, level, dynamic, st);
+        if (c->use_cluster_panel && cluster_size_for(L.large_max_m) > 0) {
+          CK(launch_cluster_panel(c->d_desc, c->d_state, d_large, static_cast<int>(L.large.size()), L.large_max_m,
+                                  kPanelWidth, ko, c->d_glob, level, dynamic, st));
+        } else {
+          launch_panel(c->d_desc, c->d_state, d_large, static_cast<int>(L.large.size()), L.large_max_m, kPanelWidth,
+                       ko, c->d_glob, level, dynamic, st);
+        }
       });
       const double tf = it < static_cast<int>(L.trailing_flops.size()) ? L.trailing_flops[it] : 0.0;
       timed(c, SYMLA_KERNEL_TRAILING, tf, 0.0, [&] {
@@ -1016,8 +1022,11 @@ extern "C" int symla_gpu_create(const symla_symbolic* sym, int n, const int* col
     static bool configured[64] = {};
     if (!configured[device]) {
       CK(configure_factor_kernels());
+      CK(configure_cluster_panel());
       configured[device] = true;
     }
+    const char* env = getenv("SYMLA_PANEL");
+    c->use_cluster_panel = !(env && std::string(env) == "single");
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     c->n = n;
     c->nnz = n > 0 ? colptr[n] : 0;

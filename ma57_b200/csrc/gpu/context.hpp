@@ -154,6 +154,9 @@ struct symla_gpu_ctx {
   long long nnzL = 0;
   int last_precision = 0;
 
+  // panel kernel choice (the cluster kernel unless SYMLA_PANEL=single)
+  bool use_cluster_panel = true;
+
   // instrumentation
   bool profiling = false;
   long long launches = 0;

@@ -23,6 +23,13 @@ void launch_factor_small(const FrontDesc* fronts, const ChildLink* links, FrontS
                          cudaStream_t stream);
 void launch_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m, int nb,
                   const KernelOpts& o, FactorGlobals* g, int level, int dynamic, cudaStream_t stream);
+// Cluster panel (panel_cluster.cu): returns 0 from cluster_size_for when a
+// front is too large for it (the single-CTA panel kernel then runs).
+int cluster_size_for(int max_m);
+cudaError_t configure_cluster_panel();
+cudaError_t launch_cluster_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m,
+                                 int nb, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
+                                 cudaStream_t stream);
 void launch_trailing(const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
                      const FactorGlobals* g, int level, int dynamic, cudaStream_t stream);
 

@@ -1,0 +1,556 @@
+// Panel factorization of large fronts by a thread-block cluster.
+//
+// One cluster of CS CTAs (8 or 16) factors up to NB pivots of one front.
+// The rows [ps, m) of the front are split into CS contiguous slices; CTA q
+// keeps, in its shared memory, the panel's L values of its rows (one column
+// per pivot of the panel) and the current values of the candidate columns.
+// Per pivot every CTA brings its rows of column k up to date
+// (raw - L_panel * D * L_panel(k, :)^T, dense_kernel.hpp:516-545), reduces
+// its part of the eligible-row argmax, and the partial results are exchanged
+// through distributed shared memory; every CTA then takes the same
+// Bunch-Kaufman decision (dense_kernel.hpp:576-793). Two cluster barriers per
+// pivot in the common (1x1 at k) case.
+//
+// The front in global memory holds the panel-start ("raw") values of every
+// non-pivoted column; row/column interchanges are applied to it and to the
+// shared-memory copies. The trailing update of the panel follows in
+// trailing_update_kernel.
+#include <cooperative_groups.h>
+
+#include <cmath>
+
+#include "common.cuh"
+#include "factor_kernels.h"
+#include "reduce.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace symla_gpu {
+
+namespace {
+
+constexpr double kAlphaBK = 0.64038820320220756;  // (1 + sqrt(17)) / 8
+constexpr int kCT = 256;                           // threads per CTA
+constexpr int kNBMax = 34;                         // panel width + 2
+
+struct ClusterShared {
+  double w[kNBMax];     // D * L(k, :)^T for the current pivot row
+  double wr[kNBMax];    // D * L(r, :)^T for the partner row
+  double Dd[kNBMax], Do[kNBMax];
+  int pk[kNBMax];
+  double ex_v[16];      // per-CTA partial maxima
+  int ex_i[16];         // per-CTA argmax rows
+  double ex_x[4];       // values broadcast by the owner of a row
+  double red_v[kCT / 32];
+  int red_i[kCT / 32];
+  double rowtmp[kNBMax];  // D * L(row, :) staging
+  double rowA[kNBMax], rowB[kNBMax];  // row interchange staging
+  double vA[2], vB[2];
+};
+
+}  // namespace
+
+template <int CS>
+__global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
+                                                            const int* __restrict__ front_list, int nb, int R,
+                                                            KernelOpts o, FactorGlobals* g, int level, int dynamic) {
+  if (!dynamic && g->delay_level < level) return;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int q = static_cast<int>(cluster.block_rank());
+  const int s = front_list[blockIdx.x / CS];
+  const FrontDesc f = fronts[s];
+  FrontState S = st[s];
+  if (S.flags & kFlagDone) {
+    if (q == 0 && threadIdx.x == 0) st[s].panel_start = S.k;
+    return;
+  }
+  extern __shared__ double dsm[];
+  __shared__ ClusterShared sh;
+  const int m = f.m, effEnd = f.nelig;
+  const int64_t ld = f.ld;
+  double* F = f.F;
+  const int ps = S.k;
+  const int pe = ps + min(nb, effEnd - ps);
+  const int span = m - ps;
+  const int Rr = (span + CS - 1) / CS;  // rows per CTA (<= R)
+  const int base = ps + q * Rr;
+  const int rend = min(base + Rr, m);
+  double* Lr = dsm;                 // column-major: Lr[col * R + li]
+  double* vk = dsm + static_cast<size_t>(nb + 2) * R;
+  double* vr = vk + R;
+
+  auto owner = [&](int i) { return (i - ps) / Rr; };
+  auto remote = [&](auto* p, int rank) { return cluster.map_shared_rank(p, rank); };
+
+  // ---- orig_max over the whole front at the first panel (cluster-wide)
+  if (ps == 0) {
+    double tmax = 0.0;
+    for (int j = q; j < m; j += CS)
+      for (int i = j + threadIdx.x; i < m; i += kCT) tmax = fmax(tmax, fabs(F[j * ld + i]));
+    tmax = block_max<kCT>(tmax, sh.red_v);
+    if (threadIdx.x == 0)
+      for (int d = 0; d < CS; ++d) remote(sh.ex_v, d)[q] = tmax;
+    cluster.sync();
+    double om = 0.0;
+    for (int d = 0; d < CS; ++d) om = fmax(om, sh.ex_v[d]);
+    if (o.mode == 1) {
+      if (om < o.static_abs_floor) om = 1.0;
+    } else {
+      if (om < o.zero_tol) om = 1.0;
+    }
+    S.orig_max = om;
+    S.running_max = om;
+    S.n_pos = S.n_neg = S.n_zero = 0;
+    S.num_perturbed = 0;
+    S.perturb = 0.0;
+    S.delta = o.front_delta ? o.front_delta[s] : (o.static_delta > 0.0 ? o.static_delta : 1.4901161193847656e-08 * om);
+    cluster.sync();
+  }
+  const double orig_max = S.orig_max;
+  int n_pos = S.n_pos, n_neg = S.n_neg, n_zero = S.n_zero, nPert = S.num_perturbed;
+  double pert = S.perturb;
+  double thread_rmax = 0.0;
+  double rm_known = S.running_max;
+
+  // compute current values of column `col` for this CTA's rows >= k
+  auto current_column = [&](int col, int k, int p, const double* w, double* v) {
+    for (int i = max(base, k) + threadIdx.x; i < rend; i += kCT) {
+      const int li = i - base;
+      const double raw = (i >= col) ? F[col * ld + i] : F[i * ld + col];
+      double acc = 0.0;
+      for (int t = 0; t < p; ++t) acc += Lr[t * R + li] * w[t];
+      v[li] = raw - acc;
+    }
+  };
+  // D * L(row, 0:p)^T from the owner's shared copy (block diagonal D)
+  auto d_times_row = [&](int row, int p, double* out) {
+    const int li = row - base;
+    for (int t = threadIdx.x; t < p; t += kCT) {
+      const int kind = sh.pk[t];
+      const double lt = Lr[t * R + li];
+      double v;
+      if (kind == 0)
+        v = sh.Dd[t] * lt;
+      else if (kind == 1)
+        v = sh.Dd[t] * lt + sh.Do[t] * Lr[(t + 1) * R + li];
+      else
+        v = sh.Do[t - 1] * Lr[(t - 1) * R + li] + sh.Dd[t] * lt;
+      out[t] = v;
+    }
+  };
+  // symmetric interchange of positions a < b: global front, row indices and
+  // the shared copies of both rows / current values
+  auto interchange = [&](int a, int b, bool swapVr) {
+    // global front: split the m-1 index range over the cluster
+    for (int t = q * kCT + threadIdx.x; t < m - 1; t += CS * kCT) {
+      if (t < a) {
+        const int c = t;
+        double x = F[c * ld + a];
+        F[c * ld + a] = F[c * ld + b];
+        F[c * ld + b] = x;
+      } else if (t < b - 1) {
+        const int c = t + 1;
+        double x = F[a * ld + c];
+        F[a * ld + c] = F[c * ld + b];
+        F[c * ld + b] = x;
+      } else if (t == b - 1) {
+        double x = F[a * ld + a];
+        F[a * ld + a] = F[b * ld + b];
+        F[b * ld + b] = x;
+      } else {
+        const int r = t + 1;
+        double x = F[a * ld + r];
+        F[a * ld + r] = F[b * ld + r];
+        F[b * ld + r] = x;
+      }
+    }
+    if (q == 0 && threadIdx.x == 0) {
+      int x = f.fidx[a];
+      f.fidx[a] = f.fidx[b];
+      f.fidx[b] = x;
+      x = f.lperm[a];
+      f.lperm[a] = f.lperm[b];
+      f.lperm[b] = x;
+    }
+    // shared copies: each owner stages the partner row (a CTA owning both
+    // rows stages both), then writes after a barrier
+    const int oa = owner(a), ob = owner(b);
+    auto stage_row = [&](int row, double* dst, double* vdst) {
+      const int oo = owner(row);
+      const int lo = row - (ps + oo * Rr);
+      double* Lo = remote(dsm, oo);
+      const double* vko = Lo + static_cast<size_t>(nb + 2) * R;
+      const double* vro = vko + R;
+      for (int t = threadIdx.x; t < nb + 2; t += kCT) dst[t] = Lo[static_cast<size_t>(t) * R + lo];
+      if (threadIdx.x == 0) {
+        vdst[0] = vko[lo];
+        vdst[1] = vro[lo];
+      }
+    };
+    if (q == oa) stage_row(b, sh.rowB, sh.vB);
+    if (q == ob) stage_row(a, sh.rowA, sh.vA);
+    __threadfence();
+    cluster.sync();
+    auto write_row = [&](int row, const double* src, const double* vsrc) {
+      const int li = row - base;
+      for (int t = threadIdx.x; t < nb + 2; t += kCT) Lr[static_cast<size_t>(t) * R + li] = src[t];
+      if (threadIdx.x == 0) {
+        vk[li] = vsrc[0];
+        if (swapVr) vr[li] = vsrc[1];
+      }
+    };
+    if (q == oa) write_row(a, sh.rowB, sh.vB);
+    if (q == ob) write_row(b, sh.rowA, sh.vA);
+    __threadfence();
+    cluster.sync();
+  };
+
+  int k = ps;
+  bool stopped = false;
+  // w for the first pivot of the panel: no panel columns yet
+  while (k < pe) {
+    const int p = k - ps;
+    // ---- column k
+    current_column(k, k, p, sh.w, vk);
+    if (o.mode == 1) {
+      // static pivoting (dense_kernel.hpp:982-1034): owner of k decides d
+      if (q == owner(k) && threadIdx.x == 0) {
+        const double akk = vk[k - base];
+        const int sign = o.sign_final ? o.sign_final[f.fidx[k]] : 0;
+        const double floorv = fmax(o.static_abs_floor, o.static_rel_floor * orig_max);
+        bool need;
+        if (sign > 0)
+          need = akk < floorv;
+        else if (sign < 0)
+          need = akk > -floorv;
+        else
+          need = fabs(akk) < floorv;
+        double d = akk, applied = 0.0;
+        if (need) {
+          const double sg = (sign != 0) ? static_cast<double>(sign) : (akk >= 0.0 ? 1.0 : -1.0);
+          d = akk + sg * S.delta;
+          applied = d - akk;
+        }
+        for (int dd = 0; dd < CS; ++dd) {
+          double* x = remote(sh.ex_x, dd);
+          x[0] = d;
+          x[1] = applied;
+        }
+      }
+      __syncthreads();
+      cluster.sync();
+      const double d = sh.ex_x[0], applied = sh.ex_x[1];
+      if (applied != 0.0) {
+        pert += fabs(applied);
+        ++nPert;
+      }
+      if (d > 0)
+        ++n_pos;
+      else if (d < 0)
+        ++n_neg;
+      else
+        ++n_zero;
+      thread_rmax = fmax(thread_rmax, fabs(d));
+      for (int i = max(base, k + 1) + threadIdx.x; i < rend; i += kCT) {
+        const int li = i - base;
+        const double a = vk[li];
+        thread_rmax = fmax(thread_rmax, fabs(a));
+        const double l = a / d;
+        Lr[p * R + li] = l;
+        F[k * ld + i] = l;
+      }
+      if (threadIdx.x == 0) {
+        sh.Dd[p] = d;
+        sh.Do[p] = 0.0;
+        sh.pk[p] = 0;
+      }
+      if (q == 0 && threadIdx.x == 0) {
+        F[k * ld + k] = d;
+        f.Dd[k] = d;
+        f.Do[k] = 0.0;
+        f.pk[k] = 0;
+      }
+      __syncthreads();
+      ++k;
+      if (k < pe) {
+        if (q == owner(k)) {
+          d_times_row(k, p + 1, sh.rowtmp);
+          __syncthreads();
+          for (int t = threadIdx.x; t < (p + 1) * CS; t += kCT) remote(sh.w, t / (p + 1))[t % (p + 1)] = sh.rowtmp[t % (p + 1)];
+        }
+        __threadfence();
+        cluster.sync();
+      }
+      continue;
+    }
+
+    // ---- threshold Bunch-Kaufman: lambda over the eligible rows
+    ArgMax am{0.0, -1};
+    for (int i = max(base, k + 1) + threadIdx.x; i < min(rend, effEnd); i += kCT)
+      am = argmax_combine(am, ArgMax{fabs(vk[i - base]), i});
+    am = block_argmax<kCT>(am, sh.red_v, sh.red_i);
+    if (threadIdx.x == 0) {
+      for (int dd = 0; dd < CS; ++dd) {
+        remote(sh.ex_v, dd)[q] = am.v;
+        remote(sh.ex_i, dd)[q] = am.i;
+      }
+      if (q == owner(k))
+        for (int dd = 0; dd < CS; ++dd) remote(sh.ex_x, dd)[0] = vk[k - base];
+    }
+    __threadfence();
+    cluster.sync();
+    ArgMax gm{sh.ex_v[0], sh.ex_i[0]};
+    for (int dd = 1; dd < CS; ++dd) gm = argmax_combine(gm, ArgMax{sh.ex_v[dd], sh.ex_i[dd]});
+    const double lambda = gm.v;
+    const int r = gm.i;
+    const double akk = sh.ex_x[0];
+    int dec;
+    double arr = 0.0, vkr = 0.0;
+    if (lambda <= o.zero_tol) {
+      const double isolatedFloor = fmax(o.zero_tol, o.rel_floor * orig_max);
+      dec = (fabs(akk) <= isolatedFloor) ? 3 : 0;
+    } else if (fabs(akk) >= kAlphaBK * lambda) {
+      dec = 0;
+    } else {
+      // partner column r
+      if (q == owner(r)) {
+        d_times_row(r, p, sh.rowtmp);
+        __syncthreads();
+        for (int t = threadIdx.x; t < p * CS; t += kCT) remote(sh.wr, t / p)[t % p] = sh.rowtmp[t % p];
+      }
+      __threadfence();
+      cluster.sync();
+      current_column(r, k, p, sh.wr, vr);
+      double smx = 0.0;
+      for (int i = max(base, k) + threadIdx.x; i < min(rend, effEnd); i += kCT)
+        if (i != r) smx = fmax(smx, fabs(vr[i - base]));
+      smx = block_max<kCT>(smx, sh.red_v);
+      if (threadIdx.x == 0) {
+        for (int dd = 0; dd < CS; ++dd) remote(sh.ex_v, dd)[q] = smx;
+        if (q == owner(r))
+          for (int dd = 0; dd < CS; ++dd) {
+            double* x = remote(sh.ex_x, dd);
+            x[1] = vr[r - base];
+            x[2] = vk[r - base];
+          }
+      }
+      __threadfence();
+      cluster.sync();
+      double sigma = 0.0;
+      for (int dd = 0; dd < CS; ++dd) sigma = fmax(sigma, sh.ex_v[dd]);
+      arr = sh.ex_x[1];
+      vkr = sh.ex_x[2];
+      if (fabs(akk) * sigma >= kAlphaBK * lambda * lambda)
+        dec = 0;
+      else if (fabs(arr) >= kAlphaBK * sigma)
+        dec = 1;
+      else
+        dec = 2;
+    }
+    if (dec == 3) {
+      stopped = true;
+      break;
+    }
+    if (dec == 0 || dec == 1) {
+      double d;
+      double* col;
+      if (dec == 1) {
+        // new column k = old column r with positions k, r exchanged
+        interchange(k, r, true);
+        // after the interchange vk holds old vk values moved, vr likewise;
+        // the pivot column is vr with entries k and r exchanged (done above)
+        col = vr;
+        d = arr;
+      } else {
+        col = vk;
+        d = akk;
+      }
+      if (d > 0)
+        ++n_pos;
+      else if (d < 0)
+        ++n_neg;
+      else
+        ++n_zero;
+      thread_rmax = fmax(thread_rmax, fabs(d));
+      for (int i = max(base, k + 1) + threadIdx.x; i < rend; i += kCT) {
+        const int li = i - base;
+        const double a = col[li];
+        thread_rmax = fmax(thread_rmax, fabs(a));
+        const double l = a / d;
+        Lr[p * R + li] = l;
+        F[k * ld + i] = l;
+      }
+      if (threadIdx.x == 0) {
+        sh.Dd[p] = d;
+        sh.Do[p] = 0.0;
+        sh.pk[p] = 0;
+      }
+      if (q == 0 && threadIdx.x == 0) {
+        F[k * ld + k] = d;
+        f.Dd[k] = d;
+        f.Do[k] = 0.0;
+        f.pk[k] = 0;
+      }
+      __syncthreads();
+      k += 1;
+    } else {
+      // 2x2 at (k, r): bring r to k+1
+      if (r != k + 1) interchange(k + 1, r, true);
+      const double d11 = akk, d21 = vkr, d22 = arr;
+      const double det = d11 * d22 - d21 * d21;
+      // cluster-uniform value (the running max known at panel start), so
+      // every thread takes the same branch
+      const double rm1 = fmax(1.0, rm_known);
+      if (fabs(det) <= o.zero_tol * rm1 * rm1) {
+        stopped = true;
+        break;
+      }
+      thread_rmax = fmax(thread_rmax, fmax(fabs(d11), fmax(fabs(d21), fabs(d22))));
+      if (det < 0) {
+        ++n_pos;
+        ++n_neg;
+      } else {
+        const double tr = d11 + d22;
+        if (tr > 0)
+          n_pos += 2;
+        else if (tr < 0)
+          n_neg += 2;
+        else {
+          ++n_pos;
+          ++n_neg;
+        }
+      }
+      const double inv11 = d22 / det, inv21 = -d21 / det, inv22 = d11 / det;
+      for (int i = max(base, k + 2) + threadIdx.x; i < rend; i += kCT) {
+        const int li = i - base;
+        const double a0 = vk[li], a1 = vr[li];
+        thread_rmax = fmax(thread_rmax, fmax(fabs(a0), fabs(a1)));
+        const double l0 = a0 * inv11 + a1 * inv21;
+        const double l1 = a0 * inv21 + a1 * inv22;
+        Lr[p * R + li] = l0;
+        Lr[(p + 1) * R + li] = l1;
+        F[k * ld + i] = l0;
+        F[(k + 1) * ld + i] = l1;
+      }
+      if (threadIdx.x == 0) {
+        sh.Dd[p] = d11;
+        sh.Dd[p + 1] = d22;
+        sh.Do[p] = d21;
+        sh.Do[p + 1] = 0.0;
+        sh.pk[p] = 1;
+        sh.pk[p + 1] = 2;
+      }
+      if (q == 0 && threadIdx.x == 0) {
+        F[k * ld + k] = d11;
+        F[k * ld + k + 1] = d21;
+        F[(k + 1) * ld + k + 1] = d22;
+        f.Dd[k] = d11;
+        f.Dd[k + 1] = d22;
+        f.Do[k] = d21;
+        f.Do[k + 1] = 0.0;
+        f.pk[k] = 1;
+        f.pk[k + 1] = 2;
+      }
+      __syncthreads();
+      k += 2;
+    }
+    // w for the next pivot row, from its owner
+    if (k < pe) {
+      const int pn = k - ps;
+      if (q == owner(k)) {
+        d_times_row(k, pn, sh.rowtmp);
+        __syncthreads();
+        for (int t = threadIdx.x; t < pn * CS; t += kCT) remote(sh.w, t / pn)[t % pn] = sh.rowtmp[t % pn];
+      }
+      __threadfence();
+      cluster.sync();
+    }
+  }
+
+  // ---- finish: cluster-wide running max; state written by rank 0
+  __threadfence();
+  const double lmax = block_max<kCT>(thread_rmax, sh.red_v);
+  cluster.sync();
+  if (threadIdx.x == 0)
+    for (int dd = 0; dd < CS; ++dd) remote(sh.ex_v, dd)[q] = lmax;
+  cluster.sync();
+  double rmax = 0.0;
+  for (int dd = 0; dd < CS; ++dd) rmax = fmax(rmax, sh.ex_v[dd]);
+  const bool done = stopped || k >= effEnd;
+  if (done)
+    for (int t = q * kCT + threadIdx.x; t < m; t += CS * kCT) f.lpos[f.lperm[t]] = t;
+  if (q == 0 && threadIdx.x == 0) {
+    FrontState& W = st[s];
+    W.orig_max = orig_max;
+    W.delta = S.delta;
+    W.running_max = fmax(S.running_max, rmax);
+    W.n_pos = n_pos;
+    W.n_neg = n_neg;
+    W.n_zero = n_zero;
+    W.num_perturbed = nPert;
+    W.perturb = pert;
+    W.panel_start = ps;
+    W.k = k;
+    W.npiv = k;
+    int flags = 0;
+    if (done) {
+      flags |= kFlagDone;
+      if (k < effEnd) {
+        if (f.parent >= 0) {
+          flags |= kFlagDelayed;
+          atomicMin(&g->delay_level, f.level);
+        } else {
+          flags |= kFlagSingularRoot;
+        }
+      } else if (k < m && f.parent < 0) {
+        flags |= kFlagSingularRoot;
+      }
+    }
+    W.flags = flags;
+  }
+  cluster.sync();
+}
+
+int cluster_size_for(int max_m) {
+  const size_t limit = 190 * 1024;
+  if (static_cast<size_t>((max_m + 7) / 8) * (kPanelWidth + 4) * sizeof(double) <= limit) return 8;
+  if (static_cast<size_t>((max_m + 15) / 16) * (kPanelWidth + 4) * sizeof(double) <= limit) return 16;
+  return 0;  // too large for the cluster kernel
+}
+
+size_t cluster_panel_smem(int max_m, int nb, int cs) {
+  const int R = (max_m + cs - 1) / cs;
+  return static_cast<size_t>(nb + 4) * R * sizeof(double);
+}
+
+cudaError_t configure_cluster_panel() {
+  cudaError_t e = cudaFuncSetAttribute(cluster_panel_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(cluster_panel_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(cluster_panel_kernel<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+
+cudaError_t launch_cluster_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m,
+                                 int nb, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
+                                 cudaStream_t stream) {
+  if (count <= 0) return cudaSuccess;
+  const int cs = cluster_size_for(max_m);
+  const int R = (max_m + cs - 1) / cs;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cs * count);
+  cfg.blockDim = dim3(kCT);
+  cfg.dynamicSmemBytes = cluster_panel_smem(max_m, nb, cs);
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (cs == 16) return cudaLaunchKernelEx(&cfg, cluster_panel_kernel<16>, fronts, st, list, nb, R, o, g, level, dynamic);
+  return cudaLaunchKernelEx(&cfg, cluster_panel_kernel<8>, fronts, st, list, nb, R, o, g, level, dynamic);
+}
+
+}  // namespace symla_gpu

@@ -207,3 +207,54 @@ def test_gpu_dense_random_matches_lapack_inertia(n):
     b = np.random.default_rng(n).standard_normal(n)
     x = s.solve(b)
     assert ref_residual(A0, x, b) < 1e-10
+
+
+def _dense_lower_csc(A0):
+    n = A0.shape[0]
+    ii, jj = np.tril_indices(n)
+    return sp.csc_matrix((A0[ii, jj], (ii, jj)), shape=(n, n))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n1,n2", [(120, 60), (400, 200)])
+def test_gpu_dense_static_large_front(n1, n2):
+    """One large front under Mode::StaticRegularized (the cluster panel's
+    static branch): SQD inertia (n2, n1, 0)."""
+    from ma57_b200 import Mode
+    st = np.random.default_rng(n1)
+    E = st.standard_normal((n1, n1))
+    E = E @ E.T / n1 + np.eye(n1)
+    Fm = st.standard_normal((n2, n2))
+    Fm = Fm @ Fm.T / n2 + np.eye(n2)
+    Ac = st.standard_normal((n2, n1)) * 0.3
+    K = np.block([[-E, Ac.T], [Ac, Fm]])
+    A = _dense_lower_csc(K)
+    s = SymLDLT()
+    s.setOrdering(OrderingType.Natural)
+    s.setMode(Mode.StaticRegularized)
+    s.setKKTBlockSizes(n1, n2)
+    s.analyzePattern(A)
+    s.factorize(A)
+    assert s.inertia().as_tuple() == (n2, n1, 0)
+    b = st.standard_normal(n1 + n2)
+    assert ref_residual(K, s.solve(b), b) < 1e-10
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,z", [(300, 20), (700, 5)])
+def test_gpu_large_front_singular_tail(n, z):
+    """A large single front whose last z rows/columns are zero: those columns
+    can never pivot (delayed at the root -> singular), the rest factor."""
+    A0 = random_symmetric_indefinite_eig(n - z, 90 + n)
+    K = np.zeros((n, n))
+    K[: n - z, : n - z] = A0
+    A = _dense_lower_csc(K + np.diag(np.r_[np.zeros(n - z), np.zeros(z)]))
+    s = SymLDLT()
+    s.setOrdering(OrderingType.Natural)
+    s.analyzePattern(A)
+    s.factorize(A)
+    assert s.isSingular()
+    assert sorted(s.singularColumns()) == list(range(n - z, n))
+    _, ref = dense_factor(A0)
+    i = s.inertia().as_tuple()
+    assert i[:2] == ref["inertia"][:2]
