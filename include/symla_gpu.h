@@ -228,12 +228,14 @@ int symla_gpu_phase_ms(symla_gpu_ctx* ctx, float* ms, int cap);
 /* Kernel instrumentation. When enabled, every launch of the library's
  * kernels is bracketed by CUDA events on the context's stream; per kernel
  * kind the launch count, summed device time and algorithmic work are kept
- * until reset. Kinds: 0 trailing (Schur) update, 1 panel factorization,
- * 2 small-front kernel, 3 assembly, 4 forward solve, 5 backward solve,
- * 6 residual. out[0] launches, out[1] total ms, out[2] algorithmic flops,
- * out[3] algorithmic bytes. */
+ * until reset. Kinds: 0 far (deferred, outer-block) Schur-complement update,
+ * 1 panel factorization, 2 small-front kernel, 3 assembly, 4 forward solve,
+ * 5 backward solve, 6 residual, 7 near (in-block) Schur-complement update.
+ * out[0] launches, out[1] total ms, out[2] algorithmic flops, out[3]
+ * algorithmic bytes. */
 enum { SYMLA_KERNEL_TRAILING = 0, SYMLA_KERNEL_PANEL = 1, SYMLA_KERNEL_SMALL = 2, SYMLA_KERNEL_ASSEMBLE = 3,
-       SYMLA_KERNEL_FORWARD = 4, SYMLA_KERNEL_BACKWARD = 5, SYMLA_KERNEL_RESIDUAL = 6, SYMLA_KERNEL_KINDS = 7 };
+       SYMLA_KERNEL_FORWARD = 4, SYMLA_KERNEL_BACKWARD = 5, SYMLA_KERNEL_RESIDUAL = 6, SYMLA_KERNEL_NEAR = 7,
+       SYMLA_KERNEL_KINDS = 8 };
 int symla_gpu_set_profiling(symla_gpu_ctx* ctx, int enable);
 int symla_gpu_kernel_stats(symla_gpu_ctx* ctx, int kind, double* out4);
 void symla_gpu_reset_kernel_stats(symla_gpu_ctx* ctx);

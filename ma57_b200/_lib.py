@@ -100,7 +100,7 @@ _SIGS = {
     "symla_gpu_launch_count": (C.c_longlong, [_p]),
 }
 
-KERNEL_KINDS = ["trailing", "panel", "small", "assemble", "forward", "backward", "residual"]
+KERNEL_KINDS = ["far_update", "panel", "small", "assemble", "forward", "backward", "residual", "near_update"]
 
 # Every symbol declared in include/symla_gpu.h that is a function.
 EXPORTED = tuple(_SIGS.keys())

@@ -70,7 +70,9 @@ def build(verbose: bool = False, force: bool = False) -> Path:
             _run(cmd)
     metis = CUDA_HOME / "lib64" / "libmetis_static.a"
     if force or _stale(LIB, objs):
-        _run([NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), str(metis), "-lcudart_static"])
+        # --no-undefined: a missing symbol fails the build, not the first dlopen
+        _run([NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), str(metis), "-lcudart_static",
+              "-Xlinker", "--no-undefined"])
     return LIB
 
 

@@ -268,13 +268,13 @@ void build_level_lists(symla_gpu_ctx* c, const std::vector<int>& frontsOfLevel, 
       }
       L.assemble_bytes += 8.0 * (cbsum + static_cast<double>(f.m) * (f.m + 1) / 2.0);
       const int mt = std::max(0, f.m - std::min(f.nelig, kPanelWidth));
-      const int nt = (mt + 63) / 64;
+      const int nt = (mt + 127) / 128;
       tiles = std::max(tiles, nt * (nt + 1) / 2);
     }
   }
   if (!L.large.empty()) {
-    const int budget = std::max(1, 148 * 6 / static_cast<int>(L.large.size()));
-    L.trailing_grid = std::max(1, std::min(tiles, budget));
+    // one grid over the tiles of every front of the level (one CTA per SM)
+    L.trailing_grid = std::max(1, std::min(tiles * static_cast<int>(L.large.size()), 148));
   } else {
     L.trailing_grid = 0;
   }
@@ -587,6 +587,27 @@ KernelOpts make_kernel_opts(symla_gpu_ctx* c, const symla_factor_opts* o) {
   return k;
 }
 
+void launch_panel_iteration(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
+                            const int* d_large) {
+  cudaStream_t st = c->stream;
+  const int nl = static_cast<int>(L.large.size());
+  timed(c, SYMLA_KERNEL_PANEL, 0.0, 0.0, [&] {
+    if (c->use_cluster_panel && cluster_size_for(L.large_max_m) > 0) {
+      CK(launch_cluster_panel(c->d_desc, c->d_state, d_large, nl, L.large_max_m, kPanelWidth, ko, c->d_glob, level,
+                              dynamic, st));
+    } else {
+      launch_panel(c->d_desc, c->d_state, d_large, nl, L.large_max_m, kPanelWidth, ko, c->d_glob, level, dynamic,
+                   st);
+    }
+  });
+  timed(c, SYMLA_KERNEL_NEAR, 0.0, 0.0, [&] {
+    launch_update(false, c->d_desc, c->d_state, d_large, nl, L.trailing_grid, c->d_glob, level, dynamic, st);
+  });
+  timed(c, SYMLA_KERNEL_TRAILING, 0.0, 0.0, [&] {
+    launch_update(true, c->d_desc, c->d_state, d_large, nl, L.trailing_grid, c->d_glob, level, dynamic, st);
+  });
+}
+
 void launch_level(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
                   const int* d_small, const int* d_large, const int* d_tasks) {
   cudaStream_t st = c->stream;
@@ -600,21 +621,23 @@ void launch_level(symla_gpu_ctx* c, const LevelLists& L, int level, const Kernel
       launch_assemble(c->d_desc, c->d_links, c->d_state, d_tasks, static_cast<int>(L.tasks.size() / 2),
                       c->d_a_colptr, ko, c->d_glob, level, dynamic, st);
     });
-    for (int it = 0; it < L.panels; ++it) {
-      timed(c, SYMLA_KERNEL_PANEL, 0.0, 0.0, [&] {
-        if (c->use_cluster_panel && cluster_size_for(L.large_max_m) > 0) {
-          CK(launch_cluster_panel(c->d_desc, c->d_state, d_large, static_cast<int>(L.large.size()), L.large_max_m,
-                                  kPanelWidth, ko, c->d_glob, level, dynamic, st));
-        } else {
-          launch_panel(c->d_desc, c->d_state, d_large, static_cast<int>(L.large.size()), L.large_max_m, kPanelWidth,
-                       ko, c->d_glob, level, dynamic, st);
-        }
-      });
-      const double tf = it < static_cast<int>(L.trailing_flops.size()) ? L.trailing_flops[it] : 0.0;
-      timed(c, SYMLA_KERNEL_TRAILING, tf, 0.0, [&] {
-        launch_trailing(c->d_desc, c->d_state, d_large, static_cast<int>(L.large.size()), L.trailing_grid, c->d_glob,
-                        level, dynamic, st);
-      });
+    for (int it = 0; it < L.panels; ++it) launch_panel_iteration(c, L, level, ko, dynamic, d_large);
+    // Flushes (a partner beyond the outer block) and 2x2 pivots can leave a
+    // front unfinished after the planned iterations: run more until done.
+    const int nl = static_cast<int>(L.large.size());
+    int guard = 0;
+    for (;;) {
+      int unfinished = 0;
+      CK(cudaMemsetAsync(c->d_counter, 0, sizeof(int), st));
+      launch_count_unfinished(c->d_state, d_large, nl, c->d_counter, st);
+      CK(cudaMemcpyAsync(&unfinished, c->d_counter, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (unfinished == 0) break;
+      FactorGlobals gl;
+      CK(cudaMemcpy(&gl, c->d_glob, sizeof gl, cudaMemcpyDeviceToHost));
+      if (!dynamic && gl.delay_level < level) break;  // aborted level, re-run by the delay path
+      if (++guard > 4 * L.panels + 64) throw SymlaError(SYMLA_ERR_INTERNAL, "large front did not finish");
+      for (int it = 0; it < 4; ++it) launch_panel_iteration(c, L, level, ko, dynamic, d_large);
     }
   }
   CK(cudaGetLastError());
@@ -733,7 +756,7 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
   reset_to_static(c);
   const KernelOpts ko = make_kernel_opts(c, o);
   CK(cudaMemsetAsync(c->d_state, 0, c->numSN * sizeof(FrontState), st));
-  FactorGlobals g0{INT_MAX, 0, -1, 0};
+  FactorGlobals g0{INT_MAX, 0, -1, 0, 0.0, 0.0};
   CK(cudaMemcpyAsync(c->d_glob, &g0, sizeof g0, cudaMemcpyHostToDevice, st));
   CK(cudaEventRecord(c->ev[0], st));
   for (int l = 0; l < c->numLevels; ++l) {
@@ -767,6 +790,12 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
   CK(cudaEventRecord(c->ev[1], st));
   CK(cudaEventSynchronize(c->ev[1]));
   collect_pending(c);
+  if (c->profiling) {
+    FactorGlobals gf;
+    CK(cudaMemcpy(&gf, c->d_glob, sizeof gf, cudaMemcpyDeviceToHost));
+    c->kstat[SYMLA_KERNEL_TRAILING].flops += gf.flops_far;
+    c->kstat[SYMLA_KERNEL_NEAR].flops += gf.flops_near;
+  }
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
   if (!dynamic) read_states(c);
@@ -1032,6 +1061,7 @@ extern "C" int symla_gpu_create(const symla_symbolic* sym, int n, const int* col
     c->nnz = n > 0 ? colptr[n] : 0;
     CK(solve_max_resident(device, &c->fwd_resident, &c->bwd_resident));
     c->d_solve_err = dalloc<int>(1);
+    c->d_counter = dalloc<int>(1);
     CK(cudaMemsetAsync(c->d_solve_err, 0, sizeof(int), c->stream));
     build_plan(c, sym->sf, colptr, rowind);
   });
@@ -1052,7 +1082,7 @@ extern "C" void symla_gpu_destroy(symla_gpu_ctx* c) {
                   c->d_glob, c->d_a_colptr, c->d_a_j, c->d_a_pos, c->d_a_idx, c->d_values, c->d_sign_final,
                   c->d_front_delta, c->d_perm, c->d_rowptr, c->d_colind, c->d_vidx, c->d_srowptr, c->d_svidx, c->d_W,
                   c->d_Bp, c->d_Z, c->d_Xf, c->d_B, c->d_X, c->d_R, c->d_dX, c->d_Xn, c->d_Rn, c->d_norms,
-                  c->d_scratch_int, c->d_flag_base, c->d_flags, c->d_solve_err};
+                  c->d_scratch_int, c->d_flag_base, c->d_flags, c->d_solve_err, c->d_counter};
   for (void* p : ptrs) dfree(p);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);

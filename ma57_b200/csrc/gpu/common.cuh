@@ -43,13 +43,19 @@ struct FrontState {
   int num_perturbed;
   int k;           // next column (panel driver progress)
   int panel_start; // first column of the panel in flight
+  int ob, ob_end;  // outer block [ob, ob_end): its pivots' update of the
+                   // columns beyond ob_end is deferred to one far update
+  int far;         // 1: the far update of [ob, k) is due after this panel
   double perturb;
   double orig_max;
   double running_max;
   double delta;    // static pivoting delta used for this front
 };
 
-enum : int { kFlagDone = 1, kFlagDelayed = 2, kFlagSingularRoot = 4 };
+enum : int { kFlagDone = 1, kFlagDelayed = 2, kFlagSingularRoot = 4, kFlagFlush = 8 };
+
+// Columns per outer block of the large-front factorization.
+constexpr int kOuterBlock = 128;
 
 // Error word of the pipelined solve kernels.
 constexpr int kSolveErrTimeout = 1;
@@ -60,6 +66,8 @@ struct FactorGlobals {
   int error;           // nonzero: internal error code
   int err_front;
   int pad;
+  double flops_near;   // algorithmic flops of the near (in-block) updates
+  double flops_far;    // algorithmic flops of the far (deferred) updates
 };
 
 // Options visible to kernels.

@@ -133,6 +133,7 @@ struct symla_gpu_ctx {
   int* d_flag_base = nullptr;
   int* d_flags = nullptr;
   int* d_solve_err = nullptr;
+  int* d_counter = nullptr;  // unfinished-front counter
   int flag_count = 0;
   int solve_epoch = 0;
   int fwd_resident = 0, bwd_resident = 0;
@@ -163,7 +164,7 @@ struct symla_gpu_ctx {
   struct KStat {
     long long launches = 0;
     double ms = 0.0, flops = 0.0, bytes = 0.0;
-  } kstat[7];
+  } kstat[8];
   struct PendingEv {
     cudaEvent_t a, b;
     int kind;

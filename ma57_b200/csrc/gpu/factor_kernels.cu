@@ -64,7 +64,7 @@ __device__ __forceinline__ int a_local_row(int pos, int ncols, int nextra) {
 // columns are added.
 __global__ void __launch_bounds__(256) assemble_kernel(const FrontDesc* __restrict__ fronts,
                                                        const ChildLink* __restrict__ links,
-                                                       const FrontState* __restrict__ st, const int* __restrict__ tasks,
+                                                       FrontState* st, const int* __restrict__ tasks,
                                                        const int* __restrict__ a_colptr, KernelOpts o,
                                                        const FactorGlobals* __restrict__ g, int level, int dynamic) {
   if (level_aborted(g, level, dynamic)) return;
@@ -88,6 +88,16 @@ __global__ void __launch_bounds__(256) assemble_kernel(const FrontDesc* __restri
       f.F[static_cast<int64_t>(j) * f.ld + i] += o.values[o.a_idx[e]];
     }
   }
+  // max |entry| of the assembled front (dense_kernel.hpp:413), folded here
+  // so the panel kernel does not rescan the front
+  __syncthreads();
+  double tmax = 0.0;
+  for (int j = j0; j < j1; ++j) {
+    const double* col = f.F + static_cast<int64_t>(j) * f.ld;
+    for (int i = j + threadIdx.x; i < f.m; i += blockDim.x) tmax = fmax(tmax, fabs(col[i]));
+  }
+  tmax = warp_max(tmax);
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&st[s].orig_max, tmax);
 }
 
 // ---------------------------------------------------------------------------
@@ -518,21 +528,27 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* _
   const FrontDesc f = fronts[s];
   FrontState S = st[s];
   if (S.flags & kFlagDone) {
-    // no panel this round: the trailing update that follows must do nothing
-    if (threadIdx.x == 0) st[s].panel_start = S.k;
+    // no panel this round: the updates that follow must do nothing
+    if (threadIdx.x == 0) {
+      st[s].panel_start = S.k;
+      st[s].far = 0;
+    }
     return;
+  }
+  if (S.ob_end == 0 || S.far) {
+    S.ob = S.k;
+    S.ob_end = min(S.k + kOuterBlock, f.nelig);
+    S.far = 0;
+    S.flags &= ~kFlagFlush;
   }
   const int m = f.m;
   const int effEnd = f.nelig;
   double* colk = smem;
   double* colr = smem + m;
 
-  // First panel: orig_max over the assembled front.
+  // First panel: orig_max of the assembled front (from the assembly kernel).
   if (S.k == 0) {
-    double tmax = 0.0;
-    for (int j = 0; j < m; ++j)
-      for (int i = j + threadIdx.x; i < m; i += NT) tmax = fmax(tmax, fabs(f.F[static_cast<int64_t>(j) * f.ld + i]));
-    double om = block_max<NT>(tmax, red_v);
+    double om = S.orig_max;
     if (o.mode == 1) {
       if (om < o.static_abs_floor) om = 1.0;
     } else {
@@ -548,9 +564,10 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* _
   const double orig_max = S.orig_max;
   int k = S.k;
   const int ps = k;
-  const int pe = ps + min(nb, effEnd - ps);
+  const int pe = ps + min(nb, S.ob_end - ps);
   double thread_rmax = 0.0;
   bool stopped = false;
+  bool flush = false;
   int n_pos = S.n_pos, n_neg = S.n_neg, n_zero = S.n_zero, nPert = S.num_perturbed;
   double pert = S.perturb;
 
@@ -612,6 +629,8 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* _
       dec = (fabs(akk) <= isolatedFloor) ? 3 : 0;
     } else if (fabs(akk) >= kAlpha * lambda) {
       dec = 0;
+    } else if (r >= S.ob_end && ps > S.ob) {
+      dec = 4;  // partner beyond the outer block: apply the deferred update first
     } else {
       panel_current_column(f, ps, p, k, r, colr, wbuf);
       double sm = 0.0;
@@ -627,6 +646,10 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* _
     }
     if (dec == 3) {
       stopped = true;
+      break;
+    }
+    if (dec == 4) {
+      flush = true;
       break;
     }
     __syncthreads();
@@ -727,6 +750,7 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* _
   const double rmax = block_max<NT>(thread_rmax, red_v);
   if (stopped || k >= effEnd)
     for (int t = threadIdx.x; t < m; t += NT) f.lpos[f.lperm[t]] = t;
+  __syncthreads();
   if (threadIdx.x == 0) {
     FrontState& W = st[s];
     W.orig_max = orig_max;
@@ -740,7 +764,10 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* _
     W.panel_start = ps;
     W.k = k;
     W.npiv = k;
-    int flags = 0;
+    W.ob = S.ob;
+    W.ob_end = S.ob_end;
+    W.far = (stopped || k >= effEnd || flush || k >= S.ob_end) ? 1 : 0;
+    int flags = flush ? kFlagFlush : 0;
     if (stopped || k >= effEnd) {
       flags |= kFlagDone;
       if (k < effEnd) {
@@ -759,97 +786,224 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* _
 }
 
 // ---------------------------------------------------------------------------
-// Trailing update T(k1:m, k1:m) -= L(k1:m, ps:k1) * (L D)(k1:m, ps:k1)^T on
-// the lower triangle, FP64, 64x64 tiles, K = panel width (<= NB+1).
+// Schur-complement updates of a large front, FP64:
+//   near (after every panel): columns [k1, ob_end) of the outer block,
+//        pivots [ps, k1) of the panel;
+//   far  (after an outer block, a flush or the last panel): columns
+//        [max(ob_end, k1), m), pivots [ob, k1) of the whole block.
+// C(i, j) -= sum_q L(i, q) (L D)(j, q) for i >= j. 128 x 128 tiles, 256
+// threads, 8 x 8 register blocks (rows tx + 16u, columns ty + 16v, so a
+// half-warp touches 16 consecutive rows of a column); the K range is staged
+// in shared memory 32 pivots at a time. The tile's C values are loaded
+// before the staging so their latency overlaps it.
 namespace {
-constexpr int kTT = 64;        // tile edge
-constexpr int kTThreads = 256;  // 16 x 16 threads, 4 x 4 outputs each
-constexpr int kKMax = 40;  // panel width + 1 (2x2 straddle) <= 40
+constexpr int kTT = 128;        // tile edge
+constexpr int kTThreads = 256;  // 16 x 16 threads, 8 x 8 outputs each
+constexpr int kKC = 32;         // K chunk
+constexpr int kMaxUpdateFronts = 1024;  // fronts per update launch
 }  // namespace
 
-__global__ void __launch_bounds__(kTThreads) trailing_update_kernel(const FrontDesc* __restrict__ fronts,
-                                                                    FrontState* st,
-                                                                    const int* __restrict__ front_list,
-                                                                    const FactorGlobals* __restrict__ g, int level,
-                                                                    int dynamic) {
+__device__ __forceinline__ bool update_range(const FrontState& S, int m, bool far, int& c0, int& c1, int& q0,
+                                             int& q1) {
+  if (!far) {
+    q0 = S.panel_start;
+    q1 = S.k;
+    c0 = S.k;
+    c1 = min(S.ob_end, m);
+  } else {
+    if (!S.far) return false;
+    q0 = S.ob;
+    q1 = S.k;
+    c0 = max(S.ob_end, S.k);
+    c1 = m;
+  }
+  return q1 > q0 && c1 > c0;
+}
+
+__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  const int n = valid ? 8 : 0;  // zero-fill rows beyond the front
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Stage pivots [kc, kc + kn) of rows i0.. (A side) and rows j0.. (B side,
+// with one halo column on each side for the 2x2 blocks of D) into smem.
+__device__ __forceinline__ void update_stage(const FrontDesc& f, int q0, int q1, int kc, int kn, int i0, int j0,
+                                             double* Ls, double* Lj) {
+  const int64_t ld = f.ld;
+  const int m = f.m;
+  for (int t = threadIdx.x; t < kn * kTT; t += kTThreads) {
+    const int q = t / kTT, r = t % kTT;
+    const int gi = i0 + r;
+    const double* src = f.F + (kc + q) * ld + (gi < m ? gi : 0);
+    cp_async8(Ls + q * kTT + r, src, gi < m);
+  }
+  for (int t = threadIdx.x; t < (kn + 2) * kTT; t += kTThreads) {
+    const int q = t / kTT - 1, r = t % kTT;
+    const int pq = kc + q;
+    const int gj = j0 + r;
+    const bool ok = gj < m && pq >= q0 && pq < q1;
+    const double* src = f.F + (ok ? pq * ld + gj : 0);
+    cp_async8(Lj + (q + 1) * kTT + r, src, ok);
+  }
+}
+
+// Tiles of front s's update region: column tiles over [c0, c1), each with
+// row tiles from its diagonal down to m.
+__device__ __forceinline__ int update_tiles(int m, int c0, int c1) {
+  int n = 0;
+  for (int j = c0; j < c1; j += kTT) n += (m - j + kTT - 1) / kTT;
+  return n;
+}
+
+template <bool FAR>
+__global__ void __launch_bounds__(kTThreads) update_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
+                                                           const int* __restrict__ front_list, int count,
+                                                           FactorGlobals* g, int level, int dynamic) {
   if (level_aborted(g, level, dynamic)) return;
-  __shared__ double Li[kKMax][kTT + 1];
-  __shared__ double Wj[kKMax][kTT + 1];
-  const int s = front_list[blockIdx.y];
-  const FrontDesc f = fronts[s];
-  const FrontState S = st[s];
-  const int ps = S.panel_start, k1 = S.k;
-  const int p = k1 - ps;
-  if (p <= 0) return;
-  const int mt = f.m - k1;
-  if (mt <= 0) return;
-  const int nt = (mt + kTT - 1) / kTT;
-  const int ntiles = nt * (nt + 1) / 2;
+  // two stages of {A rows (kKC x kTT), B rows with halo ((kKC+2) x kTT)} and
+  // one (L D) buffer (kKC x kTT)
+  extern __shared__ double usm[];
+  double* LsBuf[2] = {usm, usm + (2 * kKC + 2) * kTT};
+  double* LjBuf[2] = {usm + kKC * kTT, usm + (3 * kKC + 2) * kTT};
+  double* Wj = usm + (4 * kKC + 4) * kTT;
+  __shared__ double dd[kKC], dlo[kKC], dhi[kKC];
+  __shared__ int8_t kk[kKC];
+  __shared__ int tile_end[kMaxUpdateFronts];
+  // one tile space over every front of the launch, so idle fronts do not
+  // leave CTAs without work
+  for (int t = threadIdx.x; t < count; t += kTThreads) {
+    const int sf = front_list[t];
+    int c0, c1, q0, q1;
+    const FrontState S = st[sf];
+    tile_end[t] = update_range(S, fronts[sf].m, FAR, c0, c1, q0, q1) ? update_tiles(fronts[sf].m, c0, c1) : 0;
+    if (blockIdx.x == 0 && tile_end[t] > 0) {
+      const double nc = c1 - c0, mm = fronts[sf].m;
+      const double entries = nc * mm - (static_cast<double>(c0) + c1 - 1) * nc / 2.0;
+      atomicAdd(FAR ? &g->flops_far : &g->flops_near, 2.0 * (q1 - q0) * entries);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int t = 1; t < count; ++t) tile_end[t] += tile_end[t - 1];
+  __syncthreads();
+  const int total = count > 0 ? tile_end[count - 1] : 0;
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
   double tmax = 0.0;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    // tile -> (ti, tj), ti >= tj, column-major over the lower triangle
-    int tj = 0, rem = tile;
-    while (rem >= nt - tj) {
-      rem -= nt - tj;
+  int cur = -1, s = -1;
+  FrontDesc f;
+  int m = 0, c0 = 0, c1 = 0, q0 = 0, q1 = 0, nchunks = 0;
+  int64_t ld = 0;
+  for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
+    int fi = 0;
+    while (tile >= tile_end[fi]) ++fi;
+    if (fi != cur) {
+      if (cur >= 0) {
+        tmax = warp_max(tmax);
+        if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&st[s].running_max, tmax);
+        tmax = 0.0;
+      }
+      cur = fi;
+      s = front_list[fi];
+      f = fronts[s];
+      m = f.m;
+      ld = f.ld;
+      update_range(st[s], m, FAR, c0, c1, q0, q1);
+      nchunks = (q1 - q0 + kKC - 1) / kKC;
+    }
+    int rem = tile - (fi > 0 ? tile_end[fi - 1] : 0);
+    int tj = 0;
+    for (;;) {
+      const int nr = (m - (c0 + tj * kTT) + kTT - 1) / kTT;
+      if (rem < nr) break;
+      rem -= nr;
       ++tj;
     }
-    const int ti = tj + rem;
-    const int i0 = k1 + ti * kTT, j0 = k1 + tj * kTT;
-    __syncthreads();
-    for (int t = threadIdx.x; t < p * kTT; t += kTThreads) {
-      const int q = t / kTT, r = t % kTT;
-      const int pq = ps + q;
-      const int gi = i0 + r, gj = j0 + r;
-      Li[q][r] = (gi < f.m) ? f.F[static_cast<int64_t>(pq) * f.ld + gi] : 0.0;
-      double w = 0.0;
-      if (gj < f.m) {
+    const int j0 = c0 + tj * kTT, i0 = j0 + rem * kTT;
+    __syncthreads();  // previous tile done with the buffers
+    update_stage(f, q0, q1, q0, min(kKC, q1 - q0), i0, j0, LsBuf[0], LjBuf[0]);
+    cp_async_commit();
+    double acc[8][8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      const int gj = j0 + ty + 16 * v;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int gi = i0 + tx + 16 * u;
+        acc[u][v] = (gj < c1 && gi < m && gi >= gj) ? f.F[gj * ld + gi] : 0.0;
+      }
+    }
+    for (int c = 0; c < nchunks; ++c) {
+      const int kc = q0 + c * kKC, kn = min(kKC, q1 - kc);
+      if (c + 1 < nchunks) {
+        const int kc2 = kc + kKC;
+        update_stage(f, q0, q1, kc2, min(kKC, q1 - kc2), i0, j0, LsBuf[(c + 1) & 1], LjBuf[(c + 1) & 1]);
+      }
+      cp_async_commit();
+      if (threadIdx.x < kn) {
+        const int pq = kc + threadIdx.x;
         const int8_t kind = f.pk[pq];
-        const double lq = f.F[static_cast<int64_t>(pq) * f.ld + gj];
-        if (kind == 0)
-          w = f.Dd[pq] * lq;
-        else if (kind == 1)
-          w = f.Dd[pq] * lq + f.Do[pq] * f.F[static_cast<int64_t>(pq + 1) * f.ld + gj];
-        else
-          w = f.Do[pq - 1] * f.F[static_cast<int64_t>(pq - 1) * f.ld + gj] + f.Dd[pq] * lq;
+        kk[threadIdx.x] = kind;
+        dd[threadIdx.x] = f.Dd[pq];
+        dlo[threadIdx.x] = (kind == 2) ? f.Do[pq - 1] : 0.0;
+        dhi[threadIdx.x] = (kind == 1) ? f.Do[pq] : 0.0;
       }
-      Wj[q][r] = w;
-    }
-    __syncthreads();
-    double acc[4][4] = {};
-    for (int q = 0; q < p; ++q) {
-      double a[4], b[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        a[u] = Li[q][ty + 16 * u];
-        b[u] = Wj[q][tx + 16 * u];
+      cp_async_wait<1>();
+      __syncthreads();
+      const double* Ls = LsBuf[c & 1];
+      const double* Lj = LjBuf[c & 1];
+      // (L D)(j, q) from the staged L rows of the B side and D's blocks
+      for (int t = threadIdx.x; t < kn * kTT; t += kTThreads) {
+        const int q = t / kTT, r = t % kTT;
+        const double* col = Lj + (q + 1) * kTT + r;
+        double w = dd[q] * col[0];
+        if (kk[q] == 1) w += dhi[q] * col[kTT];
+        if (kk[q] == 2) w += dlo[q] * col[-kTT];
+        Wj[q * kTT + r] = w;
       }
+      __syncthreads();
+      for (int q = 0; q < kn; ++q) {
+        double a[8], b[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < 8; ++u) {
+          a[u] = Ls[q * kTT + tx + 16 * u];
+          b[u] = Wj[q * kTT + ty + 16 * u];
+        }
 #pragma unroll
-        for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+          for (int v = 0; v < 8; ++v) acc[u][v] = fma(-a[u], b[v], acc[u][v]);
+      }
+      __syncthreads();
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+    for (int v = 0; v < 8; ++v) {
+      const int gj = j0 + ty + 16 * v;
 #pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const int gi = i0 + ty + 16 * u, gj = j0 + tx + 16 * v;
-        if (gi < f.m && gj < f.m && gi >= gj) {
-          double* c = f.F + static_cast<int64_t>(gj) * f.ld + gi;
-          const double nv = *c - acc[u][v];
-          *c = nv;
-          tmax = fmax(tmax, fabs(nv));
+      for (int u = 0; u < 8; ++u) {
+        const int gi = i0 + tx + 16 * u;
+        if (gj < c1 && gi < m && gi >= gj) {
+          f.F[gj * ld + gi] = acc[u][v];
+          tmax = fmax(tmax, fabs(acc[u][v]));
         }
       }
+    }
   }
-  tmax = warp_max(tmax);
-  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&st[s].running_max, tmax);
+  if (cur >= 0) {
+    tmax = warp_max(tmax);
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&st[s].running_max, tmax);
+  }
 }
 
 // ---------------------------------------------------------------------------
 // Host launchers
 
-void launch_assemble(const FrontDesc* fronts, const ChildLink* links, const FrontState* st, const int* tasks,
+void launch_assemble(const FrontDesc* fronts, const ChildLink* links, FrontState* st, const int* tasks,
                      int ntasks, const int* a_colptr, const KernelOpts& o, const FactorGlobals* g, int level,
                      int dynamic, cudaStream_t stream) {
   if (ntasks <= 0) return;
@@ -879,11 +1033,32 @@ void launch_panel(const FrontDesc* fronts, FrontState* st, const int* list, int 
   panel_kernel<<<count, kPanelThreads, sm, stream>>>(fronts, st, list, nb, o, g, level, dynamic);
 }
 
-void launch_trailing(const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
-                     const FactorGlobals* g, int level, int dynamic, cudaStream_t stream) {
+
+__global__ void count_unfinished_kernel(const FrontState* __restrict__ st, const int* __restrict__ list, int count,
+                                        int* out) {
+  int c = 0;
+  for (int t = threadIdx.x; t < count; t += blockDim.x)
+    if (!(st[list[t]].flags & kFlagDone)) ++c;
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+void launch_count_unfinished(const FrontState* st, const int* list, int count, int* out, cudaStream_t stream) {
+  if (count <= 0) return;
+  count_unfinished_kernel<<<1, 256, 0, stream>>>(st, list, count, out);
+}
+
+void launch_update(bool far, const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
+                   FactorGlobals* g, int level, int dynamic, cudaStream_t stream) {
   if (count <= 0 || grid_x <= 0) return;
-  dim3 grid(grid_x, count);
-  trailing_update_kernel<<<grid, kTThreads, 0, stream>>>(fronts, st, list, g, level, dynamic);
+  const size_t sm = static_cast<size_t>(5 * kKC + 4) * kTT * sizeof(double);
+  for (int b = 0; b < count; b += kMaxUpdateFronts) {
+    const int cnt = count - b < kMaxUpdateFronts ? count - b : kMaxUpdateFronts;
+    if (far)
+      update_kernel<true><<<grid_x, kTThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic);
+    else
+      update_kernel<false><<<grid_x, kTThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic);
+  }
 }
 
 cudaError_t configure_factor_kernels() {
@@ -893,6 +1068,10 @@ cudaError_t configure_factor_kernels() {
   e = cudaFuncSetAttribute(factor_small_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(update_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   return e;
 }
 

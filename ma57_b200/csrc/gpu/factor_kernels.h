@@ -15,7 +15,7 @@ constexpr int kPanelWidth = 32;
 cudaError_t configure_factor_kernels();
 size_t small_front_smem(int m);
 
-void launch_assemble(const FrontDesc* fronts, const ChildLink* links, const FrontState* st, const int* tasks,
+void launch_assemble(const FrontDesc* fronts, const ChildLink* links, FrontState* st, const int* tasks,
                      int ntasks, const int* a_colptr, const KernelOpts& o, const FactorGlobals* g, int level,
                      int dynamic, cudaStream_t stream);
 void launch_factor_small(const FrontDesc* fronts, const ChildLink* links, FrontState* st, const int* list, int count,
@@ -30,8 +30,11 @@ cudaError_t configure_cluster_panel();
 cudaError_t launch_cluster_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m,
                                  int nb, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
                                  cudaStream_t stream);
-void launch_trailing(const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
-                     const FactorGlobals* g, int level, int dynamic, cudaStream_t stream);
+// *out += number of fronts in list not yet finished (flag kFlagDone unset)
+void launch_count_unfinished(const FrontState* st, const int* list, int count, int* out, cudaStream_t stream);
+// near (far = false) / far (far = true) Schur-complement update, FP64
+void launch_update(bool far, const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
+                   FactorGlobals* g, int level, int dynamic, cudaStream_t stream);
 
 // Solve
 void launch_permute_in(int n, int nrhs, const int* perm, const double* B, int ldb, double* Bp, cudaStream_t stream);

@@ -38,9 +38,17 @@ struct ClusterShared {
   double wr[kNBMax];    // D * L(r, :)^T for the partner row
   double Dd[kNBMax], Do[kNBMax];
   int pk[kNBMax];
-  double ex_v[16];      // per-CTA partial maxima
-  int ex_i[16];         // per-CTA argmax rows
-  double ex_x[4];       // values broadcast by the owner of a row
+  double ex_v[16];      // per-CTA partial maxima (slow path)
+  int ex_i[16];         // per-CTA argmax rows (slow path)
+  double ex_x[4];       // values broadcast by the owner of a row (slow path)
+  // fast path, double-buffered by step parity: partial argmax per CTA, the
+  // pivot's diagonal, and row k+1's current value, sign and panel L row
+  double fx_v[2][16];
+  int fx_i[2][16];
+  double fx_kk[2];
+  int fx_sign[2];
+  double fx_k1[2];
+  double fx_row[2][kNBMax];
   double red_v[kCT / 32];
   int red_i[kCT / 32];
   double rowtmp[kNBMax];  // D * L(row, :) staging
@@ -61,8 +69,19 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
   const FrontDesc f = fronts[s];
   FrontState S = st[s];
   if (S.flags & kFlagDone) {
-    if (q == 0 && threadIdx.x == 0) st[s].panel_start = S.k;
+    if (q == 0 && threadIdx.x == 0) {
+      st[s].panel_start = S.k;
+      st[s].far = 0;
+    }
     return;
+  }
+  // outer block bookkeeping: a new block starts at the first panel and after
+  // every far update (the far kernel of the previous iteration ran)
+  if (S.ob_end == 0 || S.far) {
+    S.ob = S.k;
+    S.ob_end = min(S.k + kOuterBlock, f.nelig);
+    S.far = 0;
+    S.flags &= ~kFlagFlush;
   }
   extern __shared__ double dsm[];
   __shared__ ClusterShared sh;
@@ -70,7 +89,7 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
   const int64_t ld = f.ld;
   double* F = f.F;
   const int ps = S.k;
-  const int pe = ps + min(nb, effEnd - ps);
+  const int pe = ps + min(nb, S.ob_end - ps);
   const int span = m - ps;
   const int Rr = (span + CS - 1) / CS;  // rows per CTA (<= R)
   const int base = ps + q * Rr;
@@ -84,15 +103,8 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
 
   // ---- orig_max over the whole front at the first panel (cluster-wide)
   if (ps == 0) {
-    double tmax = 0.0;
-    for (int j = q; j < m; j += CS)
-      for (int i = j + threadIdx.x; i < m; i += kCT) tmax = fmax(tmax, fabs(F[j * ld + i]));
-    tmax = block_max<kCT>(tmax, sh.red_v);
-    if (threadIdx.x == 0)
-      for (int d = 0; d < CS; ++d) remote(sh.ex_v, d)[q] = tmax;
-    cluster.sync();
-    double om = 0.0;
-    for (int d = 0; d < CS; ++d) om = fmax(om, sh.ex_v[d]);
+    // max |entry| of the assembled front, accumulated by the assembly kernel
+    double om = S.orig_max;
     if (o.mode == 1) {
       if (om < o.static_abs_floor) om = 1.0;
     } else {
@@ -104,7 +116,6 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     S.num_perturbed = 0;
     S.perturb = 0.0;
     S.delta = o.front_delta ? o.front_delta[s] : (o.static_delta > 0.0 ? o.static_delta : 1.4901161193847656e-08 * om);
-    cluster.sync();
   }
   const double orig_max = S.orig_max;
   int n_pos = S.n_pos, n_neg = S.n_neg, n_zero = S.n_zero, nPert = S.num_perturbed;
@@ -207,103 +218,150 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
 
   int k = ps;
   bool stopped = false;
-  // w for the first pivot of the panel: no panel columns yet
+  bool flush = false;
+  int step = 0;
+  // prefetched raw values of column k for this thread's rows
+  constexpr int kPF = 4;
+  double pf[kPF];
+  int pf_col = -1;
+  auto prefetch = [&](int col, int kfrom) {
+    int j = 0;
+    for (int i = max(base, kfrom) + threadIdx.x; i < rend && j < kPF; i += kCT, ++j)
+      pf[j] = (i >= col) ? F[col * ld + i] : F[i * ld + col];
+    pf_col = col;
+  };
+  auto current_column_pf = [&](int col, int kk, int p, const double* w, double* v) {
+    int j = 0;
+    for (int i = max(base, kk) + threadIdx.x; i < rend; i += kCT, ++j) {
+      const int li = i - base;
+      double raw;
+      if (pf_col == col && j < kPF)
+        raw = pf[j];
+      else
+        raw = (i >= col) ? F[col * ld + i] : F[i * ld + col];
+      double acc = 0.0;
+      for (int t = 0; t < p; ++t) acc += Lr[t * R + li] * w[t];
+      v[li] = raw - acc;
+    }
+  };
+  // new w for row k+1 after a 1x1 pivot d at panel position p, from the
+  // broadcast L row of k+1 and its current value vk1
+  auto local_w_next = [&](int p, double d, const double* lrow, double vk1) {
+    for (int t = threadIdx.x; t <= p; t += kCT) {
+      double v;
+      if (t == p) {
+        v = d * (vk1 / d);
+      } else {
+        const int kind = sh.pk[t];
+        if (kind == 0)
+          v = sh.Dd[t] * lrow[t];
+        else if (kind == 1)
+          v = sh.Dd[t] * lrow[t] + sh.Do[t] * lrow[t + 1];
+        else
+          v = sh.Do[t - 1] * lrow[t - 1] + sh.Dd[t] * lrow[t];
+      }
+      sh.w[t] = v;
+    }
+  };
+  // record a 1x1 pivot d in column col (this CTA's rows) and in D
+  auto finish_1x1 = [&](int p, double d, const double* col) {
+    if (d > 0)
+      ++n_pos;
+    else if (d < 0)
+      ++n_neg;
+    else
+      ++n_zero;
+    thread_rmax = fmax(thread_rmax, fabs(d));
+    for (int i = max(base, k + 1) + threadIdx.x; i < rend; i += kCT) {
+      const int li = i - base;
+      const double a = col[li];
+      thread_rmax = fmax(thread_rmax, fabs(a));
+      const double l = a / d;
+      Lr[p * R + li] = l;
+      F[k * ld + i] = l;
+    }
+    if (threadIdx.x == 0) {
+      sh.Dd[p] = d;
+      sh.Do[p] = 0.0;
+      sh.pk[p] = 0;
+    }
+    if (q == 0 && threadIdx.x == 0) {
+      F[k * ld + k] = d;
+      f.Dd[k] = d;
+      f.Do[k] = 0.0;
+      f.pk[k] = 0;
+    }
+  };
+
   while (k < pe) {
     const int p = k - ps;
-    // ---- column k
-    current_column(k, k, p, sh.w, vk);
+    const int b = step & 1;
+    ++step;
+    current_column_pf(k, k, p, sh.w, vk);
+    __syncthreads();
+    // fast-path exchange: partial argmax (threshold) and the values every
+    // CTA needs to continue without a second barrier
+    ArgMax am{0.0, -1};
+    if (o.mode != 1) {
+      for (int i = max(base, k + 1) + threadIdx.x; i < min(rend, effEnd); i += kCT)
+        am = argmax_combine(am, ArgMax{fabs(vk[i - base]), i});
+      am = block_argmax<kCT>(am, sh.red_v, sh.red_i);
+    }
+    const bool haveNext = (k + 1 < pe) && (k + 1 < m);
+    const int o1 = haveNext ? owner(k + 1) : -1;
+    // one thread per destination CTA
+    if (threadIdx.x < CS) {
+      const int dd = threadIdx.x;
+      remote(sh.fx_v[b], dd)[q] = am.v;
+      remote(sh.fx_i[b], dd)[q] = am.i;
+      if (q == owner(k)) {
+        remote(sh.fx_kk, dd)[b] = vk[k - base];
+        remote(sh.fx_sign, dd)[b] = (o.mode == 1 && o.sign_final) ? o.sign_final[f.fidx[k]] : 0;
+      }
+      if (q == o1) remote(sh.fx_k1, dd)[b] = vk[k + 1 - base];
+    }
+    if (q == o1)
+      for (int t = threadIdx.x; t < p * CS; t += kCT)
+        remote(sh.fx_row[b], t / p)[t % p] = Lr[(t % p) * R + (k + 1 - base)];
+    // prefetch the next column while the exchange completes
+    if (haveNext) prefetch(k + 1, k + 1);
+    // the cluster barrier orders the distributed shared-memory stores; the
+    // global stores of this step are not read by other CTAs in this launch
+    cluster.sync();
+    const double akk = sh.fx_kk[b];
+
     if (o.mode == 1) {
-      // static pivoting (dense_kernel.hpp:982-1034): owner of k decides d
-      if (q == owner(k) && threadIdx.x == 0) {
-        const double akk = vk[k - base];
-        const int sign = o.sign_final ? o.sign_final[f.fidx[k]] : 0;
-        const double floorv = fmax(o.static_abs_floor, o.static_rel_floor * orig_max);
-        bool need;
-        if (sign > 0)
-          need = akk < floorv;
-        else if (sign < 0)
-          need = akk > -floorv;
-        else
-          need = fabs(akk) < floorv;
-        double d = akk, applied = 0.0;
-        if (need) {
-          const double sg = (sign != 0) ? static_cast<double>(sign) : (akk >= 0.0 ? 1.0 : -1.0);
-          d = akk + sg * S.delta;
-          applied = d - akk;
-        }
-        for (int dd = 0; dd < CS; ++dd) {
-          double* x = remote(sh.ex_x, dd);
-          x[0] = d;
-          x[1] = applied;
-        }
-      }
-      __syncthreads();
-      cluster.sync();
-      const double d = sh.ex_x[0], applied = sh.ex_x[1];
-      if (applied != 0.0) {
-        pert += fabs(applied);
-        ++nPert;
-      }
-      if (d > 0)
-        ++n_pos;
-      else if (d < 0)
-        ++n_neg;
+      // static pivoting (dense_kernel.hpp:982-1034), decided by every CTA
+      const int sign = sh.fx_sign[b];
+      const double floorv = fmax(o.static_abs_floor, o.static_rel_floor * orig_max);
+      bool need;
+      if (sign > 0)
+        need = akk < floorv;
+      else if (sign < 0)
+        need = akk > -floorv;
       else
-        ++n_zero;
-      thread_rmax = fmax(thread_rmax, fabs(d));
-      for (int i = max(base, k + 1) + threadIdx.x; i < rend; i += kCT) {
-        const int li = i - base;
-        const double a = vk[li];
-        thread_rmax = fmax(thread_rmax, fabs(a));
-        const double l = a / d;
-        Lr[p * R + li] = l;
-        F[k * ld + i] = l;
+        need = fabs(akk) < floorv;
+      double d = akk;
+      if (need) {
+        const double sg = (sign != 0) ? static_cast<double>(sign) : (akk >= 0.0 ? 1.0 : -1.0);
+        d = akk + sg * S.delta;
+        const double applied = d - akk;
+        if (applied != 0.0) {
+          pert += fabs(applied);
+          ++nPert;
+        }
       }
-      if (threadIdx.x == 0) {
-        sh.Dd[p] = d;
-        sh.Do[p] = 0.0;
-        sh.pk[p] = 0;
-      }
-      if (q == 0 && threadIdx.x == 0) {
-        F[k * ld + k] = d;
-        f.Dd[k] = d;
-        f.Do[k] = 0.0;
-        f.pk[k] = 0;
-      }
+      finish_1x1(p, d, vk);
+      if (haveNext) local_w_next(p, d, sh.fx_row[b], sh.fx_k1[b]);
       __syncthreads();
       ++k;
-      if (k < pe) {
-        if (q == owner(k)) {
-          d_times_row(k, p + 1, sh.rowtmp);
-          __syncthreads();
-          for (int t = threadIdx.x; t < (p + 1) * CS; t += kCT) remote(sh.w, t / (p + 1))[t % (p + 1)] = sh.rowtmp[t % (p + 1)];
-        }
-        __threadfence();
-        cluster.sync();
-      }
       continue;
     }
 
-    // ---- threshold Bunch-Kaufman: lambda over the eligible rows
-    ArgMax am{0.0, -1};
-    for (int i = max(base, k + 1) + threadIdx.x; i < min(rend, effEnd); i += kCT)
-      am = argmax_combine(am, ArgMax{fabs(vk[i - base]), i});
-    am = block_argmax<kCT>(am, sh.red_v, sh.red_i);
-    if (threadIdx.x == 0) {
-      for (int dd = 0; dd < CS; ++dd) {
-        remote(sh.ex_v, dd)[q] = am.v;
-        remote(sh.ex_i, dd)[q] = am.i;
-      }
-      if (q == owner(k))
-        for (int dd = 0; dd < CS; ++dd) remote(sh.ex_x, dd)[0] = vk[k - base];
-    }
-    __threadfence();
-    cluster.sync();
-    ArgMax gm{sh.ex_v[0], sh.ex_i[0]};
-    for (int dd = 1; dd < CS; ++dd) gm = argmax_combine(gm, ArgMax{sh.ex_v[dd], sh.ex_i[dd]});
+    ArgMax gm{sh.fx_v[b][0], sh.fx_i[b][0]};
+    for (int dd = 1; dd < CS; ++dd) gm = argmax_combine(gm, ArgMax{sh.fx_v[b][dd], sh.fx_i[b][dd]});
     const double lambda = gm.v;
     const int r = gm.i;
-    const double akk = sh.ex_x[0];
     int dec;
     double arr = 0.0, vkr = 0.0;
     if (lambda <= o.zero_tol) {
@@ -311,8 +369,13 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
       dec = (fabs(akk) <= isolatedFloor) ? 3 : 0;
     } else if (fabs(akk) >= kAlphaBK * lambda) {
       dec = 0;
+    } else if (r >= S.ob_end && ps > S.ob) {
+      // the partner lies beyond the outer block while earlier panels of the
+      // block have not been applied there yet: stop before pivot k so the
+      // deferred update is applied first, then restart the block at k
+      dec = 4;
     } else {
-      // partner column r
+      // partner column r (slow path)
       if (q == owner(r)) {
         d_times_row(r, p, sh.rowtmp);
         __syncthreads();
@@ -346,51 +409,29 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
         dec = 1;
       else
         dec = 2;
+      // the slow path consumed extra barriers; make every CTA finish reading
+      // the exchange slots before anyone writes them again
+      cluster.sync();
     }
     if (dec == 3) {
       stopped = true;
       break;
     }
-    if (dec == 0 || dec == 1) {
-      double d;
-      double* col;
-      if (dec == 1) {
-        // new column k = old column r with positions k, r exchanged
-        interchange(k, r, true);
-        // after the interchange vk holds old vk values moved, vr likewise;
-        // the pivot column is vr with entries k and r exchanged (done above)
-        col = vr;
-        d = arr;
-      } else {
-        col = vk;
-        d = akk;
-      }
-      if (d > 0)
-        ++n_pos;
-      else if (d < 0)
-        ++n_neg;
-      else
-        ++n_zero;
-      thread_rmax = fmax(thread_rmax, fabs(d));
-      for (int i = max(base, k + 1) + threadIdx.x; i < rend; i += kCT) {
-        const int li = i - base;
-        const double a = col[li];
-        thread_rmax = fmax(thread_rmax, fabs(a));
-        const double l = a / d;
-        Lr[p * R + li] = l;
-        F[k * ld + i] = l;
-      }
-      if (threadIdx.x == 0) {
-        sh.Dd[p] = d;
-        sh.Do[p] = 0.0;
-        sh.pk[p] = 0;
-      }
-      if (q == 0 && threadIdx.x == 0) {
-        F[k * ld + k] = d;
-        f.Dd[k] = d;
-        f.Do[k] = 0.0;
-        f.pk[k] = 0;
-      }
+    if (dec == 4) {
+      flush = true;
+      break;
+    }
+    if (dec == 0) {
+      finish_1x1(p, akk, vk);
+      if (haveNext) local_w_next(p, akk, sh.fx_row[b], sh.fx_k1[b]);
+      __syncthreads();
+      k += 1;
+      continue;
+    }
+    pf_col = -1;  // an interchange invalidates the prefetched column
+    if (dec == 1) {
+      interchange(k, r, true);
+      finish_1x1(p, arr, vr);
       __syncthreads();
       k += 1;
     } else {
@@ -454,7 +495,7 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
       __syncthreads();
       k += 2;
     }
-    // w for the next pivot row, from its owner
+    // after an interchange or a 2x2 the next row's w comes from its owner
     if (k < pe) {
       const int pn = k - ps;
       if (q == owner(k)) {
@@ -492,7 +533,10 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     W.panel_start = ps;
     W.k = k;
     W.npiv = k;
-    int flags = 0;
+    W.ob = S.ob;
+    W.ob_end = S.ob_end;
+    W.far = (done || flush || k >= S.ob_end) ? 1 : 0;
+    int flags = flush ? kFlagFlush : 0;
     if (done) {
       flags |= kFlagDone;
       if (k < effEnd) {
