@@ -287,8 +287,94 @@ void free_level_device(LevelLists& L) {
   dfree(L.d_all);
   dfree(L.d_fwd_tasks);
   dfree(L.d_bwd_tasks);
+  dfree(L.d_tcmaps);
+  dfree(L.d_tcws);
   L.d_small = L.d_large = L.d_tasks = L.d_all = nullptr;
   L.d_fwd_tasks = L.d_bwd_tasks = nullptr;
+  L.d_tcmaps = nullptr;
+  L.d_tcws = nullptr;
+  L.tc_grid = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Mixed-precision far update plumbing: a TF32 hi/lo workspace of
+// m x 4 x kTcKpad floats per large front and a TMA tensor map over it
+// (32-float x 128-row boxes, 128-byte swizzle, zero fill past row m).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !p)
+      throw SymlaError(SYMLA_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+size_t tc_level_floats(const symla_gpu_ctx* c, const LevelLists& L) {
+  size_t t = 0;
+  for (int s : L.large) t += static_cast<size_t>(c->hdesc[s].m) * 4 * kTcKpad;
+  return t;
+}
+
+void prepare_tc_level(symla_gpu_ctx* c, LevelLists& L, float* base) {
+  dfree(L.d_tcmaps);
+  dfree(L.d_tcws);
+  L.d_tcmaps = nullptr;
+  L.d_tcws = nullptr;
+  const int nl = static_cast<int>(L.large.size());
+  if (nl == 0) return;
+  std::vector<CUtensorMap> maps(nl);
+  std::vector<float*> ptrs(nl);
+  size_t off = 0;
+  long long tiles = 0;
+  for (int i = 0; i < nl; ++i) {
+    const int m = c->hdesc[L.large[i]].m;
+    ptrs[i] = base + off;
+    off += static_cast<size_t>(m) * 4 * kTcKpad;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(4 * kTcKpad), static_cast<cuuint64_t>(m)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(4 * kTcKpad * sizeof(float))};
+    const cuuint32_t box[2] = {32, 128};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encode_tiled()(&maps[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, ptrs[i], dims, strides, box, estr,
+                                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw SymlaError(SYMLA_ERR_CUDA, "cuTensorMapEncodeTiled failed for a front workspace");
+    const long long nt = (m + 127) / 128;
+    tiles += nt * (nt + 1) / 2;
+  }
+  L.d_tcmaps = dupload(maps, c->stream);
+  L.d_tcws = dupload(ptrs, c->stream);
+  L.tc_grid = static_cast<int>(std::min<long long>(tiles, 148));
+}
+
+// Growth-guard maxima: 2 doubles per large front of the largest level.
+void ensure_tc_guard(symla_gpu_ctx* c, const std::vector<LevelLists>& levels) {
+  size_t nl = 0;
+  for (const auto& L : levels) nl = std::max(nl, L.large.size());
+  if (nl <= c->tc_guard_cap) return;
+  dfree(c->d_tc_guard);
+  c->d_tc_guard = dalloc<double>(2 * nl);
+  c->tc_guard_cap = nl;
+}
+
+// Static levels: one workspace sized for the largest level, shared by all.
+void ensure_tc_static(symla_gpu_ctx* c) {
+  if (c->tc_static_ready) return;
+  size_t need = 0;
+  for (const auto& L : c->levels) need = std::max(need, tc_level_floats(c, L));
+  dfree(c->d_tcws);
+  c->d_tcws = dalloc<float>(need);
+  for (auto& L : c->levels) prepare_tc_level(c, L, c->d_tcws);
+  if (!c->d_tc_err) c->d_tc_err = dalloc<int>(1);
+  ensure_tc_guard(c, c->levels);
+  c->tc_static_ready = true;
 }
 
 void upload_level_lists(LevelLists& L, cudaStream_t s) {
@@ -603,9 +689,27 @@ void launch_panel_iteration(symla_gpu_ctx* c, const LevelLists& L, int level, co
   timed(c, SYMLA_KERNEL_NEAR, 0.0, 0.0, [&] {
     launch_update(false, c->d_desc, c->d_state, d_large, nl, L.trailing_grid, c->d_glob, level, dynamic, st);
   });
-  timed(c, SYMLA_KERNEL_TRAILING, 0.0, 0.0, [&] {
-    launch_update(true, c->d_desc, c->d_state, d_large, nl, L.trailing_grid, c->d_glob, level, dynamic, st);
-  });
+  if (ko.precision == SYMLA_PREC_MIXED) {
+    timed(c, SYMLA_KERNEL_TRAILING, 0.0, 0.0, [&] {
+      const int bmax = tc_max_fronts();
+      CK(cudaMemsetAsync(c->d_tc_guard, 0, 2 * sizeof(double) * nl, st));
+      for (int b = 0; b < nl; b += bmax) {
+        const int cnt = std::min(bmax, nl - b);
+        double* guard = c->d_tc_guard + 2 * b;
+        launch_tc_split(c->d_desc, c->d_state, d_large + b, cnt, L.d_tcws + b, guard, L.large_max_m, c->d_glob,
+                        level, dynamic, st);
+        launch_tc_far(c->d_desc, c->d_state, d_large + b, cnt, L.d_tcmaps + b, guard, L.tc_grid, c->d_glob, level,
+                      dynamic, c->d_tc_err, st);
+        // blocks the growth guard kept off the tensor cores
+        launch_update(true, c->d_desc, c->d_state, d_large + b, cnt, L.trailing_grid, c->d_glob, level, dynamic,
+                      st, guard);
+      }
+    });
+  } else {
+    timed(c, SYMLA_KERNEL_TRAILING, 0.0, 0.0, [&] {
+      launch_update(true, c->d_desc, c->d_state, d_large, nl, L.trailing_grid, c->d_glob, level, dynamic, st);
+    });
+  }
 }
 
 void launch_level(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
@@ -756,8 +860,14 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
   reset_to_static(c);
   const KernelOpts ko = make_kernel_opts(c, o);
   CK(cudaMemsetAsync(c->d_state, 0, c->numSN * sizeof(FrontState), st));
-  FactorGlobals g0{INT_MAX, 0, -1, 0, 0.0, 0.0};
+  FactorGlobals g0{INT_MAX, 0, -1, 0, 0.0, 0.0, 0.0};
   CK(cudaMemcpyAsync(c->d_glob, &g0, sizeof g0, cudaMemcpyHostToDevice, st));
+  const bool mixed = o->precision == SYMLA_PREC_MIXED;
+  if (mixed) {
+    ensure_tc_static(c);
+    CK(cudaMemsetAsync(c->d_tc_err, 0, sizeof(int), st));
+    launch_absmax(c->d_values, c->nnz, &c->d_glob->amax, st);  // scale of the growth guard
+  }
   CK(cudaEventRecord(c->ev[0], st));
   for (int l = 0; l < c->numLevels; ++l) {
     const LevelLists& L = c->levels[l];
@@ -782,6 +892,16 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
       LevelLists L;
       build_level_lists(c, Ls.all, L);
       upload_level_lists(L, st);
+      if (mixed && !L.large.empty()) {
+        float* ws = dalloc<float>(tc_level_floats(c, L));
+        c->dyn_allocs.push_back(ws);
+        prepare_tc_level(c, L, ws);
+        if (L.large.size() > c->tc_guard_cap) {
+          dfree(c->d_tc_guard);
+          c->d_tc_guard = dalloc<double>(2 * L.large.size());
+          c->tc_guard_cap = L.large.size();
+        }
+      }
       launch_level(c, L, l, ko, 1, L.d_small, L.d_large, L.d_tasks);
       read_states(c);
       free_level_device(L);
@@ -798,6 +918,11 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
   }
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+  if (mixed) {
+    int tcerr = 0;
+    CK(cudaMemcpy(&tcerr, c->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (tcerr != 0) throw SymlaError(SYMLA_ERR_TIMEOUT, "tensor-core Schur update: a pipeline wait timed out");
+  }
   if (!dynamic) read_states(c);
 
   // reductions (multifrontal.hpp:795-803)
@@ -1052,6 +1177,7 @@ extern "C" int symla_gpu_create(const symla_symbolic* sym, int n, const int* col
     if (!configured[device]) {
       CK(configure_factor_kernels());
       CK(configure_cluster_panel());
+      CK(configure_tc_far());
       configured[device] = true;
     }
     const char* env = getenv("SYMLA_PANEL");
@@ -1082,7 +1208,8 @@ extern "C" void symla_gpu_destroy(symla_gpu_ctx* c) {
                   c->d_glob, c->d_a_colptr, c->d_a_j, c->d_a_pos, c->d_a_idx, c->d_values, c->d_sign_final,
                   c->d_front_delta, c->d_perm, c->d_rowptr, c->d_colind, c->d_vidx, c->d_srowptr, c->d_svidx, c->d_W,
                   c->d_Bp, c->d_Z, c->d_Xf, c->d_B, c->d_X, c->d_R, c->d_dX, c->d_Xn, c->d_Rn, c->d_norms,
-                  c->d_scratch_int, c->d_flag_base, c->d_flags, c->d_solve_err, c->d_counter};
+                  c->d_scratch_int, c->d_flag_base, c->d_flags, c->d_solve_err, c->d_counter,
+                  c->d_tcws, c->d_tc_err, c->d_tc_guard};
   for (void* p : ptrs) dfree(p);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);

@@ -56,6 +56,23 @@ enum : int { kFlagDone = 1, kFlagDelayed = 2, kFlagSingularRoot = 4, kFlagFlush 
 
 // Columns per outer block of the large-front factorization.
 constexpr int kOuterBlock = 128;
+// Pivots per far update the tensor-core workspace holds (>= kOuterBlock + 1,
+// a multiple of 32).
+constexpr int kTcKpad = 160;
+// Growth guard of the mixed-precision far update. A block of K pivots goes
+// to the tensor cores only when max|L| * max|L D| over the rows it updates
+// is at most this multiple of max|a_ij| of the original matrix: TF32x3
+// rounds each product to about 2^-22 of |l||w|, and that rounding is a
+// perturbation of the matrix entry the update lands on (the backward-error
+// view of elimination), so it stays a small multiple of 2^-22 max|A|. Blocks
+// with larger multipliers (threshold pivoting restricted to the eligible rows
+// lets them grow) take the FP64 update instead. Both far-update kernels
+// evaluate this one predicate on the same recorded maxima, so each block is
+// applied exactly once.
+constexpr double kTcGrowthGuard = 8.0;
+__host__ __device__ inline bool tc_block_ok(int K, double lmax, double wmax, double amax) {
+  return K <= kTcKpad && lmax * wmax <= kTcGrowthGuard * amax;
+}
 
 // Error word of the pipelined solve kernels.
 constexpr int kSolveErrTimeout = 1;
@@ -68,6 +85,7 @@ struct FactorGlobals {
   int pad;
   double flops_near;   // algorithmic flops of the near (in-block) updates
   double flops_far;    // algorithmic flops of the far (deferred) updates
+  double amax;         // max |a_ij| of the matrix being factorized (mixed precision only)
 };
 
 // Options visible to kernels.

@@ -1,6 +1,7 @@
 // Device context behind the C ABI (include/symla_gpu.h).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -49,6 +50,11 @@ struct LevelLists {
   int* d_large = nullptr;
   int* d_tasks = nullptr;
   int* d_all = nullptr;
+  // mixed-precision far update: per large front (list order) its TF32
+  // workspace and the tensor map over it (built on first use)
+  CUtensorMap* d_tcmaps = nullptr;
+  float** d_tcws = nullptr;
+  int tc_grid = 0;
 };
 
 struct DeviceBuf {
@@ -138,6 +144,13 @@ struct symla_gpu_ctx {
   int solve_epoch = 0;
   int fwd_resident = 0, bwd_resident = 0;
   std::vector<int> solve_np;  // npiv per front the task lists were built for
+
+  // mixed-precision far update workspace (static plan) and error word
+  float* d_tcws = nullptr;
+  bool tc_static_ready = false;
+  int* d_tc_err = nullptr;
+  double* d_tc_guard = nullptr;  // growth-guard maxima, 2 per large front of a level
+  size_t tc_guard_cap = 0;
 
   // dynamic (delayed-pivot) allocations for the current factorization
   std::vector<void*> dyn_allocs;

@@ -864,7 +864,8 @@ __device__ __forceinline__ int update_tiles(int m, int c0, int c1) {
 template <bool FAR>
 __global__ void __launch_bounds__(kTThreads) update_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
                                                            const int* __restrict__ front_list, int count,
-                                                           FactorGlobals* g, int level, int dynamic) {
+                                                           FactorGlobals* g, int level, int dynamic,
+                                                           const double* __restrict__ tc_guard) {
   if (level_aborted(g, level, dynamic)) return;
   // two stages of {A rows (kKC x kTT), B rows with halo ((kKC+2) x kTT)} and
   // one (L D) buffer (kKC x kTT)
@@ -881,7 +882,10 @@ __global__ void __launch_bounds__(kTThreads) update_kernel(const FrontDesc* __re
     const int sf = front_list[t];
     int c0, c1, q0, q1;
     const FrontState S = st[sf];
-    tile_end[t] = update_range(S, fronts[sf].m, FAR, c0, c1, q0, q1) ? update_tiles(fronts[sf].m, c0, c1) : 0;
+    bool use = update_range(S, fronts[sf].m, FAR, c0, c1, q0, q1);
+    if (FAR && use && tc_guard && tc_block_ok(q1 - q0, tc_guard[2 * t], tc_guard[2 * t + 1], g->amax))
+      use = false;  // the tensor-core kernel applied this block
+    tile_end[t] = use ? update_tiles(fronts[sf].m, c0, c1) : 0;
     if (blockIdx.x == 0 && tile_end[t] > 0) {
       const double nc = c1 - c0, mm = fronts[sf].m;
       const double entries = nc * mm - (static_cast<double>(c0) + c1 - 1) * nc / 2.0;
@@ -1049,15 +1053,16 @@ void launch_count_unfinished(const FrontState* st, const int* list, int count, i
 }
 
 void launch_update(bool far, const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
-                   FactorGlobals* g, int level, int dynamic, cudaStream_t stream) {
+                   FactorGlobals* g, int level, int dynamic, cudaStream_t stream, const double* tc_guard) {
   if (count <= 0 || grid_x <= 0) return;
   const size_t sm = static_cast<size_t>(5 * kKC + 4) * kTT * sizeof(double);
   for (int b = 0; b < count; b += kMaxUpdateFronts) {
     const int cnt = count - b < kMaxUpdateFronts ? count - b : kMaxUpdateFronts;
     if (far)
-      update_kernel<true><<<grid_x, kTThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic);
+      update_kernel<true><<<grid_x, kTThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic,
+                                                             tc_guard ? tc_guard + 2 * b : nullptr);
     else
-      update_kernel<false><<<grid_x, kTThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic);
+      update_kernel<false><<<grid_x, kTThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic, nullptr);
   }
 }
 

@@ -1,6 +1,7 @@
 // Host launchers for the factorization and solve kernels.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -30,11 +31,24 @@ cudaError_t configure_cluster_panel();
 cudaError_t launch_cluster_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m,
                                  int nb, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
                                  cudaStream_t stream);
+// Mixed-precision far update (schur_tc.cu): TF32x3 tcgen05 GEMM fed by TMA.
+size_t tc_far_smem();
+cudaError_t configure_tc_far();
+int tc_max_fronts();
+// guard: 2 doubles per list entry, zeroed before launch_tc_split (max|L|, max|L D|)
+void launch_tc_split(const FrontDesc* fronts, const FrontState* st, const int* list, int count, float* const* ws,
+                     double* guard, int max_m, const FactorGlobals* g, int level, int dynamic, cudaStream_t stream);
+void launch_tc_far(const FrontDesc* fronts, FrontState* st, const int* list, int count, const CUtensorMap* maps,
+                   const double* guard, int grid, FactorGlobals* g, int level, int dynamic, int* err,
+                   cudaStream_t stream);
+
 // *out += number of fronts in list not yet finished (flag kFlagDone unset)
 void launch_count_unfinished(const FrontState* st, const int* list, int count, int* out, cudaStream_t stream);
-// near (far = false) / far (far = true) Schur-complement update, FP64
+// near (far = false) / far (far = true) Schur-complement update, FP64. With
+// tc_guard (far only; the split pre-pass's maxima, 2 per list entry) it
+// applies just the blocks that tc_block_ok sends away from the tensor cores.
 void launch_update(bool far, const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
-                   FactorGlobals* g, int level, int dynamic, cudaStream_t stream);
+                   FactorGlobals* g, int level, int dynamic, cudaStream_t stream, const double* tc_guard = nullptr);
 
 // Solve
 void launch_permute_in(int n, int nrhs, const int* perm, const double* B, int ldb, double* Bp, cudaStream_t stream);
