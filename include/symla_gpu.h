@@ -247,6 +247,31 @@ long long symla_gpu_launch_count(symla_gpu_ctx* ctx);
  * (lower-triangle convention), [5] nnz(L) entries, [6] arena doubles. */
 int symla_gpu_plan_stats(symla_gpu_ctx* ctx, double* out, int cap);
 
+/* Relative residual ||B - A X||_inf / (||A||_inf ||X||_inf + ||B||_inf) of
+ * a device-resident candidate solution X against device-resident B
+ * (column-major, n x nrhs, leading dimensions ldx, ldb >= n), for the matrix
+ * of the last factorization; *rel_residual receives it on the host. It is
+ * the measure symla_gpu_solve_refine reports, computed without allocating
+ * any device memory: for callers whose device memory is owned by another
+ * allocator, or whose loop cannot take the device-wide synchronisation of
+ * cudaMalloc / cudaFree. This entry point has no counterpart in the
+ * reference.
+ *
+ * Its scratch (the residual and four norm accumulators) is one fixed
+ * device array inside the library, of SYMLA_NOALLOC_RESIDUAL_MAX_ENTRIES
+ * doubles plus 256 bytes, present on every GPU that loads the library until
+ * the process exits. n * nrhs above that maximum is rejected with
+ * SYMLA_ERR_BAD_SIZE. The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that
+ * first call before any stream capture. Every call uses the same array and
+ * clears the accumulators it needs at its start, so calls whose work
+ * overlaps on the GPU (from several threads, contexts or streams) race and
+ * must be serialised by the caller. Runs on the context's stream and
+ * returns after it synchronises. */
+#define SYMLA_NOALLOC_RESIDUAL_MAX_ENTRIES (1 << 20)
+int symla_gpu_relative_residual_noalloc(symla_gpu_ctx* ctx, const double* X, int ldx, const double* B, int ldb,
+                                        int nrhs, double* rel_residual);
+
 #ifdef __cplusplus
 }
 #endif

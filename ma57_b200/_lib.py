@@ -98,7 +98,10 @@ _SIGS = {
     "symla_gpu_kernel_stats": (_i, [_p, _i, _pd]),
     "symla_gpu_reset_kernel_stats": (None, [_p]),
     "symla_gpu_launch_count": (C.c_longlong, [_p]),
+    "symla_gpu_relative_residual_noalloc": (_i, [_p, _p, _i, _p, _i, _i, _pd]),
 }
+
+NOALLOC_RESIDUAL_MAX_ENTRIES = 1 << 20
 
 KERNEL_KINDS = ["far_update", "panel", "small", "assemble", "forward", "backward", "residual", "near_update"]
 

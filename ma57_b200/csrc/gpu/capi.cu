@@ -27,6 +27,12 @@ int set_error(int code, const std::string& msg) {
   g_last_error = msg;
   return code;
 }
+}  // namespace
+
+// Error recording for entry points defined in other translation units.
+int symla_gpu::record_error(int code, const std::string& msg) { return set_error(code, msg); }
+
+namespace {
 
 struct CudaError : std::runtime_error {
   cudaError_t err;

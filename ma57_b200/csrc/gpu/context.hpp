@@ -62,6 +62,9 @@ struct DeviceBuf {
   size_t bytes = 0;
 };
 
+// Sets the message symla_last_error returns; returns code.
+int record_error(int code, const std::string& msg);
+
 }  // namespace symla_gpu
 
 struct symla_gpu_ctx {
