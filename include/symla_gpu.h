@@ -244,7 +244,11 @@ long long symla_gpu_launch_count(symla_gpu_ctx* ctx);
 
 /* Front-size statistics of the plan: [0] fronts, [1] levels, [2] max m,
  * [3] sum m^2, [4] algorithmic factorization flops of the last factorize
- * (lower-triangle convention), [5] nnz(L) entries, [6] arena doubles. */
+ * (lower-triangle convention), [5] nnz(L) entries, [6] arena doubles;
+ * large-front panels of the last factorize: [7] speculated and accepted
+ * whole, [8] accepted up to a failing pivot, [9] failed at the first pivot
+ * (one sequential decision), [10] run sequentially throughout. Returns the
+ * number of entries (11). */
 int symla_gpu_plan_stats(symla_gpu_ctx* ctx, double* out, int cap);
 
 /* Relative residual ||B - A X||_inf / (||A||_inf ||X||_inf + ||B||_inf) of

@@ -684,7 +684,7 @@ void launch_panel_iteration(symla_gpu_ctx* c, const LevelLists& L, int level, co
   cudaStream_t st = c->stream;
   const int nl = static_cast<int>(L.large.size());
   timed(c, SYMLA_KERNEL_PANEL, 0.0, 0.0, [&] {
-    if (c->use_cluster_panel && cluster_size_for(L.large_max_m) > 0) {
+    if (c->use_cluster_panel && cluster_size_for(L.large_max_m, nl) > 0) {
       CK(launch_cluster_panel(c->d_desc, c->d_state, d_large, nl, L.large_max_m, kPanelWidth, ko, c->d_glob, level,
                               dynamic, st));
     } else {
@@ -866,7 +866,7 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
   reset_to_static(c);
   const KernelOpts ko = make_kernel_opts(c, o);
   CK(cudaMemsetAsync(c->d_state, 0, c->numSN * sizeof(FrontState), st));
-  FactorGlobals g0{INT_MAX, 0, -1, 0, 0.0, 0.0, 0.0};
+  FactorGlobals g0{INT_MAX, 0, -1, 0, 0.0, 0.0, 0.0, 0, 0, 0, 0};
   CK(cudaMemcpyAsync(c->d_glob, &g0, sizeof g0, cudaMemcpyHostToDevice, st));
   const bool mixed = o->precision == SYMLA_PREC_MIXED;
   if (mixed) {
@@ -924,6 +924,14 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
   }
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+  {
+    FactorGlobals gp;
+    CK(cudaMemcpy(&gp, c->d_glob, sizeof gp, cudaMemcpyDeviceToHost));
+    c->panel_counts[0] = gp.spec_full;
+    c->panel_counts[1] = gp.spec_partial;
+    c->panel_counts[2] = gp.spec_failed;
+    c->panel_counts[3] = gp.seq_panels;
+  }
   if (mixed) {
     int tcerr = 0;
     CK(cudaMemcpy(&tcerr, c->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost));
@@ -1542,7 +1550,7 @@ extern "C" int symla_gpu_phase_ms(symla_gpu_ctx* c, float* ms, int cap) {
 
 extern "C" int symla_gpu_plan_stats(symla_gpu_ctx* c, double* out, int cap) {
   if (!c) return 0;
-  double v[7] = {0};
+  double v[11] = {0};
   v[0] = c->numSN;
   v[1] = c->numLevels;
   v[2] = c->plan_max_m;
@@ -1571,8 +1579,9 @@ extern "C" int symla_gpu_plan_stats(symla_gpu_ctx* c, double* out, int cap) {
     v[5] = nnzL;
   }
   v[6] = static_cast<double>(c->arena_doubles);
-  for (int i = 0; i < cap && i < 7; ++i) out[i] = v[i];
-  return 7;
+  for (int i = 0; i < 4; ++i) v[7 + i] = c->panel_counts[i];
+  for (int i = 0; i < cap && i < 11; ++i) out[i] = v[i];
+  return 11;
 }
 
 extern "C" int symla_gpu_set_profiling(symla_gpu_ctx* c, int enable) {

@@ -46,6 +46,7 @@ struct FrontState {
   int ob, ob_end;  // outer block [ob, ob_end): its pivots' update of the
                    // columns beyond ob_end is deferred to one far update
   int far;         // 1: the far update of [ob, k) is due after this panel
+  int spec;        // consecutive panels whose speculative first pivot failed
   double perturb;
   double orig_max;
   double running_max;
@@ -86,6 +87,9 @@ struct FactorGlobals {
   double flops_near;   // algorithmic flops of the near (in-block) updates
   double flops_far;    // algorithmic flops of the far (deferred) updates
   double amax;         // max |a_ij| of the matrix being factorized (mixed precision only)
+  // large-front panels of the last factorization: speculation accepted the
+  // whole panel / a prefix / failed at its first pivot; whole sequential panels
+  int spec_full, spec_partial, spec_failed, seq_panels;
 };
 
 // Options visible to kernels.

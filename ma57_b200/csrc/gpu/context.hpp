@@ -170,6 +170,7 @@ struct symla_gpu_ctx {
   int plan_max_m = 0;
   long long nnzL = 0;
   int last_precision = 0;
+  int panel_counts[4] = {0, 0, 0, 0};  // large-front panels: speculative full / prefix / failed, sequential
 
   // panel kernel choice (the cluster kernel unless SYMLA_PANEL=single)
   bool use_cluster_panel = true;

@@ -26,7 +26,7 @@ void launch_panel(const FrontDesc* fronts, FrontState* st, const int* list, int 
                   const KernelOpts& o, FactorGlobals* g, int level, int dynamic, cudaStream_t stream);
 // Cluster panel (panel_cluster.cu): returns 0 from cluster_size_for when a
 // front is too large for it (the single-CTA panel kernel then runs).
-int cluster_size_for(int max_m);
+int cluster_size_for(int max_m, int count);
 cudaError_t configure_cluster_panel();
 cudaError_t launch_cluster_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m,
                                  int nb, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,

@@ -13,8 +13,22 @@
 //
 // The front in global memory holds the panel-start ("raw") values of every
 // non-pivoted column; row/column interchanges are applied to it and to the
-// shared-memory copies. The trailing update of the panel follows in
-// trailing_update_kernel.
+// shared-memory copies. The near and far updates of the panel follow in
+// update_kernel / the tensor-core far update.
+//
+// Speculative panel. Most pivots of most fronts are 1x1 pivots at k (the
+// Bunch-Kaufman test |a_kk| >= alpha * lambda passes), and the test can be
+// checked after the fact: factor the panel without pivoting, then compare
+// each pivot with lambda = max over the eligible rows of its column's
+// current values, which the unpivoted factorization produces exactly (the
+// same left-looking sums as the sequential path). Every CTA factors the
+// panel's diagonal block redundantly in shared memory (no exchange needed
+// for D and the L rows of the block), then its own rows below the block in
+// one pass with no per-pivot synchronisation; the per-pivot partial lambdas
+// cross the cluster once. The pivots before the first one that fails are
+// accepted (identical values and decisions to the sequential path); if the
+// very first pivot fails, the sequential path takes over for one decision
+// (or for the whole panel after repeated failures).
 #include <cooperative_groups.h>
 
 #include <cmath>
@@ -32,6 +46,8 @@ namespace {
 constexpr double kAlphaBK = 0.64038820320220756;  // (1 + sqrt(17)) / 8
 constexpr int kCT = 256;                           // threads per CTA
 constexpr int kNBMax = 34;                         // panel width + 2
+constexpr int kSpecMax = 32;                       // pivots per speculative panel (= panel width)
+constexpr int kSpecRetry = 2;                      // consecutive failures before a whole sequential panel
 
 struct ClusterShared {
   double w[kNBMax];     // D * L(k, :)^T for the current pivot row
@@ -54,7 +70,25 @@ struct ClusterShared {
   double rowtmp[kNBMax];  // D * L(row, :) staging
   double rowA[kNBMax], rowB[kNBMax];  // row interchange staging
   double vA[2], vB[2];
+  // speculative panel
+  double db[kSpecMax][kSpecMax + 1];  // diagonal block: raw lower triangle -> L, d on the diagonal
+  double wv[kSpecMax][kSpecMax + 1];  // wv[c][t] = d_t * L(c, t), t < c
+  double aabs[kSpecMax][kSpecMax + 1];  // |current value| of the diagonal-block column entries
+  double dv[kSpecMax], iv[kSpecMax];  // pivots (after static perturbation) and 1 / pivot
+  double pv[kSpecMax];                // applied perturbation (static mode)
+  double lamd[kSpecMax], rmd[kSpecMax];  // diagonal-block rows: lambda part, running-max part
+  double lamw[kCT / 32][kSpecMax], rvw[kCT / 32][kSpecMax];  // per warp, rows below the block
+  double lamx[16][kSpecMax];          // per CTA partial lambda (exchange)
+  int kstar;                          // accepted speculative pivots
 };
+
+// 8-byte asynchronous global -> shared copy (no register round trip, so
+// the copies of a staging loop are all in flight at once)
+__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 }  // namespace
 
@@ -118,9 +152,13 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     S.delta = o.front_delta ? o.front_delta[s] : (o.static_delta > 0.0 ? o.static_delta : 1.4901161193847656e-08 * om);
   }
   const double orig_max = S.orig_max;
+  for (int t = threadIdx.x; t < (kCT / 32) * kSpecMax; t += kCT) {
+    sh.lamw[t / kSpecMax][t % kSpecMax] = 0.0;
+    sh.rvw[t / kSpecMax][t % kSpecMax] = 0.0;
+  }
   int n_pos = S.n_pos, n_neg = S.n_neg, n_zero = S.n_zero, nPert = S.num_perturbed;
   double pert = S.perturb;
-  double thread_rmax = 0.0;
+  double thread_rmax = S.running_max;  // includes orig_max at the first panel
   double rm_known = S.running_max;
 
   // compute current values of column `col` for this CTA's rows >= k
@@ -220,6 +258,207 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
   bool stopped = false;
   bool flush = false;
   int step = 0;
+
+  // ---- speculative panel: 1x1 pivots at k, verified against lambda after
+  // the fact (see the file comment)
+  int spec = S.spec;
+  int seq_limit = 1 << 30;  // sequential decisions allowed in this panel
+  bool run_seq = true;
+  const int np = pe - ps;
+  if (np > 0 && spec < kSpecRetry) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r0 = max(base, pe);
+    // raw diagonal block (lower triangle)
+    for (int j = 0; j < np; ++j)
+      for (int i = j + threadIdx.x; i < np; i += kCT) cp_async8(&sh.db[i][j], F + static_cast<int64_t>(ps + j) * ld + ps + i);
+    cp_async_wait_all();
+    __syncthreads();
+    // diagonal block, left-looking: warp 0 of every CTA, lane = row (the
+    // row lives in sh.db, conflict-free with the odd row stride). The sums
+    // use four partial accumulators to shorten the dependency chain; |a| of
+    // the column values go to shared memory and are reduced afterwards.
+    if (warp == 0) {
+      const double floorv = fmax(o.static_abs_floor, o.static_rel_floor * orig_max);
+      const int lr = lane < np ? lane : 0;
+      for (int c = 0; c < np; ++c) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int t = 0;
+        for (; t + 4 <= c; t += 4) {
+          s0 = fma(sh.db[lr][t], sh.wv[c][t], s0);
+          s1 = fma(sh.db[lr][t + 1], sh.wv[c][t + 1], s1);
+          s2 = fma(sh.db[lr][t + 2], sh.wv[c][t + 2], s2);
+          s3 = fma(sh.db[lr][t + 3], sh.wv[c][t + 3], s3);
+        }
+        for (; t < c; ++t) s0 = fma(sh.db[lr][t], sh.wv[c][t], s0);
+        const double a = sh.db[lr][c] - ((s0 + s1) + (s2 + s3));
+        const double akk = __shfl_sync(0xffffffffu, a, c);
+        double d = akk, applied = 0.0;
+        if (o.mode == 1) {
+          // static pivoting (dense_kernel.hpp:982-1034), as in the sequential path
+          const int sign = o.sign_final ? o.sign_final[f.fidx[ps + c]] : 0;
+          bool need;
+          if (sign > 0)
+            need = akk < floorv;
+          else if (sign < 0)
+            need = akk > -floorv;
+          else
+            need = fabs(akk) < floorv;
+          if (need) {
+            const double sg = (sign != 0) ? static_cast<double>(sign) : (akk >= 0.0 ? 1.0 : -1.0);
+            d = akk + sg * S.delta;
+            applied = d - akk;
+          }
+        }
+        const double inv = __drcp_rn(d);
+        __syncwarp();
+        if (lane > c && lane < np) {
+          const double l = a * inv;
+          sh.db[lane][c] = l;
+          sh.aabs[c][lane] = fabs(a);
+          sh.wv[lane][c] = d * l;
+        } else if (lane == c) {
+          sh.db[c][c] = d;
+        }
+        if (lane == 0) {
+          sh.dv[c] = d;
+          sh.iv[c] = inv;
+          sh.pv[c] = applied;
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    // lambda and running-max parts of the diagonal-block rows
+    if (threadIdx.x < np) {
+      const int c = threadIdx.x;
+      double lm = 0.0, rv = fabs(sh.dv[c]);
+      for (int i = c + 1; i < np; ++i) {
+        const double v = sh.aabs[c][i];
+        if (ps + i < effEnd) lm = fmax(lm, v);
+        rv = fmax(rv, v);
+      }
+      sh.lamd[c] = lm;
+      sh.rmd[c] = rv;
+    }
+    // rows below the block, left-looking: the raw panel columns of this
+    // CTA's rows are staged in Lr, then each thread walks its rows pivot by
+    // pivot (two rows interleaved), touching only its own rows, so no
+    // synchronisation is needed between pivots. Lr receives the current
+    // values a_ic = raw_ic - sum_t a_it L_ct (L = a_ic / d_c on write-back).
+    for (int c = 0; c < np; ++c)
+      for (int i = r0 + threadIdx.x; i < rend; i += kCT)
+        cp_async8(Lr + c * R + (i - base), F + static_cast<int64_t>(ps + c) * ld + i);
+    cp_async_wait_all();
+    __syncthreads();
+    for (int i0 = r0 + threadIdx.x; i0 < rend; i0 += 2 * kCT) {
+      const int i1 = i0 + kCT;
+      const bool two = i1 < rend;
+      const int l0 = i0 - base, l1 = two ? i1 - base : l0;
+      for (int c = 0; c < np; ++c) {
+        // sum_t L_it d_t L_ct = sum_t a_it L_ct (a_it = L_it d_t), two
+        // partial sums per row
+        double a0 = 0.0, b0 = 0.0, a1 = 0.0, b1 = 0.0;
+        int t = 0;
+        for (; t + 2 <= c; t += 2) {
+          const double x = sh.db[c][t], y = sh.db[c][t + 1];
+          a0 = fma(Lr[t * R + l0], x, a0);
+          b0 = fma(Lr[(t + 1) * R + l0], y, b0);
+          a1 = fma(Lr[t * R + l1], x, a1);
+          b1 = fma(Lr[(t + 1) * R + l1], y, b1);
+        }
+        if (t < c) {
+          const double x = sh.db[c][t];
+          a0 = fma(Lr[t * R + l0], x, a0);
+          a1 = fma(Lr[t * R + l1], x, a1);
+        }
+        Lr[c * R + l0] -= a0 + b0;
+        if (two) Lr[c * R + l1] -= a1 + b1;
+      }
+    }
+    __syncthreads();
+    // per pivot and warp: lambda part (eligible rows) and running-max part
+    // (all rows) of this CTA's rows below the block
+    for (int c = warp; c < np; c += kCT / 32) {
+      double lm = 0.0, rv = 0.0;
+      for (int i = r0 + lane; i < rend; i += 32) {
+        const double v = fabs(Lr[c * R + (i - base)]);
+        if (i < effEnd) lm = fmax(lm, v);
+        rv = fmax(rv, v);
+      }
+      lm = warp_max_nonneg(lm);
+      rv = warp_max_nonneg(rv);
+      if (lane == 0) {
+        sh.lamw[0][c] = lm;
+        sh.rvw[0][c] = rv;
+      }
+    }
+    __syncthreads();
+    int kstar = np;
+    if (o.mode != 1) {
+      // lambda per pivot: this CTA's part to every CTA of the cluster
+      if (threadIdx.x < np) {
+        const double lc = sh.lamw[0][threadIdx.x];
+        for (int dd = 0; dd < CS; ++dd) *cluster.map_shared_rank(&sh.lamx[q][threadIdx.x], dd) = lc;
+      }
+      cluster.sync();
+      if (warp == 0) {
+        // the sequential path's 1x1-at-k decision (dense_kernel.hpp:576-600),
+        // one lane per pivot; the first failing pivot ends the accepted prefix
+        bool fail = false;
+        if (lane < np) {
+          const double isolatedFloor = fmax(o.zero_tol, o.rel_floor * orig_max);
+          double lam = sh.lamd[lane];
+          for (int dd = 0; dd < CS; ++dd) lam = fmax(lam, sh.lamx[dd][lane]);
+          const double akk = sh.dv[lane];
+          const bool pass = (lam <= o.zero_tol) ? (fabs(akk) > isolatedFloor) : (fabs(akk) >= kAlphaBK * lam);
+          fail = !pass;
+        }
+        const unsigned bad = __ballot_sync(0xffffffffu, fail);
+        if (lane == 0) sh.kstar = bad ? __ffs(bad) - 1 : np;
+      }
+      __syncthreads();
+      kstar = sh.kstar;
+    }
+    if (kstar > 0) {
+      for (int c = 0; c < kstar; ++c) {
+        const double iv = sh.iv[c];
+        for (int i = r0 + threadIdx.x; i < rend; i += kCT) F[static_cast<int64_t>(ps + c) * ld + i] = Lr[c * R + (i - base)] * iv;
+      }
+      if (q == 0) {
+        for (int c = 0; c < kstar; ++c)
+          for (int i = c + threadIdx.x; i < np; i += kCT) F[static_cast<int64_t>(ps + c) * ld + ps + i] = sh.db[i][c];
+        for (int c = threadIdx.x; c < kstar; c += kCT) {
+          f.Dd[ps + c] = sh.dv[c];
+          f.Do[ps + c] = 0.0;
+          f.pk[ps + c] = 0;
+        }
+      }
+      for (int c = 0; c < kstar; ++c) {
+        const double d = sh.dv[c];
+        if (d > 0)
+          ++n_pos;
+        else if (d < 0)
+          ++n_neg;
+        else
+          ++n_zero;
+        if (sh.pv[c] != 0.0) {
+          pert += fabs(sh.pv[c]);
+          ++nPert;
+        }
+      }
+      if (threadIdx.x < kstar) {
+        // running max of the accepted columns (one thread per column)
+        thread_rmax = fmax(thread_rmax, fmax(sh.rmd[threadIdx.x], sh.rvw[0][threadIdx.x]));
+      }
+      k = ps + kstar;
+      run_seq = false;
+      spec = 0;
+    } else {
+      seq_limit = 1;  // the first pivot needs the sequential decision
+      spec += 1;
+    }
+  }
+  int decisions = 0, nontrivial = 0;
   // prefetched raw values of column k for this thread's rows
   constexpr int kPF = 4;
   double pf[kPF];
@@ -250,7 +489,7 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     for (int t = threadIdx.x; t <= p; t += kCT) {
       double v;
       if (t == p) {
-        v = d * (vk1 / d);
+        v = d * (vk1 * (1.0 / d));
       } else {
         const int kind = sh.pk[t];
         if (kind == 0)
@@ -272,11 +511,12 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     else
       ++n_zero;
     thread_rmax = fmax(thread_rmax, fabs(d));
+    const double inv = 1.0 / d;
     for (int i = max(base, k + 1) + threadIdx.x; i < rend; i += kCT) {
       const int li = i - base;
       const double a = col[li];
       thread_rmax = fmax(thread_rmax, fabs(a));
-      const double l = a / d;
+      const double l = a * inv;
       Lr[p * R + li] = l;
       F[k * ld + i] = l;
     }
@@ -293,7 +533,9 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     }
   };
 
-  while (k < pe) {
+  while (run_seq && k < pe) {
+    if (decisions >= seq_limit) break;
+    ++decisions;
     const int p = k - ps;
     const int b = step & 1;
     ++step;
@@ -413,6 +655,7 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
       // the exchange slots before anyone writes them again
       cluster.sync();
     }
+    if (dec != 0) ++nontrivial;
     if (dec == 3) {
       stopped = true;
       break;
@@ -508,15 +751,9 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     }
   }
 
-  // ---- finish: cluster-wide running max; state written by rank 0
-  __threadfence();
+  // ---- finish: running max by a global atomic (monotone), state by rank 0
   const double lmax = block_max<kCT>(thread_rmax, sh.red_v);
-  cluster.sync();
-  if (threadIdx.x == 0)
-    for (int dd = 0; dd < CS; ++dd) remote(sh.ex_v, dd)[q] = lmax;
-  cluster.sync();
-  double rmax = 0.0;
-  for (int dd = 0; dd < CS; ++dd) rmax = fmax(rmax, sh.ex_v[dd]);
+  if (threadIdx.x == 0) atomic_max_nonneg(&st[s].running_max, lmax);
   const bool done = stopped || k >= effEnd;
   if (done)
     for (int t = q * kCT + threadIdx.x; t < m; t += CS * kCT) f.lpos[f.lperm[t]] = t;
@@ -524,7 +761,6 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     FrontState& W = st[s];
     W.orig_max = orig_max;
     W.delta = S.delta;
-    W.running_max = fmax(S.running_max, rmax);
     W.n_pos = n_pos;
     W.n_neg = n_neg;
     W.n_zero = n_zero;
@@ -536,6 +772,13 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     W.ob = S.ob;
     W.ob_end = S.ob_end;
     W.far = (done || flush || k >= S.ob_end) ? 1 : 0;
+    // a whole sequential panel without interchanges or 2x2 pivots: try
+    // speculation again next time
+    W.spec = (spec >= kSpecRetry && run_seq && nontrivial == 0) ? 0 : spec;
+    if (!run_seq)
+      atomicAdd(k - ps == np ? &g->spec_full : &g->spec_partial, 1);
+    else
+      atomicAdd(seq_limit == 1 ? &g->spec_failed : &g->seq_panels, 1);
     int flags = flush ? kFlagFlush : 0;
     if (done) {
       flags |= kFlagDone;
@@ -555,10 +798,15 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
   cluster.sync();
 }
 
-int cluster_size_for(int max_m) {
-  const size_t limit = 190 * 1024;
-  if (static_cast<size_t>((max_m + 7) / 8) * (kPanelWidth + 4) * sizeof(double) <= limit) return 8;
-  if (static_cast<size_t>((max_m + 15) / 16) * (kPanelWidth + 4) * sizeof(double) <= limit) return 16;
+int cluster_size_for(int max_m, int count) {
+  const size_t limit = 184 * 1024;  // + the static ClusterShared (~38 KB) <= 227 KB
+  const bool fits8 = static_cast<size_t>((max_m + 7) / 8) * (kPanelWidth + 4) * sizeof(double) <= limit;
+  const bool fits16 = static_cast<size_t>((max_m + 15) / 16) * (kPanelWidth + 4) * sizeof(double) <= limit;
+  // The panel is latency- and per-SM-traffic-bound: 16 CTAs halve each
+  // CTA's rows. Use them when every front of the launch still gets its
+  // cluster in one wave over the 148 SMs, and for fronts too tall for 8.
+  if (fits16 && (!fits8 || (max_m >= 768 && count * 16 <= 144))) return 16;
+  if (fits8) return 8;
   return 0;  // too large for the cluster kernel
 }
 
@@ -568,9 +816,9 @@ size_t cluster_panel_smem(int max_m, int nb, int cs) {
 }
 
 cudaError_t configure_cluster_panel() {
-  cudaError_t e = cudaFuncSetAttribute(cluster_panel_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(cluster_panel_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 184 * 1024);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(cluster_panel_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  e = cudaFuncSetAttribute(cluster_panel_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 184 * 1024);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(cluster_panel_kernel<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
@@ -579,7 +827,7 @@ cudaError_t launch_cluster_panel(const FrontDesc* fronts, FrontState* st, const 
                                  int nb, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
                                  cudaStream_t stream) {
   if (count <= 0) return cudaSuccess;
-  const int cs = cluster_size_for(max_m);
+  const int cs = cluster_size_for(max_m, count);
   const int R = (max_m + cs - 1) / cs;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cs * count);

@@ -65,6 +65,17 @@ __device__ __forceinline__ double block_max(double v, double* sv) {
   return r;
 }
 
+// Warp max of non-negative doubles (NaN, whose pattern is larger, wins):
+// the bit patterns order like the values, so two 32-bit reductions on the
+// high and then the low word give the exact maximum.
+__device__ __forceinline__ double warp_max_nonneg(double v) {
+  const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(v));
+  const unsigned hi = static_cast<unsigned>(b >> 32), lo = static_cast<unsigned>(b);
+  const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+  return __longlong_as_double(static_cast<long long>((static_cast<unsigned long long>(mh) << 32) | ml));
+}
+
 // atomicMax for non-negative doubles (IEEE order == integer order there).
 __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
   if (!(v >= 0.0)) return;

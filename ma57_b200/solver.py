@@ -525,7 +525,8 @@ class SymLDLT:
         return list(buf)
 
     def plan_stats(self):
-        buf = (C.c_double * 7)()
-        L.load().symla_gpu_plan_stats(self._ctx.h, buf, 7)
-        keys = ["fronts", "levels", "max_m", "sum_m2", "factor_flops", "nnz_L", "arena_doubles"]
+        buf = (C.c_double * 11)()
+        L.load().symla_gpu_plan_stats(self._ctx.h, buf, 11)
+        keys = ["fronts", "levels", "max_m", "sum_m2", "factor_flops", "nnz_L", "arena_doubles",
+                "panels_spec_full", "panels_spec_prefix", "panels_spec_failed", "panels_sequential"]
         return dict(zip(keys, list(buf)))
