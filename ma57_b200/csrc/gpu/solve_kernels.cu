@@ -100,19 +100,54 @@ __global__ void permute_out_kernel(int n, int nrhs, const int* __restrict__ perm
   Xout[perm[i] + static_cast<long long>(c) * ldx] = X[t];
 }
 
+// Shared-memory layout of both pipelined kernels (dynamic, doubles):
+//   acc[kRB][kRhsChunk + 1]   the task's result block
+//   xb [kRB][kRhsChunk + 1]   the right-hand-side block of the current tile
+//   Lb [2][kRB][kRB + 1]      double-buffered L tiles (odd stride: rows and
+//                             columns are both conflict-free)
+// Every L tile a task needs is known from its position alone, so the next
+// tile is copied (cp.async) while the current one is used and before the
+// flag that guards its right-hand side is awaited.
+constexpr int kAccStride = kRhsChunk + 1;
+constexpr int kTileStride = kRB + 1;
+constexpr size_t kSolveSmem = (2 * kRB * kAccStride + 2 * kRB * kTileStride) * sizeof(double);
+
+__device__ __forceinline__ void scp_async8(double* smem_dst, const double* gsrc) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void scp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void scp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Tile (rows [i0, i0 + ni), columns [j0, j0 + nj)) of a front into T,
+// T[ii * kTileStride + jj]; entries outside the ranges are zero.
+__device__ __forceinline__ void stage_tile(double* T, const double* F, int64_t ld, int i0, int ni, int j0, int nj) {
+  for (int t = threadIdx.x; t < kRB * kRB; t += kST) {
+    const int ii = t % kRB, jj = t / kRB;
+    double* d = T + ii * kTileStride + jj;
+    if (ii < ni && jj < nj)
+      scp_async8(d, F + static_cast<int64_t>(j0 + jj) * ld + i0 + ii);
+    else
+      *d = 0.0;
+  }
+  scp_commit();
+}
+
 // Forward task = (front, row block); flag of a pivot row block at
 // flag_base[front] + row block.
 __global__ void __launch_bounds__(kST) forward_pipelined_kernel(
     const FrontDesc* __restrict__ fronts, const ChildLink* __restrict__ links, const FrontState* __restrict__ st,
     const int2* __restrict__ tasks, int ntasks, const int* __restrict__ flag_base, int* flags, int epoch, int* err,
     int nrhs, int c0, const double* __restrict__ Bp, int n) {
-  __shared__ double acc[kRB][kRhsChunk + 1];
-  // the staged y block (step 2) and the diagonal L block (step 3) are never
-  // live at the same time
-  __shared__ double stage[kRB * (kRB + 1)];
-  double(*yb)[kRhsChunk + 1] = reinterpret_cast<double(*)[kRhsChunk + 1]>(stage);
-  double(*Ld)[kRB + 1] = reinterpret_cast<double(*)[kRB + 1]>(stage);
+  extern __shared__ double ssm[];
+  double* acc = ssm;
+  double* xb = acc + kRB * kAccStride;
+  double* Lb0 = xb + kRB * kAccStride;
   const int nc = min(kRhsChunk, nrhs - c0);
+  const int row = threadIdx.x % kRB, cg = threadIdx.x / kRB;  // product layout: a row, 4 right-hand sides
   for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
     if (ld_acquire(err) != 0) return;
     const int s = tasks[task].x, rb = tasks[task].y;
@@ -122,6 +157,21 @@ __global__ void __launch_bounds__(kST) forward_pipelined_kernel(
     const int64_t ld = f.ld;
     double* W = f.W;
     const int wld = f.wld;
+    const int nbp = (np + kRB - 1) / kRB;
+    const int jend = min(rb, nbp);
+    const bool hasDiag = r0 < np;
+    const int ntiles = jend + (hasDiag ? 1 : 0);
+    // tile tt: pivot block tt (tt < jend) or the diagonal block
+    auto stage = [&](int tt) {
+      double* T = Lb0 + (tt & 1) * kRB * kTileStride;
+      if (tt < jend) {
+        const int j0 = tt * kRB;
+        stage_tile(T, f.F, ld, r0, nr, j0, min(j0 + kRB, np) - j0);
+      } else {
+        stage_tile(T, f.F, ld, r0, nr, r0, min(r1, np) - r0);
+      }
+    };
+    if (ntiles > 0) stage(0);
     // 1. Bp for pivot rows plus the children's forwarded rows, gathered
     //    through each row's pre-pivot position
     for (int t = threadIdx.x; t < nr * nc; t += kST) {
@@ -137,65 +187,81 @@ __global__ void __launch_bounds__(kST) forward_pipelined_kernel(
         const int cnp = st[L.child].npiv;
         v += cf.W[cnp + a + static_cast<int64_t>(c0 + c) * cf.wld];
       }
-      acc[ii][c] = v;
+      acc[ii * kAccStride + c] = v;
+    }
+    for (int tt = 0; tt < ntiles; ++tt) {
+      const bool more = tt + 1 < ntiles;
+      if (more) stage(tt + 1);
+      double* T = Lb0 + (tt & 1) * kRB * kTileStride;
+      if (tt < jend) {
+        // 2. contribution of finished pivot block j = tt
+        const int j = tt;
+        if (!wait_flag(flags, flag_base[s] + j, epoch, err)) {
+          scp_wait<0>();
+          return;
+        }
+        const int j0 = j * kRB, nj = min(j0 + kRB, np) - j0;
+        for (int t = threadIdx.x; t < kRB * nc; t += kST) {
+          const int jj = t % kRB, c = t / kRB;
+          xb[jj * kAccStride + c] = (jj < nj) ? W[j0 + jj + static_cast<int64_t>(c0 + c) * wld] : 0.0;
+        }
+        if (more)
+          scp_wait<1>();
+        else
+          scp_wait<0>();
+        __syncthreads();
+        // a 2x2 pivot straddling the block boundary: its d21 slot in L is
+        // not an L entry
+        if (threadIdx.x == 0 && j == rb - 1 && r0 - 1 >= j0 && f.pk[r0 - 1] == 1) T[0 * kTileStride + (r0 - 1 - j0)] = 0.0;
+        __syncthreads();
+        if (row < nr) {
+          double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
+          const int cb4 = cg * 4;
+          for (int jj = 0; jj < nj; ++jj) {
+            const double l = T[row * kTileStride + jj];
+            const double* y = xb + jj * kAccStride + cb4;
+            p0 = fma(l, y[0], p0);
+            p1 = fma(l, y[1], p1);
+            p2 = fma(l, y[2], p2);
+            p3 = fma(l, y[3], p3);
+          }
+          double* a = acc + row * kAccStride + cb4;
+          if (cb4 + 0 < nc) a[0] -= p0;
+          if (cb4 + 1 < nc) a[1] -= p1;
+          if (cb4 + 2 < nc) a[2] -= p2;
+          if (cb4 + 3 < nc) a[3] -= p3;
+        }
+        __syncthreads();
+      } else {
+        // 3. the block's own pivot columns: unit-lower solve for its pivot
+        //    rows and the matching update of its non-pivot rows
+        scp_wait<0>();
+        __syncthreads();
+        const int npv = min(r1, np) - r0;
+        if (threadIdx.x < npv - 1 && f.pk[r0 + threadIdx.x] == 1)
+          T[(threadIdx.x + 1) * kTileStride + threadIdx.x] = 0.0;  // d21 slot of a 2x2 pivot
+        __syncthreads();
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for (int c = warp; c < nc; c += kST / 32) {
+          double y0 = (lane < nr) ? acc[lane * kAccStride + c] : 0.0;
+          double y1 = (lane + 32 < nr) ? acc[(lane + 32) * kAccStride + c] : 0.0;
+          for (int jj = 0; jj < npv; ++jj) {
+            const double yj = __shfl_sync(0xffffffffu, jj < 32 ? y0 : y1, jj & 31);
+            if (lane > jj) y0 -= T[lane * kTileStride + jj] * yj;
+            if (lane + 32 > jj) y1 -= T[(lane + 32) * kTileStride + jj] * yj;
+          }
+          if (lane < nr) acc[lane * kAccStride + c] = y0;
+          if (lane + 32 < nr) acc[(lane + 32) * kAccStride + c] = y1;
+        }
+        __syncthreads();
+      }
     }
     __syncthreads();
-    // 2. contributions of the finished pivot blocks before this row block
-    const int nbp = (np + kRB - 1) / kRB;
-    const int jend = min(rb, nbp);
-    for (int j = 0; j < jend; ++j) {
-      if (!wait_flag(flags, flag_base[s] + j, epoch, err)) return;
-      const int j0 = j * kRB, j1 = min(j0 + kRB, np), nj = j1 - j0;
-      for (int t = threadIdx.x; t < nj * nc; t += kST) {
-        const int jj = t % nj, c = t / nj;
-        yb[jj][c] = W[j0 + jj + static_cast<int64_t>(c0 + c) * wld];
-      }
-      __syncthreads();
-      for (int t = threadIdx.x; t < nr * nc; t += kST) {
-        const int ii = t % nr, c = t / nr;
-        const int i = r0 + ii;
-        double sacc = 0.0;
-        for (int jj = 0; jj < nj; ++jj) {
-          const int jc = j0 + jj;
-          if (i == jc + 1 && f.pk[jc] == 1) continue;
-          sacc += f.F[jc * ld + i] * yb[jj][c];
-        }
-        acc[ii][c] -= sacc;
-      }
-      __syncthreads();
-    }
-    // 3. the block's own pivot columns: unit-lower solve for its pivot rows
-    //    and the matching update of its non-pivot rows
-    if (r0 < np) {
-      const int npv = min(r1, np) - r0;
-      for (int t = threadIdx.x; t < kRB * kRB; t += kST) {
-        const int ii = t % kRB, jj = t / kRB;
-        const int i = r0 + ii, jc = r0 + jj;
-        double l = 0.0;
-        if (ii < nr && jj < npv && i > jc) l = f.F[jc * ld + i];
-        if (ii < nr && jj < npv && i == jc + 1 && f.pk[jc] == 1) l = 0.0;
-        Ld[ii][jj] = l;
-      }
-      __syncthreads();
-      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-      for (int c = warp; c < nc; c += kST / 32) {
-        double y0 = (lane < nr) ? acc[lane][c] : 0.0;
-        double y1 = (lane + 32 < nr) ? acc[lane + 32][c] : 0.0;
-        for (int jj = 0; jj < npv; ++jj) {
-          const double yj = __shfl_sync(0xffffffffu, jj < 32 ? y0 : y1, jj & 31);
-          if (lane > jj) y0 -= Ld[lane][jj] * yj;
-          if (lane + 32 > jj) y1 -= Ld[lane + 32][jj] * yj;
-        }
-        if (lane < nr) acc[lane][c] = y0;
-        if (lane + 32 < nr) acc[lane + 32][c] = y1;
-      }
-      __syncthreads();
-    }
     for (int t = threadIdx.x; t < nr * nc; t += kST) {
       const int ii = t % nr, c = t / nr;
-      W[r0 + ii + static_cast<int64_t>(c0 + c) * wld] = acc[ii][c];
+      W[r0 + ii + static_cast<int64_t>(c0 + c) * wld] = acc[ii * kAccStride + c];
     }
-    if (r0 < np) publish(flags, flag_base[s] + rb, epoch);
+    if (hasDiag) publish(flags, flag_base[s] + rb, epoch);
     __syncthreads();
   }
 }
@@ -206,14 +272,14 @@ __global__ void __launch_bounds__(kST) backward_pipelined_kernel(
     const FrontDesc* __restrict__ fronts, const FrontState* __restrict__ st, const int2* __restrict__ tasks,
     int ntasks, const int* __restrict__ flag_base, int* flags, int epoch, int* err, int nrhs, int c0,
     double* __restrict__ X, int n) {
-  __shared__ double acc[kRB][kRhsChunk + 1];
-  // staged x rows (step 2) and the diagonal L block (step 3) share storage
-  __shared__ double stage[kRB * (kRB + 1)];
-  double(*xb)[kRhsChunk + 1] = reinterpret_cast<double(*)[kRhsChunk + 1]>(stage);
-  double(*Ld)[kRB + 1] = reinterpret_cast<double(*)[kRB + 1]>(stage);
+  extern __shared__ double ssm[];
+  double* acc = ssm;
+  double* xb = acc + kRB * kAccStride;
+  double* Lb0 = xb + kRB * kAccStride;
   const int nc = min(kRhsChunk, nrhs - c0);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int NW = kST / 32;
+  const int col = threadIdx.x % kRB, cg = threadIdx.x / kRB;
   for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
     if (ld_acquire(err) != 0) return;
     const int s = tasks[task].x, cb = tasks[task].y;
@@ -223,6 +289,31 @@ __global__ void __launch_bounds__(kST) backward_pipelined_kernel(
     const int64_t ld = f.ld;
     const double* W = f.W;
     const int wld = f.wld;
+    const int nbp = (np + kRB - 1) / kRB;
+    // tiles: the ancestor rows [np, m) in chunks, then the later pivot
+    // blocks nbp-1 .. cb+1, then the diagonal block
+    const int nanc = (m - np + kRB - 1) / kRB;
+    const int nlater = nbp - 1 - cb;
+    const int ntiles = nanc + nlater + 1;
+    auto tile_rows = [&](int tt, int& i0, int& i1) {
+      if (tt < nanc) {
+        i0 = np + tt * kRB;
+        i1 = min(i0 + kRB, m);
+      } else if (tt < nanc + nlater) {
+        const int j = nbp - 1 - (tt - nanc);
+        i0 = j * kRB;
+        i1 = min(i0 + kRB, np);
+      } else {
+        i0 = q0;
+        i1 = q1;
+      }
+    };
+    auto stage = [&](int tt) {
+      int i0, i1;
+      tile_rows(tt, i0, i1);
+      stage_tile(Lb0 + (tt & 1) * kRB * kTileStride, f.F, ld, i0, i1 - i0, q0, nq);
+    };
+    stage(0);
     // 1. z = D^{-1} y for the block's pivots (a 2x2 partner may sit in the
     //    neighbouring block; y is complete in W after the forward pass)
     for (int t = threadIdx.x; t < nq * nc; t += kST) {
@@ -242,82 +333,82 @@ __global__ void __launch_bounds__(kST) backward_pipelined_kernel(
         const double det = d11 * d22 - d21 * d21;
         z = (-d21 * w[q - 1] + d11 * w[q]) / det;
       }
-      acc[qq][c] = z;
+      acc[qq * kAccStride + c] = z;
     }
-    __syncthreads();
-    // 2. minus L(rows below, block)^T x(rows below): the ancestor rows
-    //    [np, m) are final from earlier levels; later pivot blocks of this
-    //    front are waited for.
-    const int nbp = (np + kRB - 1) / kRB;
-    for (int j = nbp; j > cb; --j) {
+    for (int tt = 0; tt < ntiles; ++tt) {
+      const bool more = tt + 1 < ntiles;
+      if (more) stage(tt + 1);
+      double* T = Lb0 + (tt & 1) * kRB * kTileStride;
       int i0, i1;
-      if (j == nbp) {
-        i0 = np;
-        i1 = m;
+      tile_rows(tt, i0, i1);
+      if (tt < nanc + nlater) {
+        // 2. minus L(rows of the tile, block)^T x(rows of the tile): the
+        //    ancestor rows are final from earlier levels; later pivot blocks
+        //    of this front are waited for
+        if (tt >= nanc) {
+          const int j = nbp - 1 - (tt - nanc);
+          if (!wait_flag(flags, flag_base[s] + j, epoch, err)) {
+            scp_wait<0>();
+            return;
+          }
+        }
+        const int ni = i1 - i0;
+        for (int t = threadIdx.x; t < kRB * nc; t += kST) {
+          const int ii = t % kRB, c = t / kRB;
+          xb[ii * kAccStride + c] = (ii < ni) ? X[f.fidx[i0 + ii] + static_cast<int64_t>(c0 + c) * n] : 0.0;
+        }
+        if (more)
+          scp_wait<1>();
+        else
+          scp_wait<0>();
+        __syncthreads();
+        // a 2x2 pivot straddling the block boundary: d21 is not an L entry
+        if (threadIdx.x == 0 && i0 == q1 && nq > 0 && f.pk[q1 - 1] == 1) T[0 * kTileStride + (nq - 1)] = 0.0;
+        __syncthreads();
+        if (col < nq) {
+          double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
+          const int cb4 = cg * 4;
+          for (int ii = 0; ii < ni; ++ii) {
+            const double l = T[ii * kTileStride + col];
+            const double* x = xb + ii * kAccStride + cb4;
+            p0 = fma(l, x[0], p0);
+            p1 = fma(l, x[1], p1);
+            p2 = fma(l, x[2], p2);
+            p3 = fma(l, x[3], p3);
+          }
+          double* a = acc + col * kAccStride + cb4;
+          if (cb4 + 0 < nc) a[0] -= p0;
+          if (cb4 + 1 < nc) a[1] -= p1;
+          if (cb4 + 2 < nc) a[2] -= p2;
+          if (cb4 + 3 < nc) a[3] -= p3;
+        }
+        __syncthreads();
       } else {
-        if (!wait_flag(flags, flag_base[s] + j, epoch, err)) return;
-        i0 = j * kRB;
-        i1 = min(i0 + kRB, np);
-      }
-      for (int base = i0; base < i1; base += kRB) {
-        const int ni = min(kRB, i1 - base);
-        for (int t = threadIdx.x; t < ni * nc; t += kST) {
-          const int ii = t % ni, c = t / ni;
-          xb[ii][c] = X[f.fidx[base + ii] + static_cast<int64_t>(c0 + c) * n];
-        }
+        // 3. transposed unit-lower solve on the diagonal block
+        scp_wait<0>();
         __syncthreads();
-        for (int qq = warp; qq < nq; qq += NW) {  // warp per column, lanes over rows
-          const int q = q0 + qq;
-          const double* Lq = f.F + q * ld;
-          double part[kRhsChunk];
-#pragma unroll
-          for (int c = 0; c < kRhsChunk; ++c) part[c] = 0.0;
-          for (int ii = lane; ii < ni; ii += 32) {
-            const int i = base + ii;
-            double l = Lq[i];
-            if (i == q + 1 && f.pk[q] == 1) l = 0.0;
-#pragma unroll
-            for (int c = 0; c < kRhsChunk; ++c)
-              if (c < nc) part[c] += l * xb[ii][c];
+        if (threadIdx.x < nq - 1 && f.pk[q0 + threadIdx.x] == 1)
+          T[(threadIdx.x + 1) * kTileStride + threadIdx.x] = 0.0;  // d21 slot of a 2x2 pivot
+        __syncthreads();
+        for (int c = warp; c < nc; c += NW) {
+          double x0 = (lane < nq) ? acc[lane * kAccStride + c] : 0.0;
+          double x1 = (lane + 32 < nq) ? acc[(lane + 32) * kAccStride + c] : 0.0;
+          for (int jj = nq - 1; jj >= 0; --jj) {
+            // x[jj] is final once every row below it has been applied; row jj
+            // of Ltop then updates the unknowns above it
+            const double xj = __shfl_sync(0xffffffffu, jj < 32 ? x0 : x1, jj & 31);
+            if (lane < jj) x0 -= T[jj * kTileStride + lane] * xj;
+            if (lane + 32 < jj) x1 -= T[jj * kTileStride + lane + 32] * xj;
           }
-#pragma unroll
-          for (int c = 0; c < kRhsChunk; ++c) {
-            double v = part[c];
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-            if (lane == 0 && c < nc) acc[qq][c] -= v;
-          }
+          if (lane < nq) acc[lane * kAccStride + c] = x0;
+          if (lane + 32 < nq) acc[(lane + 32) * kAccStride + c] = x1;
         }
         __syncthreads();
       }
     }
-    // 3. transposed unit-lower solve on the diagonal block
-    for (int t = threadIdx.x; t < kRB * kRB; t += kST) {
-      const int ii = t % kRB, jj = t / kRB;
-      const int i = q0 + ii, jc = q0 + jj;
-      double l = 0.0;
-      if (ii < nq && jj < nq && i > jc) l = f.F[jc * ld + i];
-      if (ii < nq && jj < nq && i == jc + 1 && f.pk[jc] == 1) l = 0.0;
-      Ld[ii][jj] = l;
-    }
-    __syncthreads();
-    for (int c = warp; c < nc; c += NW) {
-      double x0 = (lane < nq) ? acc[lane][c] : 0.0;
-      double x1 = (lane + 32 < nq) ? acc[lane + 32][c] : 0.0;
-      for (int jj = nq - 1; jj >= 0; --jj) {
-        // x[jj] is final once every row below it has been applied; row jj of
-        // Ltop then updates the unknowns above it
-        const double xj = __shfl_sync(0xffffffffu, jj < 32 ? x0 : x1, jj & 31);
-        if (lane < jj) x0 -= Ld[jj][lane] * xj;
-        if (lane + 32 < jj) x1 -= Ld[jj][lane + 32] * xj;
-      }
-      if (lane < nq) acc[lane][c] = x0;
-      if (lane + 32 < nq) acc[lane + 32][c] = x1;
-    }
-    __syncthreads();
     for (int t = threadIdx.x; t < nq * nc; t += kST) {
       const int qq = t % nq, c = t / nq;
-      X[f.fidx[q0 + qq] + static_cast<int64_t>(c0 + c) * n] = acc[qq][c];
+      X[f.fidx[q0 + qq] + static_cast<int64_t>(c0 + c) * n] = acc[qq * kAccStride + c];
     }
     publish(flags, flag_base[s] + cb, epoch);
     __syncthreads();
@@ -383,9 +474,15 @@ cudaError_t solve_max_resident(int device, int* fwd_ctas, int* bwd_ctas) {
   int sms = 0, a = 0, b = 0;
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, forward_pipelined_kernel, kST, 0);
+  e = cudaFuncSetAttribute(forward_pipelined_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(kSolveSmem));
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, backward_pipelined_kernel, kST, 0);
+  e = cudaFuncSetAttribute(backward_pipelined_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(kSolveSmem));
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, forward_pipelined_kernel, kST, kSolveSmem);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, backward_pipelined_kernel, kST, kSolveSmem);
   if (e != cudaSuccess) return e;
   *fwd_ctas = a * sms;
   *bwd_ctas = b * sms;
@@ -401,7 +498,7 @@ cudaError_t launch_forward_pipelined(const FrontDesc* fronts, const ChildLink* l
                   (void*)&flag_base, (void*)&flags, (void*)&epoch, (void*)&err, (void*)&nrhs,
                   (void*)&c0,     (void*)&Bp,    (void*)&n};
   return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(forward_pipelined_kernel), dim3(grid), dim3(kST),
-                                     args, 0, stream);
+                                     args, kSolveSmem, stream);
 }
 
 cudaError_t launch_backward_pipelined(const FrontDesc* fronts, const FrontState* st, const int2* tasks, int ntasks,
@@ -411,7 +508,7 @@ cudaError_t launch_backward_pipelined(const FrontDesc* fronts, const FrontState*
   void* args[] = {(void*)&fronts, (void*)&st,  (void*)&tasks, (void*)&ntasks, (void*)&flag_base, (void*)&flags,
                   (void*)&epoch,  (void*)&err, (void*)&nrhs,  (void*)&c0,     (void*)&X,         (void*)&n};
   return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(backward_pipelined_kernel), dim3(grid), dim3(kST),
-                                     args, 0, stream);
+                                     args, kSolveSmem, stream);
 }
 
 void launch_permute_in(int n, int nrhs, const int* perm, const double* B, int ldb, double* Bp, cudaStream_t stream) {
