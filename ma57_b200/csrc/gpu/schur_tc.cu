@@ -322,15 +322,28 @@ __global__ void __launch_bounds__(kThreads, 1) tc_far_update_kernel(const FrontD
     const int nchunks = (K + kBoxK - 1) / kBoxK;
     const CUtensorMap* map = maps + fi;
 
+    // the tile's C region into L2 while the operands stream in (the
+    // epilogue then reads it from L2): warp w's 32 rows of each column are
+    // 256 contiguous bytes; lane l covers columns 4l .. 4l + 3
+    {
+      const int rb = i0 + warp * 32;
+      if (rb < m)
+        for (int q = 0; q < 4; ++q) {
+          const int gj = j0 + lane * 4 + q;
+          if (gj < m && gj <= rb + 31) {
+            const double* colp = f.F + static_cast<int64_t>(gj) * f.ld + rb;
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(colp));
+            if (rb + 16 < m) asm volatile("prefetch.global.L2 [%0];" ::"l"(colp + 16));
+          }
+        }
+    }
     if (threadIdx.x == 0) {
-      // producer + MMA issuer
-      for (int c = 0; c < nchunks && ok; ++c) {
+      // producer + MMA issuer: chunk c + 1's copy is in flight while chunk
+      // c is waited for and multiplied
+      auto issue = [&](int c) -> bool {
         const int st_i = c % kStages;
         if (issued[st_i]) {
-          if (!mbar_wait(&empty_bar[st_i], empty_phase[st_i], err)) {
-            ok = false;
-            break;
-          }
+          if (!mbar_wait(&empty_bar[st_i], empty_phase[st_i], err)) return false;
           empty_phase[st_i] ^= 1;
           issued[st_i] = 0;
         }
@@ -342,6 +355,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_far_update_kernel(const FrontD
         tma_load_2d(base + 2 * kTM * kBoxK * 4, map, 2 * kTcKpad + xk, j0, &full_bar[st_i]);  // W_hi rows j
         tma_load_2d(base + 3 * kTM * kBoxK * 4, map, 3 * kTcKpad + xk, j0, &full_bar[st_i]);  // W_lo rows j
         loading[st_i] = 1;
+        return true;
+      };
+      if (!issue(0)) ok = false;
+      for (int c = 0; c < nchunks && ok; ++c) {
+        const int st_i = c % kStages;
+        if (c + 1 < nchunks && !issue(c + 1)) {
+          ok = false;
+          break;
+        }
+        unsigned char* base = ring + st_i * kStageBytes;
         if (!mbar_wait(&full_bar[st_i], full_phase[st_i], err)) {
           ok = false;
           break;
@@ -388,13 +411,21 @@ __global__ void __launch_bounds__(kThreads, 1) tc_far_update_kernel(const FrontD
     for (int cc = 0; cc < kTN; cc += 32) {
       uint32_t r[32];
       tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + cc, r);
+      // all 32 loads of the chunk before any store (the front pointer may
+      // alias as far as the compiler knows, so interleaving would serialise)
+      double cv[32];
+      double* p0 = f.F + static_cast<int64_t>(j0 + cc) * ld + gi;
+#pragma unroll
+      for (int jj = 0; jj < 32; ++jj) {
+        const int gj = j0 + cc + jj;
+        cv[jj] = (gi < m && gj < m && gi >= gj) ? p0[jj * ld] : 0.0;
+      }
 #pragma unroll
       for (int jj = 0; jj < 32; ++jj) {
         const int gj = j0 + cc + jj;
         if (gi < m && gj < m && gi >= gj) {
-          double* p = f.F + gj * ld + gi;
-          const double v = *p - static_cast<double>(__uint_as_float(r[jj]));
-          *p = v;
+          const double v = cv[jj] - static_cast<double>(__uint_as_float(r[jj]));
+          p0[jj * ld] = v;
           tmax = fmax(tmax, fabs(v));
         }
       }
