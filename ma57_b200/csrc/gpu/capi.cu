@@ -1043,19 +1043,47 @@ void ensure_solve_tasks(symla_gpu_ctx* c) {
   }
   dfree(c->d_flag_base);
   c->d_flag_base = dupload(fbase, c->stream);
+  // Task shapes per level. Forward: one row block per task (the non-pivot
+  // row blocks of a front run concurrently). Backward: with many fronts (at
+  // least two per resident CTA) a small front is one task, whose blocks run
+  // in order in one CTA with no waits on other CTAs; otherwise a task is one
+  // block, and a block with many ancestor-row chunks is split into parts
+  // (helpers first) so that one CTA does not walk all of them.
+  int slots = 0;
   for (auto& L : c->levels) {
     L.fwd_tasks.clear();
     L.bwd_tasks.clear();
+    const bool whole = static_cast<int>(L.all.size()) >= 2 * std::min(c->fwd_resident, c->bwd_resident);
     for (int s : L.all) {
       const int m = c->hdesc[s].m;
-      for (int rb = 0; rb * RB < m; ++rb) L.fwd_tasks.push_back(make_int2(s, rb));
       const int nbp = (np[s] + RB - 1) / RB;
-      for (int cb = nbp - 1; cb >= 0; --cb) L.bwd_tasks.push_back(make_int2(s, cb));
+      for (int rb = 0; rb * RB < m; ++rb) L.fwd_tasks.push_back(make_int4(s, rb, 0, 0));
+      if (whole && m <= 8 * RB) {
+        if (nbp > 0) L.bwd_tasks.push_back(make_int4(s, -1, 0, 0));
+        continue;
+      }
+      const int nanc = (m - np[s] + RB - 1) / RB;
+      const int P = std::max(1, std::min(8, nanc / 4));
+      for (int cb = nbp - 1; cb >= 0; --cb) {
+        const int h0 = slots;
+        for (int p = 1; p < P; ++p) L.bwd_tasks.push_back(make_int4(s, cb, p, (P << 20) | (h0 + p - 1)));
+        L.bwd_tasks.push_back(make_int4(s, cb, 0, (P << 20) | h0));
+        slots += P - 1;
+      }
     }
     dfree(L.d_fwd_tasks);
     dfree(L.d_bwd_tasks);
     L.d_fwd_tasks = dupload(L.fwd_tasks, c->stream);
     L.d_bwd_tasks = dupload(L.bwd_tasks, c->stream);
+  }
+  if (slots > c->hslot_count || !c->d_hflags) {
+    dfree(c->d_hflags);
+    dfree(c->d_hscratch);
+    c->d_hflags = dalloc<int>(std::max(1, slots));
+    CK(cudaMemsetAsync(c->d_hflags, 0, std::max(1, slots) * sizeof(int), c->stream));
+    c->d_hscratch = dalloc<double>(static_cast<size_t>(std::max(1, slots)) * RB * solve_rhs_chunk());
+    c->hslot_count = std::max(1, slots);
+    c->solve_epoch = std::max(c->solve_epoch, 0);
   }
   c->solve_np = np;
   CK(cudaStreamSynchronize(c->stream));
@@ -1091,8 +1119,8 @@ void device_solve(symla_gpu_ctx* c, const double* dB, int ldb, int nrhs, double*
       const int nt = static_cast<int>(L.bwd_tasks.size());
       const int grid = std::min(nt, c->bwd_resident);
       timed(c, SYMLA_KERNEL_BACKWARD, 0.0, L.solve_bytes_fixed + nc * L.solve_bytes_per_rhs, [&] {
-        CK(launch_backward_pipelined(c->d_desc, c->d_state, L.d_bwd_tasks, nt, grid, c->d_flag_base, c->d_flags, eb,
-                                     c->d_solve_err, nrhs, c0, c->d_Xf, n, st));
+        CK(launch_backward_pipelined(c->d_desc, c->d_state, L.d_bwd_tasks, nt, grid, c->d_flag_base, c->d_flags,
+                                     c->d_hflags, c->d_hscratch, eb, c->d_solve_err, nrhs, c0, c->d_Xf, n, st));
       });
     }
   }
@@ -1223,7 +1251,7 @@ extern "C" void symla_gpu_destroy(symla_gpu_ctx* c) {
                   c->d_front_delta, c->d_perm, c->d_rowptr, c->d_colind, c->d_vidx, c->d_srowptr, c->d_svidx, c->d_W,
                   c->d_Bp, c->d_Z, c->d_Xf, c->d_B, c->d_X, c->d_R, c->d_dX, c->d_Xn, c->d_Rn, c->d_norms,
                   c->d_scratch_int, c->d_flag_base, c->d_flags, c->d_solve_err, c->d_counter,
-                  c->d_tcws, c->d_tc_err, c->d_tc_guard};
+                  c->d_tcws, c->d_tc_err, c->d_tc_guard, c->d_hflags, c->d_hscratch};
   for (void* p : ptrs) dfree(p);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);

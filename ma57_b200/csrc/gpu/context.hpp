@@ -42,9 +42,9 @@ struct LevelLists {
   double solve_bytes_fixed = 0.0;
   double solve_bytes_per_rhs = 0.0;
   // pipelined solve tasks {front, block}
-  std::vector<int2> fwd_tasks, bwd_tasks;
-  int2* d_fwd_tasks = nullptr;
-  int2* d_bwd_tasks = nullptr;
+  std::vector<int4> fwd_tasks, bwd_tasks;
+  int4* d_fwd_tasks = nullptr;
+  int4* d_bwd_tasks = nullptr;
   // device copies (static plan)
   int* d_small = nullptr;
   int* d_large = nullptr;
@@ -142,6 +142,9 @@ struct symla_gpu_ctx {
   int* d_flag_base = nullptr;
   int* d_flags = nullptr;
   int* d_solve_err = nullptr;
+  int* d_hflags = nullptr;        // backward helper-part flags (one per slot)
+  double* d_hscratch = nullptr;   // backward helper-part partial sums
+  int hslot_count = 0;
   int* d_counter = nullptr;  // unfinished-front counter
   int flag_count = 0;
   int solve_epoch = 0;

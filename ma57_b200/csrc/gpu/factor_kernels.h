@@ -54,18 +54,18 @@ void launch_update(bool far, const FrontDesc* fronts, FrontState* st, const int*
 void launch_permute_in(int n, int nrhs, const int* perm, const double* B, int ldb, double* Bp, cudaStream_t stream);
 void launch_permute_out(int n, int nrhs, const int* perm, const double* X, double* Xout, int ldx, cudaStream_t stream);
 // Pipelined level solves (one cooperative launch per level; see
-// solve_kernels.cu). tasks: int2 {front, block}; flags indexed by
+// solve_kernels.cu). tasks: int4 (see the kernels); flags indexed by
 // flag_base[front] + block, compared against epoch.
 int solve_block_rows();
 int solve_rhs_chunk();
 cudaError_t solve_max_resident(int device, int* fwd_ctas, int* bwd_ctas);
 cudaError_t launch_forward_pipelined(const FrontDesc* fronts, const ChildLink* links, const FrontState* st,
-                                     const int2* tasks, int ntasks, int grid, const int* flag_base, int* flags,
+                                     const int4* tasks, int ntasks, int grid, const int* flag_base, int* flags,
                                      int epoch, int* err, int nrhs, int c0, const double* Bp, int n,
                                      cudaStream_t stream);
-cudaError_t launch_backward_pipelined(const FrontDesc* fronts, const FrontState* st, const int2* tasks, int ntasks,
-                                      int grid, const int* flag_base, int* flags, int epoch, int* err, int nrhs,
-                                      int c0, double* X, int n, cudaStream_t stream);
+cudaError_t launch_backward_pipelined(const FrontDesc* fronts, const FrontState* st, const int4* tasks, int ntasks,
+                                      int grid, const int* flag_base, int* flags, int* hflags, double* hscratch,
+                                      int epoch, int* err, int nrhs, int c0, double* X, int n, cudaStream_t stream);
 
 // Residual R = B - sym(A) X in the original index space (full symmetric CSR
 // gathered from the stored lower triangle); rowptr/colind/vidx describe it.

@@ -136,184 +136,202 @@ __device__ __forceinline__ void stage_tile(double* T, const double* F, int64_t l
   scp_commit();
 }
 
-// Forward task = (front, row block); flag of a pivot row block at
-// flag_base[front] + row block.
-__global__ void __launch_bounds__(kST) forward_pipelined_kernel(
+// ---------------------------------------------------------------------------
+// Forward: one row block (front s, block rb). Returns false when a wait
+// ended in an error (the CTA then leaves the launch).
+__device__ bool forward_block(const FrontDesc* __restrict__ fronts, const ChildLink* __restrict__ links,
+                              const FrontState* __restrict__ st, int s, int rb, const int* __restrict__ flag_base,
+                              int* flags, int epoch, int* err, int nc, int c0, const double* __restrict__ Bp, int n,
+                              double* acc, double* xb, double* Lb0) {
+  const int row = threadIdx.x % kRB, cg = threadIdx.x / kRB;  // product layout: a row, 4 right-hand sides
+  const FrontDesc f = fronts[s];
+  const int m = f.m, np = st[s].npiv;
+  const int r0 = rb * kRB, r1 = min(r0 + kRB, m), nr = r1 - r0;
+  const int64_t ld = f.ld;
+  double* W = f.W;
+  const int wld = f.wld;
+  const int nbp = (np + kRB - 1) / kRB;
+  const int jend = min(rb, nbp);
+  const bool hasDiag = r0 < np;
+  const int ntiles = jend + (hasDiag ? 1 : 0);
+  // tile tt: pivot block tt (tt < jend) or the diagonal block
+  auto stage = [&](int tt) {
+    double* T = Lb0 + (tt & 1) * kRB * kTileStride;
+    if (tt < jend) {
+      const int j0 = tt * kRB;
+      stage_tile(T, f.F, ld, r0, nr, j0, min(j0 + kRB, np) - j0);
+    } else {
+      stage_tile(T, f.F, ld, r0, nr, r0, min(r1, np) - r0);
+    }
+  };
+  if (ntiles > 0) stage(0);
+  // 1. Bp for pivot rows plus the children's forwarded rows, gathered
+  //    through each row's pre-pivot position
+  for (int t = threadIdx.x; t < nr * nc; t += kST) {
+    const int ii = t % nr, c = t / nr;
+    const int i = r0 + ii;
+    double v = (i < np) ? Bp[f.fidx[i] + static_cast<int64_t>(c0 + c) * n] : 0.0;
+    const int pre = f.lperm[i];
+    for (int ch = f.ch_begin; ch < f.ch_end; ++ch) {
+      const ChildLink L = links[ch];
+      const int a = L.invmap[pre];
+      if (a < 0) continue;
+      const FrontDesc& cf = fronts[L.child];
+      const int cnp = st[L.child].npiv;
+      v += cf.W[cnp + a + static_cast<int64_t>(c0 + c) * cf.wld];
+    }
+    acc[ii * kAccStride + c] = v;
+  }
+  for (int tt = 0; tt < ntiles; ++tt) {
+    const bool more = tt + 1 < ntiles;
+    if (more) stage(tt + 1);
+    double* T = Lb0 + (tt & 1) * kRB * kTileStride;
+    if (tt < jend) {
+      // 2. contribution of finished pivot block j = tt
+      const int j = tt;
+      if (!wait_flag(flags, flag_base[s] + j, epoch, err)) {
+        scp_wait<0>();
+        return false;
+      }
+      const int j0 = j * kRB, nj = min(j0 + kRB, np) - j0;
+      for (int t = threadIdx.x; t < kRB * nc; t += kST) {
+        const int jj = t % kRB, c = t / kRB;
+        xb[jj * kAccStride + c] = (jj < nj) ? W[j0 + jj + static_cast<int64_t>(c0 + c) * wld] : 0.0;
+      }
+      if (more)
+        scp_wait<1>();
+      else
+        scp_wait<0>();
+      __syncthreads();
+      // a 2x2 pivot straddling the block boundary: its d21 slot in L is not
+      // an L entry
+      if (threadIdx.x == 0 && j == rb - 1 && r0 - 1 >= j0 && f.pk[r0 - 1] == 1) T[r0 - 1 - j0] = 0.0;
+      __syncthreads();
+      if (row < nr) {
+        double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
+        const int cb4 = cg * 4;
+        for (int jj = 0; jj < nj; ++jj) {
+          const double l = T[row * kTileStride + jj];
+          const double* y = xb + jj * kAccStride + cb4;
+          p0 = fma(l, y[0], p0);
+          p1 = fma(l, y[1], p1);
+          p2 = fma(l, y[2], p2);
+          p3 = fma(l, y[3], p3);
+        }
+        double* a = acc + row * kAccStride + cb4;
+        if (cb4 + 0 < nc) a[0] -= p0;
+        if (cb4 + 1 < nc) a[1] -= p1;
+        if (cb4 + 2 < nc) a[2] -= p2;
+        if (cb4 + 3 < nc) a[3] -= p3;
+      }
+      __syncthreads();
+    } else {
+      // 3. the block's own pivot columns: unit-lower solve for its pivot
+      //    rows and the matching update of its non-pivot rows
+      scp_wait<0>();
+      __syncthreads();
+      const int npv = min(r1, np) - r0;
+      if (threadIdx.x < npv - 1 && f.pk[r0 + threadIdx.x] == 1)
+        T[(threadIdx.x + 1) * kTileStride + threadIdx.x] = 0.0;  // d21 slot of a 2x2 pivot
+      __syncthreads();
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      for (int c = warp; c < nc; c += kST / 32) {
+        double y0 = (lane < nr) ? acc[lane * kAccStride + c] : 0.0;
+        double y1 = (lane + 32 < nr) ? acc[(lane + 32) * kAccStride + c] : 0.0;
+        for (int jj = 0; jj < npv; ++jj) {
+          const double yj = __shfl_sync(0xffffffffu, jj < 32 ? y0 : y1, jj & 31);
+          if (lane > jj) y0 -= T[lane * kTileStride + jj] * yj;
+          if (lane + 32 > jj) y1 -= T[(lane + 32) * kTileStride + jj] * yj;
+        }
+        if (lane < nr) acc[lane * kAccStride + c] = y0;
+        if (lane + 32 < nr) acc[(lane + 32) * kAccStride + c] = y1;
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nr * nc; t += kST) {
+    const int ii = t % nr, c = t / nr;
+    W[r0 + ii + static_cast<int64_t>(c0 + c) * wld] = acc[ii * kAccStride + c];
+  }
+  if (hasDiag) publish(flags, flag_base[s] + rb, epoch);
+  __syncthreads();
+  return true;
+}
+
+// Forward task = int4 {front, row block, 0, 0}, or {front, -1, 0, 0} for the
+// whole front (its row blocks in order, in this CTA). Flag of a pivot row
+// block at flag_base[front] + row block.
+__global__ void __launch_bounds__(kST, 2) forward_pipelined_kernel(
     const FrontDesc* __restrict__ fronts, const ChildLink* __restrict__ links, const FrontState* __restrict__ st,
-    const int2* __restrict__ tasks, int ntasks, const int* __restrict__ flag_base, int* flags, int epoch, int* err,
+    const int4* __restrict__ tasks, int ntasks, const int* __restrict__ flag_base, int* flags, int epoch, int* err,
     int nrhs, int c0, const double* __restrict__ Bp, int n) {
   extern __shared__ double ssm[];
   double* acc = ssm;
   double* xb = acc + kRB * kAccStride;
   double* Lb0 = xb + kRB * kAccStride;
   const int nc = min(kRhsChunk, nrhs - c0);
-  const int row = threadIdx.x % kRB, cg = threadIdx.x / kRB;  // product layout: a row, 4 right-hand sides
   for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
     if (ld_acquire(err) != 0) return;
-    const int s = tasks[task].x, rb = tasks[task].y;
-    const FrontDesc f = fronts[s];
-    const int m = f.m, np = st[s].npiv;
-    const int r0 = rb * kRB, r1 = min(r0 + kRB, m), nr = r1 - r0;
-    const int64_t ld = f.ld;
-    double* W = f.W;
-    const int wld = f.wld;
-    const int nbp = (np + kRB - 1) / kRB;
-    const int jend = min(rb, nbp);
-    const bool hasDiag = r0 < np;
-    const int ntiles = jend + (hasDiag ? 1 : 0);
-    // tile tt: pivot block tt (tt < jend) or the diagonal block
-    auto stage = [&](int tt) {
-      double* T = Lb0 + (tt & 1) * kRB * kTileStride;
-      if (tt < jend) {
-        const int j0 = tt * kRB;
-        stage_tile(T, f.F, ld, r0, nr, j0, min(j0 + kRB, np) - j0);
-      } else {
-        stage_tile(T, f.F, ld, r0, nr, r0, min(r1, np) - r0);
-      }
-    };
-    if (ntiles > 0) stage(0);
-    // 1. Bp for pivot rows plus the children's forwarded rows, gathered
-    //    through each row's pre-pivot position
-    for (int t = threadIdx.x; t < nr * nc; t += kST) {
-      const int ii = t % nr, c = t / nr;
-      const int i = r0 + ii;
-      double v = (i < np) ? Bp[f.fidx[i] + static_cast<int64_t>(c0 + c) * n] : 0.0;
-      const int pre = f.lperm[i];
-      for (int ch = f.ch_begin; ch < f.ch_end; ++ch) {
-        const ChildLink L = links[ch];
-        const int a = L.invmap[pre];
-        if (a < 0) continue;
-        const FrontDesc& cf = fronts[L.child];
-        const int cnp = st[L.child].npiv;
-        v += cf.W[cnp + a + static_cast<int64_t>(c0 + c) * cf.wld];
-      }
-      acc[ii * kAccStride + c] = v;
-    }
-    for (int tt = 0; tt < ntiles; ++tt) {
-      const bool more = tt + 1 < ntiles;
-      if (more) stage(tt + 1);
-      double* T = Lb0 + (tt & 1) * kRB * kTileStride;
-      if (tt < jend) {
-        // 2. contribution of finished pivot block j = tt
-        const int j = tt;
-        if (!wait_flag(flags, flag_base[s] + j, epoch, err)) {
-          scp_wait<0>();
+    const int4 tk = tasks[task];
+    const int s = tk.x;
+    if (tk.y >= 0) {
+      if (!forward_block(fronts, links, st, s, tk.y, flag_base, flags, epoch, err, nc, c0, Bp, n, acc, xb, Lb0)) return;
+    } else {
+      const int nb = (fronts[s].m + kRB - 1) / kRB;
+      for (int rb = 0; rb < nb; ++rb)
+        if (!forward_block(fronts, links, st, s, rb, flag_base, flags, epoch, err, nc, c0, Bp, n, acc, xb, Lb0))
           return;
-        }
-        const int j0 = j * kRB, nj = min(j0 + kRB, np) - j0;
-        for (int t = threadIdx.x; t < kRB * nc; t += kST) {
-          const int jj = t % kRB, c = t / kRB;
-          xb[jj * kAccStride + c] = (jj < nj) ? W[j0 + jj + static_cast<int64_t>(c0 + c) * wld] : 0.0;
-        }
-        if (more)
-          scp_wait<1>();
-        else
-          scp_wait<0>();
-        __syncthreads();
-        // a 2x2 pivot straddling the block boundary: its d21 slot in L is
-        // not an L entry
-        if (threadIdx.x == 0 && j == rb - 1 && r0 - 1 >= j0 && f.pk[r0 - 1] == 1) T[0 * kTileStride + (r0 - 1 - j0)] = 0.0;
-        __syncthreads();
-        if (row < nr) {
-          double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
-          const int cb4 = cg * 4;
-          for (int jj = 0; jj < nj; ++jj) {
-            const double l = T[row * kTileStride + jj];
-            const double* y = xb + jj * kAccStride + cb4;
-            p0 = fma(l, y[0], p0);
-            p1 = fma(l, y[1], p1);
-            p2 = fma(l, y[2], p2);
-            p3 = fma(l, y[3], p3);
-          }
-          double* a = acc + row * kAccStride + cb4;
-          if (cb4 + 0 < nc) a[0] -= p0;
-          if (cb4 + 1 < nc) a[1] -= p1;
-          if (cb4 + 2 < nc) a[2] -= p2;
-          if (cb4 + 3 < nc) a[3] -= p3;
-        }
-        __syncthreads();
-      } else {
-        // 3. the block's own pivot columns: unit-lower solve for its pivot
-        //    rows and the matching update of its non-pivot rows
-        scp_wait<0>();
-        __syncthreads();
-        const int npv = min(r1, np) - r0;
-        if (threadIdx.x < npv - 1 && f.pk[r0 + threadIdx.x] == 1)
-          T[(threadIdx.x + 1) * kTileStride + threadIdx.x] = 0.0;  // d21 slot of a 2x2 pivot
-        __syncthreads();
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        for (int c = warp; c < nc; c += kST / 32) {
-          double y0 = (lane < nr) ? acc[lane * kAccStride + c] : 0.0;
-          double y1 = (lane + 32 < nr) ? acc[(lane + 32) * kAccStride + c] : 0.0;
-          for (int jj = 0; jj < npv; ++jj) {
-            const double yj = __shfl_sync(0xffffffffu, jj < 32 ? y0 : y1, jj & 31);
-            if (lane > jj) y0 -= T[lane * kTileStride + jj] * yj;
-            if (lane + 32 > jj) y1 -= T[(lane + 32) * kTileStride + jj] * yj;
-          }
-          if (lane < nr) acc[lane * kAccStride + c] = y0;
-          if (lane + 32 < nr) acc[(lane + 32) * kAccStride + c] = y1;
-        }
-        __syncthreads();
-      }
     }
-    __syncthreads();
-    for (int t = threadIdx.x; t < nr * nc; t += kST) {
-      const int ii = t % nr, c = t / nr;
-      W[r0 + ii + static_cast<int64_t>(c0 + c) * wld] = acc[ii * kAccStride + c];
-    }
-    if (hasDiag) publish(flags, flag_base[s] + rb, epoch);
-    __syncthreads();
   }
 }
 
-// Backward task = (front, pivot column block), a front's blocks listed from
-// the last to the first; flag at flag_base[front] + column block.
-__global__ void __launch_bounds__(kST) backward_pipelined_kernel(
-    const FrontDesc* __restrict__ fronts, const FrontState* __restrict__ st, const int2* __restrict__ tasks,
-    int ntasks, const int* __restrict__ flag_base, int* flags, int epoch, int* err, int nrhs, int c0,
-    double* __restrict__ X, int n) {
-  extern __shared__ double ssm[];
-  double* acc = ssm;
-  double* xb = acc + kRB * kAccStride;
-  double* Lb0 = xb + kRB * kAccStride;
-  const int nc = min(kRhsChunk, nrhs - c0);
+// ---------------------------------------------------------------------------
+// Backward: pivot column block cb of front s. The tiles are the ancestor
+// rows [np, m) in 64-row chunks, then the later pivot blocks, then the
+// diagonal block. A main part (part 0) does ancestor chunks [a0, a1), the
+// later blocks, adds its helper parts' partial sums (slots hslot0 ..
+// hslot0 + nh - 1, in slot order) and finishes the block; a helper part
+// only sums its ancestor chunks into its scratch slot and raises its flag.
+__device__ bool backward_block(const FrontDesc* __restrict__ fronts, const FrontState* __restrict__ st, int s, int cb,
+                               bool helper, int a0, int a1, int hslot0, int nh, const int* __restrict__ flag_base,
+                               int* flags, int* hflags, double* hscratch, int epoch, int* err, int nc, int c0,
+                               double* __restrict__ X, int n, double* acc, double* xb, double* Lb0) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int NW = kST / 32;
   const int col = threadIdx.x % kRB, cg = threadIdx.x / kRB;
-  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
-    if (ld_acquire(err) != 0) return;
-    const int s = tasks[task].x, cb = tasks[task].y;
-    const FrontDesc f = fronts[s];
-    const int m = f.m, np = st[s].npiv;
-    const int q0 = cb * kRB, q1 = min(q0 + kRB, np), nq = q1 - q0;
-    const int64_t ld = f.ld;
-    const double* W = f.W;
-    const int wld = f.wld;
-    const int nbp = (np + kRB - 1) / kRB;
-    // tiles: the ancestor rows [np, m) in chunks, then the later pivot
-    // blocks nbp-1 .. cb+1, then the diagonal block
-    const int nanc = (m - np + kRB - 1) / kRB;
-    const int nlater = nbp - 1 - cb;
-    const int ntiles = nanc + nlater + 1;
-    auto tile_rows = [&](int tt, int& i0, int& i1) {
-      if (tt < nanc) {
-        i0 = np + tt * kRB;
-        i1 = min(i0 + kRB, m);
-      } else if (tt < nanc + nlater) {
-        const int j = nbp - 1 - (tt - nanc);
-        i0 = j * kRB;
-        i1 = min(i0 + kRB, np);
-      } else {
-        i0 = q0;
-        i1 = q1;
-      }
-    };
-    auto stage = [&](int tt) {
-      int i0, i1;
-      tile_rows(tt, i0, i1);
-      stage_tile(Lb0 + (tt & 1) * kRB * kTileStride, f.F, ld, i0, i1 - i0, q0, nq);
-    };
-    stage(0);
+  const FrontDesc f = fronts[s];
+  const int m = f.m, np = st[s].npiv;
+  const int q0 = cb * kRB, q1 = min(q0 + kRB, np), nq = q1 - q0;
+  const int64_t ld = f.ld;
+  const double* W = f.W;
+  const int wld = f.wld;
+  const int nbp = (np + kRB - 1) / kRB;
+  const int nanc = a1 - a0;
+  const int nlater = helper ? 0 : nbp - 1 - cb;
+  const int ntiles = nanc + nlater + (helper ? 0 : 1);
+  auto tile_rows = [&](int tt, int& i0, int& i1) {
+    if (tt < nanc) {
+      i0 = np + (a0 + tt) * kRB;
+      i1 = min(i0 + kRB, m);
+    } else if (tt < nanc + nlater) {
+      const int j = nbp - 1 - (tt - nanc);
+      i0 = j * kRB;
+      i1 = min(i0 + kRB, np);
+    } else {
+      i0 = q0;
+      i1 = q1;
+    }
+  };
+  auto stage = [&](int tt) {
+    int i0, i1;
+    tile_rows(tt, i0, i1);
+    stage_tile(Lb0 + (tt & 1) * kRB * kTileStride, f.F, ld, i0, i1 - i0, q0, nq);
+  };
+  if (ntiles > 0) stage(0);
+  if (helper) {
+    for (int t = threadIdx.x; t < kRB * nc; t += kST) acc[(t % kRB) * kAccStride + t / kRB] = 0.0;
+  } else {
     // 1. z = D^{-1} y for the block's pivots (a 2x2 partner may sit in the
     //    neighbouring block; y is complete in W after the forward pass)
     for (int t = threadIdx.x; t < nq * nc; t += kST) {
@@ -335,83 +353,147 @@ __global__ void __launch_bounds__(kST) backward_pipelined_kernel(
       }
       acc[qq * kAccStride + c] = z;
     }
-    for (int tt = 0; tt < ntiles; ++tt) {
-      const bool more = tt + 1 < ntiles;
-      if (more) stage(tt + 1);
-      double* T = Lb0 + (tt & 1) * kRB * kTileStride;
-      int i0, i1;
-      tile_rows(tt, i0, i1);
-      if (tt < nanc + nlater) {
-        // 2. minus L(rows of the tile, block)^T x(rows of the tile): the
-        //    ancestor rows are final from earlier levels; later pivot blocks
-        //    of this front are waited for
-        if (tt >= nanc) {
-          const int j = nbp - 1 - (tt - nanc);
-          if (!wait_flag(flags, flag_base[s] + j, epoch, err)) {
-            scp_wait<0>();
-            return;
-          }
-        }
-        const int ni = i1 - i0;
-        for (int t = threadIdx.x; t < kRB * nc; t += kST) {
-          const int ii = t % kRB, c = t / kRB;
-          xb[ii * kAccStride + c] = (ii < ni) ? X[f.fidx[i0 + ii] + static_cast<int64_t>(c0 + c) * n] : 0.0;
-        }
-        if (more)
-          scp_wait<1>();
-        else
+  }
+  for (int tt = 0; tt < ntiles; ++tt) {
+    const bool more = tt + 1 < ntiles;
+    if (more) stage(tt + 1);
+    double* T = Lb0 + (tt & 1) * kRB * kTileStride;
+    int i0, i1;
+    tile_rows(tt, i0, i1);
+    if (tt < nanc + nlater) {
+      // 2. minus L(rows of the tile, block)^T x(rows of the tile): the
+      //    ancestor rows are final from earlier levels; later pivot blocks of
+      //    this front are waited for
+      if (tt >= nanc) {
+        const int j = nbp - 1 - (tt - nanc);
+        if (!wait_flag(flags, flag_base[s] + j, epoch, err)) {
           scp_wait<0>();
-        __syncthreads();
-        // a 2x2 pivot straddling the block boundary: d21 is not an L entry
-        if (threadIdx.x == 0 && i0 == q1 && nq > 0 && f.pk[q1 - 1] == 1) T[0 * kTileStride + (nq - 1)] = 0.0;
-        __syncthreads();
-        if (col < nq) {
-          double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
-          const int cb4 = cg * 4;
-          for (int ii = 0; ii < ni; ++ii) {
-            const double l = T[ii * kTileStride + col];
-            const double* x = xb + ii * kAccStride + cb4;
-            p0 = fma(l, x[0], p0);
-            p1 = fma(l, x[1], p1);
-            p2 = fma(l, x[2], p2);
-            p3 = fma(l, x[3], p3);
-          }
-          double* a = acc + col * kAccStride + cb4;
-          if (cb4 + 0 < nc) a[0] -= p0;
-          if (cb4 + 1 < nc) a[1] -= p1;
-          if (cb4 + 2 < nc) a[2] -= p2;
-          if (cb4 + 3 < nc) a[3] -= p3;
+          return false;
         }
-        __syncthreads();
-      } else {
-        // 3. transposed unit-lower solve on the diagonal block
+      }
+      const int ni = i1 - i0;
+      for (int t = threadIdx.x; t < kRB * nc; t += kST) {
+        const int ii = t % kRB, c = t / kRB;
+        xb[ii * kAccStride + c] = (ii < ni) ? X[f.fidx[i0 + ii] + static_cast<int64_t>(c0 + c) * n] : 0.0;
+      }
+      if (more)
+        scp_wait<1>();
+      else
         scp_wait<0>();
-        __syncthreads();
-        if (threadIdx.x < nq - 1 && f.pk[q0 + threadIdx.x] == 1)
-          T[(threadIdx.x + 1) * kTileStride + threadIdx.x] = 0.0;  // d21 slot of a 2x2 pivot
-        __syncthreads();
-        for (int c = warp; c < nc; c += NW) {
-          double x0 = (lane < nq) ? acc[lane * kAccStride + c] : 0.0;
-          double x1 = (lane + 32 < nq) ? acc[(lane + 32) * kAccStride + c] : 0.0;
-          for (int jj = nq - 1; jj >= 0; --jj) {
-            // x[jj] is final once every row below it has been applied; row jj
-            // of Ltop then updates the unknowns above it
-            const double xj = __shfl_sync(0xffffffffu, jj < 32 ? x0 : x1, jj & 31);
-            if (lane < jj) x0 -= T[jj * kTileStride + lane] * xj;
-            if (lane + 32 < jj) x1 -= T[jj * kTileStride + lane + 32] * xj;
-          }
-          if (lane < nq) acc[lane * kAccStride + c] = x0;
-          if (lane + 32 < nq) acc[(lane + 32) * kAccStride + c] = x1;
+      __syncthreads();
+      // a 2x2 pivot straddling the block boundary: d21 is not an L entry
+      if (threadIdx.x == 0 && i0 == q1 && nq > 0 && f.pk[q1 - 1] == 1) T[nq - 1] = 0.0;
+      __syncthreads();
+      if (col < nq) {
+        double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
+        const int cb4 = cg * 4;
+        for (int ii = 0; ii < ni; ++ii) {
+          const double l = T[ii * kTileStride + col];
+          const double* x = xb + ii * kAccStride + cb4;
+          p0 = fma(l, x[0], p0);
+          p1 = fma(l, x[1], p1);
+          p2 = fma(l, x[2], p2);
+          p3 = fma(l, x[3], p3);
+        }
+        double* a = acc + col * kAccStride + cb4;
+        if (cb4 + 0 < nc) a[0] -= p0;
+        if (cb4 + 1 < nc) a[1] -= p1;
+        if (cb4 + 2 < nc) a[2] -= p2;
+        if (cb4 + 3 < nc) a[3] -= p3;
+      }
+      __syncthreads();
+    } else {
+      // helper parts' partial sums, in slot order (deterministic)
+      for (int h = 0; h < nh; ++h) {
+        if (!wait_flag(hflags, hslot0 + h, epoch, err)) {
+          scp_wait<0>();
+          return false;
+        }
+        const double* part = hscratch + static_cast<int64_t>(hslot0 + h) * kRB * kRhsChunk;
+        for (int t = threadIdx.x; t < nq * nc; t += kST) {
+          const int qq = t % nq, c = t / nq;
+          acc[qq * kAccStride + c] += part[c * kRB + qq];
         }
         __syncthreads();
       }
+      // 3. transposed unit-lower solve on the diagonal block
+      scp_wait<0>();
+      __syncthreads();
+      if (threadIdx.x < nq - 1 && f.pk[q0 + threadIdx.x] == 1)
+        T[(threadIdx.x + 1) * kTileStride + threadIdx.x] = 0.0;  // d21 slot of a 2x2 pivot
+      __syncthreads();
+      for (int c = warp; c < nc; c += NW) {
+        double x0 = (lane < nq) ? acc[lane * kAccStride + c] : 0.0;
+        double x1 = (lane + 32 < nq) ? acc[(lane + 32) * kAccStride + c] : 0.0;
+        for (int jj = nq - 1; jj >= 0; --jj) {
+          // x[jj] is final once every row below it has been applied; row jj
+          // of Ltop then updates the unknowns above it
+          const double xj = __shfl_sync(0xffffffffu, jj < 32 ? x0 : x1, jj & 31);
+          if (lane < jj) x0 -= T[jj * kTileStride + lane] * xj;
+          if (lane + 32 < jj) x1 -= T[jj * kTileStride + lane + 32] * xj;
+        }
+        if (lane < nq) acc[lane * kAccStride + c] = x0;
+        if (lane + 32 < nq) acc[(lane + 32) * kAccStride + c] = x1;
+      }
+      __syncthreads();
     }
+  }
+  if (helper) {
+    // acc holds minus the helper's partial sum; the main part adds it
+    double* part = hscratch + static_cast<int64_t>(hslot0) * kRB * kRhsChunk;
+    for (int t = threadIdx.x; t < nq * nc; t += kST) {
+      const int qq = t % nq, c = t / nq;
+      part[c * kRB + qq] = acc[qq * kAccStride + c];
+    }
+    publish(hflags, hslot0, epoch);
+  } else {
     for (int t = threadIdx.x; t < nq * nc; t += kST) {
       const int qq = t % nq, c = t / nq;
       X[f.fidx[q0 + qq] + static_cast<int64_t>(c0 + c) * n] = acc[qq * kAccStride + c];
     }
     publish(flags, flag_base[s] + cb, epoch);
-    __syncthreads();
+  }
+  __syncthreads();
+  return true;
+}
+
+// Backward task = int4 {front, column block, part, aux}:
+//   {s, -1, 0, 0}            the whole front (blocks last to first, this CTA)
+//   {s, cb, 0, P << 20 | h0}  main part of block cb with P parts in all; its
+//                             helpers hold scratch slots h0 .. h0 + P - 2
+//   {s, cb, p, P << 20 | h}   helper part p (1 <= p < P) in slot h
+// The ancestor chunks of a block are split evenly over its P parts. Helpers
+// are listed before their main part, and later blocks of a front before
+// earlier ones, so every wait is on a task with a smaller index.
+__global__ void __launch_bounds__(kST, 2) backward_pipelined_kernel(
+    const FrontDesc* __restrict__ fronts, const FrontState* __restrict__ st, const int4* __restrict__ tasks,
+    int ntasks, const int* __restrict__ flag_base, int* flags, int* hflags, double* hscratch, int epoch, int* err,
+    int nrhs, int c0, double* __restrict__ X, int n) {
+  extern __shared__ double ssm[];
+  double* acc = ssm;
+  double* xb = acc + kRB * kAccStride;
+  double* Lb0 = xb + kRB * kAccStride;
+  const int nc = min(kRhsChunk, nrhs - c0);
+  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
+    if (ld_acquire(err) != 0) return;
+    const int4 tk = tasks[task];
+    const int s = tk.x;
+    const int m = fronts[s].m, np = st[s].npiv;
+    const int nanc = (m - np + kRB - 1) / kRB;
+    if (tk.y < 0) {
+      const int nbp = (np + kRB - 1) / kRB;
+      for (int cb = nbp - 1; cb >= 0; --cb)
+        if (!backward_block(fronts, st, s, cb, false, 0, nanc, 0, 0, flag_base, flags, hflags, hscratch, epoch, err,
+                            nc, c0, X, n, acc, xb, Lb0))
+          return;
+    } else {
+      const int P = tk.w >> 20, slot = tk.w & ((1 << 20) - 1), p = tk.z;
+      const int a0 = static_cast<int>(static_cast<long long>(nanc) * p / P);
+      const int a1 = static_cast<int>(static_cast<long long>(nanc) * (p + 1) / P);
+      if (!backward_block(fronts, st, s, tk.y, p > 0, a0, a1, slot, p > 0 ? 1 : P - 1, flag_base, flags, hflags,
+                          hscratch, epoch, err, nc, c0, X, n, acc, xb, Lb0))
+        return;
+    }
   }
 }
 
@@ -490,7 +572,7 @@ cudaError_t solve_max_resident(int device, int* fwd_ctas, int* bwd_ctas) {
 }
 
 cudaError_t launch_forward_pipelined(const FrontDesc* fronts, const ChildLink* links, const FrontState* st,
-                                     const int2* tasks, int ntasks, int grid, const int* flag_base, int* flags,
+                                     const int4* tasks, int ntasks, int grid, const int* flag_base, int* flags,
                                      int epoch, int* err, int nrhs, int c0, const double* Bp, int n,
                                      cudaStream_t stream) {
   if (ntasks <= 0) return cudaSuccess;
@@ -501,12 +583,13 @@ cudaError_t launch_forward_pipelined(const FrontDesc* fronts, const ChildLink* l
                                      args, kSolveSmem, stream);
 }
 
-cudaError_t launch_backward_pipelined(const FrontDesc* fronts, const FrontState* st, const int2* tasks, int ntasks,
-                                      int grid, const int* flag_base, int* flags, int epoch, int* err, int nrhs,
-                                      int c0, double* X, int n, cudaStream_t stream) {
+cudaError_t launch_backward_pipelined(const FrontDesc* fronts, const FrontState* st, const int4* tasks, int ntasks,
+                                      int grid, const int* flag_base, int* flags, int* hflags, double* hscratch,
+                                      int epoch, int* err, int nrhs, int c0, double* X, int n, cudaStream_t stream) {
   if (ntasks <= 0) return cudaSuccess;
-  void* args[] = {(void*)&fronts, (void*)&st,  (void*)&tasks, (void*)&ntasks, (void*)&flag_base, (void*)&flags,
-                  (void*)&epoch,  (void*)&err, (void*)&nrhs,  (void*)&c0,     (void*)&X,         (void*)&n};
+  void* args[] = {(void*)&fronts, (void*)&st,    (void*)&tasks, (void*)&ntasks, (void*)&flag_base,
+                  (void*)&flags,  (void*)&hflags, (void*)&hscratch, (void*)&epoch, (void*)&err,
+                  (void*)&nrhs,   (void*)&c0,    (void*)&X,     (void*)&n};
   return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(backward_pipelined_kernel), dim3(grid), dim3(kST),
                                      args, kSolveSmem, stream);
 }
