@@ -137,6 +137,238 @@ def algorithmic_flops(k):
     return f
 
 
+def panel_bytes(k):
+    """Algorithmic bytes of the large-front panel factorization of cfg3 at
+    grid k: every pivot column of a front with m > 128 is read and its L
+    written once below the pivot (16 bytes per entry)."""
+    from ma57_b200 import OrderingType, SymLDLT
+    A, _ = build_problem(k, 1)
+    s = SymLDLT()
+    s.setOrdering(OrderingType.Metis)
+    s.analyzePattern(A)
+    b = 0.0
+    for sn in s.symbolicFactor().supernodes:
+        m, p = len(sn.rowPattern), sn.ncols
+        if m > 128:
+            b += 16.0 * (m * p - p * (p - 1) / 2.0)
+    return b
+
+
+def profiled_traffic(kind):
+    """DRAM bytes per launch of a kernel kind from the committed ncu summary
+    (profiles/traffic.md: lines 'kind: <kind> dram_bytes_per_launch: <N>'),
+    or None."""
+    path = os.path.join(ROOT, "profiles", "traffic.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                parts = line.replace("`", "").split()
+                if len(parts) >= 4 and parts[0] == "kind:" and parts[1] == kind and parts[2] == "dram_bytes_per_launch:":
+                    return float(parts[3])
+    except OSError:
+        pass
+    return None
+
+
+def run_dense(args):
+    """One dense front (the profiling case of the large-front kernels): a
+    random symmetric indefinite matrix with a dominant diagonal of random
+    sign, natural order, factorized `steps` times after `warmup`."""
+    import numpy as np
+    import scipy.sparse as sp
+    import torch
+    from ma57_b200 import OrderingType, Precision, SymLDLT
+    from ma57_b200 import _lib as L
+    n = args.n
+    rng = np.random.default_rng(n)
+    G = rng.standard_normal((n, n))
+    A0 = (G + G.T) / 2 + np.diag(rng.choice([-1.0, 1.0], n) * n / 51.2)
+    ii, jj = np.tril_indices(n)
+    A = sp.csc_matrix((A0[ii, jj], (ii, jj)), shape=(n, n))
+    s = SymLDLT()
+    s.setOrdering(OrderingType.Natural)
+    s.setPrecision(Precision.Mixed if args.precision == "mixed" else Precision.FP64)
+    s.analyzePattern(A)
+    for _ in range(max(1, args.warmup)):
+        s.factorize(A)
+    lib = L.load()
+    lib.symla_gpu_reset_kernel_stats(s._ctx.h)
+    lib.symla_gpu_set_profiling(s._ctx.h, 1)
+    times = []
+    for _ in range(max(1, args.steps)):
+        s.factorize(A)
+        times.append(s.phase_ms()[6])
+    lib.symla_gpu_set_profiling(s._ctx.h, 0)
+    buf = (C.c_double * 4)()
+    ks = {}
+    for kind, name in enumerate(L.KERNEL_KINDS):
+        lib.symla_gpu_kernel_stats(s._ctx.h, kind, buf)
+        if buf[0]:
+            ks[name] = {"launches": buf[0] / len(times), "ms": buf[1] / len(times)}
+    print(json.dumps({"workload": f"dense front n={n} (natural order, one front)", "precision": args.precision,
+                      "factor_ms": min(times), "inertia": list(s.inertia().as_tuple()), "kernels": ks,
+                      "panels": {k: v for k, v in s.plan_stats().items() if k.startswith("panels_")}}), flush=True)
+
+
+def run_batched(args):
+    """Config 4: independent L5-minus-shift systems of uneven size, factorized
+    and solved together (ma57_b200.batch: one block-diagonal plan, level
+    launches shared by all systems, graph launch of the factorization).
+    value = systems per second of factorize + 8-RHS solve with the matrices
+    and right-hand sides resident on the device; the per-system latency
+    percentiles come from factorizing + solving a sample of the systems one
+    at a time through the same library."""
+    import numpy as np
+    import torch
+    from ma57_b200 import SymLDLT
+    from ma57_b200 import _lib as L
+    from ma57_b200 import autotune
+    from ma57_b200 import matrices as M
+    from ma57_b200.batch import BatchedSolver
+    from ma57_b200.solver import as_csc
+    count, nrhs = args.systems, 8
+    systems = [M.config4_system(i) for i in range(count)]
+    mats = [A for A, _, _, _ in systems]
+    Bs = []
+    for i, A in enumerate(mats):
+        st = M.Stream(M.SEED_BASE + 4 + 7_000_001 * (i + 1))
+        Bs.append(st.normal(A.shape[0] * nrhs).reshape(nrhs, A.shape[0]).T.copy(order="F"))
+    t0 = time.perf_counter()
+    bs = BatchedSolver(mats, graph=bool(args.graph))
+    t_setup = time.perf_counter() - t0
+    lib = L.load()
+    s = bs.solver
+    bs.factorize()
+    schedule, t_default, t_tuned = autotune.tune(s, bs.A, reps=2)
+    n = bs.n
+    _, cp, ri, vals = as_csc(bs.A)
+    h = s._ctx.h
+    dev = torch.device("cuda", 0)
+    d_vals = torch.from_numpy(vals).to(dev)
+    d_B = torch.from_numpy(np.ascontiguousarray(bs.stack(Bs).T)).to(dev)
+    d_X = torch.zeros((nrhs, n), dtype=torch.float64, device=dev)
+    pv = C.cast(C.c_void_p(d_vals.data_ptr()), L._pd)
+    pB = C.cast(C.c_void_p(d_B.data_ptr()), L._pd)
+    pX = C.cast(C.c_void_p(d_X.data_ptr()), L._pd)
+    opts = L.FactorOpts()
+    lib.symla_factor_opts_default(C.byref(opts))
+    info = L.FactorInfo()
+    stream = torch.cuda.ExternalStream(lib.symla_gpu_stream(h), device=dev)
+
+    def step():
+        if lib.symla_gpu_factorize(h, pv, 1, C.byref(opts), C.byref(info)) != 0:
+            raise RuntimeError(L.last_error())
+        if lib.symla_gpu_solve(h, pB, n, nrhs, pX, n, 1) != 0:
+            raise RuntimeError(L.last_error())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clk = clocks_start(0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clocks_stop(clk)
+    ms = e0.elapsed_time(e1) / args.steps
+    X = d_X.cpu().numpy().T
+    Xs = bs.unstack(np.asfortranarray(X))
+    worst = 0.0
+    for A, B, Xi in zip(mats[:256], Bs[:256], Xs[:256]):
+        Af = M.sym_full(A)
+        R = B - Af @ Xi
+        worst = max(worst, np.abs(R).max() / (abs(A).sum(axis=1).max() * np.abs(Xi).max() + np.abs(B).max()))
+    # per-system latency, one at a time (factorize + solve, device timing)
+    lat = []
+    for idx in np.linspace(0, count - 1, 64).astype(int):
+        A, B = mats[idx], Bs[idx]
+        si = SymLDLT()
+        si.analyzePattern(A)
+        si.factorize(A)
+        si.solve(B)
+        si.factorize(A)
+        si.solve(B)
+        ph = si.phase_ms()
+        lat.append(ph[6] + ph[7])
+    line = {"metric": "batched factorize+solve throughput", "value": count / (ms * 1e-3), "unit": "systems/s",
+            "higher_is_better": True, "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
+            "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"config 4: {count} systems L5(a x b) - sigma I, n in [200, 4000], nrhs={nrhs}",
+                       "total_n": n, "graph": bool(args.graph), "setup_s": t_setup,
+                       "autotune": {"schedule": {k: {str(b): v for b, v in d.items()} for k, d in schedule.items()},
+                                    "default_factor_ms": t_default, "tuned_factor_ms": t_tuned},
+                       "graph_stats": s.graphStats(), "max_backward_error_first_256": worst},
+            "per_system_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                              "sample": "64 systems spread over the sizes, factorize + solve each alone"},
+            "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
+def run_learned(args):
+    """Config 5: an interior-point sequence of KKT refactorizations in
+    StaticRegularized mode. Plain escalation (first delta 1e-14 max|K|, x10
+    per failed inertia check) runs the first `ip_train` matrices and its
+    accepted deltas train the network on the GPU; the remaining matrices are
+    then run twice from the same state of the sequence, with plain
+    escalation and with the network's first-attempt deltas. Reported: mean
+    retries and total time (factorize + refinement towards 1e-10)."""
+    import math
+    import numpy as np
+    from ma57_b200 import Mode, OrderingType, RefinementOptions, SymLDLT, learned
+    from ma57_b200 import matrices as M
+    seq = M.InteriorPointSequence(k=20, steps=args.ip_steps, curvature_shift=args.curvature_shift)
+    signs = np.r_[-np.ones(seq.n1), np.ones(seq.n2)]
+
+    def run(steps, model):
+        s = SymLDLT()
+        s.setMode(Mode.StaticRegularized)
+        s.setOrdering(OrderingType.AMD)
+        s.setKKTBlockSizes(seq.n1, seq.n2)
+        s.setMaxRegularizationRetries(40)
+        sym = None
+        out = {"retries": [], "resid": [], "ms": [], "feats": [], "targets": []}
+        for step in steps:
+            K, _ = seq.matrix(step)
+            if sym is None:
+                s.analyzePattern(K)
+                sym = s.symbolicFactor()
+            F = learned.front_features(sym, K, signs)
+            t0 = time.perf_counter()
+            s.setInitialRegularizationDelta(1e-14 * abs(K.data).max())
+            s.setFrontDeltas(None if model is None else model.front_deltas(F))
+            s.factorize(K)
+            r = s.solveWithRefinement(K, seq.b, RefinementOptions(max_iterations=30, tolerance=1e-10))
+            out["ms"].append(1e3 * (time.perf_counter() - t0))
+            out["retries"].append(s.regularizationRetriesUsed())
+            out["resid"].append(r.diagnostics.final_relative_residual)
+            out["feats"].append(F)
+            out["targets"].append(np.full(F.shape[0], math.log10(s.lastRegularizationDelta())))
+        return out
+
+    train = run(range(args.ip_train), None)
+    model = learned.DeltaModel(seed=3, margin=0.5)
+    t0 = time.perf_counter()
+    loss = model.fit(np.vstack(train["feats"]), np.concatenate(train["targets"]), epochs=300, lr=3e-3,
+                     minibatch=4096)
+    t_train = time.perf_counter() - t0
+    state = (seq.logx.copy(), seq.st.pos)
+    plain = run(range(args.ip_train, args.ip_steps), None)
+    seq.logx, seq.st.pos = state
+    lrn = run(range(args.ip_train, args.ip_steps), model)
+    summ = lambda o: {"mean_retries": float(np.mean(o["retries"])), "total_s": float(np.sum(o["ms"]) / 1e3),
+                      "refined_to_1e-10": int(np.sum(np.asarray(o["resid"]) <= 1e-10)),
+                      "median_residual": float(np.median(o["resid"]))}
+    line = {"metric": "interior-point sequence: mean retries and total time, learned vs plain escalation",
+            "config": {"workload": f"config 5: K_k = [[-E_k, A^T], [A, F_k]], n1={seq.n1}, n2={seq.n2}, "
+                                   f"{args.ip_steps} matrices (train {args.ip_train})",
+                       "curvature_shift": args.curvature_shift, "train_samples": int(sum(len(t) for t in train["targets"])),
+                       "train_loss": loss, "train_s": t_train},
+            "plain": summ(plain), "learned": summ(lrn), "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -149,8 +381,8 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"L27({args.k}^3)-3I, METIS ND, nrhs={args.nrhs}, refine to 1e-12",
-                   "parallelism": "cpu-openmp-task-dag"},
+        "config": {"workload": f"L27({args.k}^3)-3I (n={args.k ** 3}), METIS ND, nrhs={args.nrhs}, "
+                               f"factorize+solve+refine to 1e-12", "parallelism": "cpu-openmp-task-dag"},
         "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port",
                          "sample": f"oracle (CPU restatement; the reference needs Eigen/SuiteSparse/LAPACK, absent) "
                                    f"factorize+solve+refine on L27({k_sample}^3)-3I, best of {max(1, args.steps)}, "
@@ -215,13 +447,13 @@ def run_ours(args):
         check(lib.symla_gpu_factorize(h, pv, 1, C.byref(opts), C.byref(info)))
         check(lib.symla_gpu_solve_refine(h, pv, pB, n, nrhs, pX, n, 1, 10, 1e-12, C.byref(rinfo)))
 
+    lib.symla_gpu_set_graph(h, int(args.graph))
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     lib.symla_gpu_reset_kernel_stats(h)
-    lib.symla_gpu_set_profiling(h, 1)
     clk = clocks_start(local)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -234,13 +466,20 @@ def run_ours(args):
     ev1.record(stream)
     torch.cuda.synchronize()
     clocks = clocks_stop(clk)
-    lib.symla_gpu_set_profiling(h, 0)
+    launches = int(lib.symla_gpu_launch_count(h)) // max(1, args.steps)
     ms = ev0.elapsed_time(ev1) / args.steps
+    # per-kernel breakdown from extra, instrumented steps (CUDA events around
+    # every launch), kept out of the timed region above
+    lib.symla_gpu_reset_kernel_stats(h)
+    lib.symla_gpu_set_profiling(h, 1)
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    lib.symla_gpu_set_profiling(h, 0)
     if dist:
         t = torch.tensor([ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    launches = int(lib.symla_gpu_launch_count(h)) // max(1, args.steps)
     kstats = {}
     buf = (C.c_double * 4)()
     for kind, name in enumerate(L.KERNEL_KINDS):
@@ -274,19 +513,27 @@ def run_ours(args):
     bw = float(np.abs(R).max() / (normA * np.abs(Xh).max() + np.abs(Bh).max()))
 
     peaks, peak_kind = load_peaks()
-    tr = kstats["far_update"]
-    achieved = (tr[2] / (tr[1] * 1e-3)) / 1e12 if tr[1] > 0 else 0.0
-    if prec == L.PREC_MIXED:
+    steps = max(1, args.steps)
+    # the dominant kernel kind by device time, with the roofline that bounds it
+    pbytes = panel_bytes(args.k) * steps
+    kstats["panel"][3] = pbytes
+    dom = max(kstats, key=lambda kk: kstats[kk][1])
+    launches_k, ms_k, flops_k, bytes_k = kstats[dom]
+    if dom in ("far_update", "near_update", "small"):
+        achieved = (flops_k / (ms_k * 1e-3)) / 1e12 if ms_k > 0 else 0.0
         peak = peaks.get("bf16_tflops")
-        peak_note = f"dense bf16 tensor, {peak_kind}"
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "peak_source": f"dense bf16 tensor, {peak_kind}",
+                    "algorithmic_flops_per_launch": flops_k / max(1, launches_k)}
     else:
-        peak = peaks.get("bf16_tflops")
-        peak_note = f"dense bf16 tensor, {peak_kind} (FP64 kernel timed against the tensor peak)"
-    roofline = {"bound": "tensor", "kernel": "far (outer-block) Schur-complement update", "achieved": achieved,
-                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
-                "traffic": None, "peak_source": peak_note,
-                "launches_per_step": tr[0] / max(1, args.steps), "ms_per_step": tr[1] / max(1, args.steps),
-                "algorithmic_flops_per_step": tr[2] / max(1, args.steps)}
+        achieved = (bytes_k / (ms_k * 1e-3)) / 1e9 if ms_k > 0 else 0.0
+        peak = peaks.get("hbm_gbs")
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "peak_source": f"HBM copy, {peak_kind}",
+                    "algorithmic_bytes_per_launch": bytes_k / max(1, launches_k)}
+    roofline.update({"frac": achieved / peak if peak else None, "traffic": profiled_traffic(dom), "kernel": dom,
+                     "launches_per_step": launches_k / steps, "ms_per_step": ms_k / steps,
+                     "avg_launch_us": 1e3 * ms_k / max(1, launches_k)})
 
     line = {
         "metric": METRIC, "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
@@ -294,7 +541,7 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "f64" if prec == L.PREC_FP64 else "f64+mixed-schur", "data": "synthetic",
         "config": {"workload": f"L27({args.k}^3)-3I (n={n}), METIS ND, nrhs={nrhs}, factorize+solve+refine to 1e-12",
                    "precision": args.precision, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (fronts 11 GB)", "inertia": list(s.inertia().as_tuple()),
+                   "l2": "inputs larger than L2 (fronts 11 GB)", "inertia": [info.n_pos, info.n_neg, info.n_zero],
                    "backward_error": bw, "refine_iterations": rinfo.iterations,
                    "analyze_s": t_analyze, "factor_flops": stats.get("factor_flops"),
                    "kernel_ms_per_step": {k: v[1] / max(1, args.steps) for k, v in kstats.items()}},
@@ -328,9 +575,23 @@ def main():
     ap.add_argument("--nrhs", type=int, default=16)
     ap.add_argument("--cpu-k", type=int, default=32)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--graph", type=int, default=1, help="graph launch of the factorization's static pass")
+    ap.add_argument("--workload", default="config3", choices=["config3", "dense", "batched", "learned"])
+    ap.add_argument("--curvature-shift", type=float, default=0.0,
+                    help="learned workload: 0 = config 5 as specified; c > 0 = E_k - c I (nonconvex variant)")
+    ap.add_argument("--ip-steps", type=int, default=500)
+    ap.add_argument("--ip-train", type=int, default=100)
+    ap.add_argument("--n", type=int, default=4096, help="dense workload: front size")
+    ap.add_argument("--systems", type=int, default=4096, help="batched workload: number of systems")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "dense":
+        run_dense(args)
+    elif args.workload == "batched":
+        run_batched(args)
+    elif args.workload == "learned":
+        run_learned(args)
     else:
         run_ours(args)
 

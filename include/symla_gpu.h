@@ -237,6 +237,26 @@ enum { SYMLA_KERNEL_TRAILING = 0, SYMLA_KERNEL_PANEL = 1, SYMLA_KERNEL_SMALL = 2
        SYMLA_KERNEL_FORWARD = 4, SYMLA_KERNEL_BACKWARD = 5, SYMLA_KERNEL_RESIDUAL = 6, SYMLA_KERNEL_NEAR = 7,
        SYMLA_KERNEL_KINDS = 8 };
 int symla_gpu_set_profiling(symla_gpu_ctx* ctx, int enable);
+
+/* Graph launch of the factorization (no reference counterpart): when
+ * enabled (and profiling is off), the static pass over all tree levels, with
+ * a few spare panel iterations per level, is captured once per set of
+ * factorization options into a CUDA graph and replayed by every later
+ * factorize; a level that its planned iterations did not finish (or a
+ * delayed pivot) is continued on the host exactly as without the graph.
+ * graph_stats: captures made and factorizations that needed that host
+ * continuation. */
+int symla_gpu_set_graph(symla_gpu_ctx* ctx, int enable);
+
+/* Tile schedule per tree level (no reference counterpart; chosen by the
+ * autotuner in ma57_b200/autotune.py). level_info: out6 = {small fronts,
+ * their max m, large fronts, their max m, small-front kernel threads, panel
+ * cluster CTAs}. set_level_schedule: small-front kernel threads in {128,
+ * 256} and panel cluster size in {8, 16}, 0 = chosen by front size; a
+ * cluster size too small for the level's fronts falls back to the default. */
+int symla_gpu_level_info(symla_gpu_ctx* ctx, int level, int* out6);
+int symla_gpu_set_level_schedule(symla_gpu_ctx* ctx, int level, int small_threads, int cluster_ctas);
+int symla_gpu_graph_stats(symla_gpu_ctx* ctx, int* captures, int* resumes);
 int symla_gpu_kernel_stats(symla_gpu_ctx* ctx, int kind, double* out4);
 void symla_gpu_reset_kernel_stats(symla_gpu_ctx* ctx);
 /* Number of kernels the library launched since the last reset. */
@@ -250,6 +270,32 @@ long long symla_gpu_launch_count(symla_gpu_ctx* ctx);
  * (one sequential decision), [10] run sequentially throughout. Returns the
  * number of entries (11). */
 int symla_gpu_plan_stats(symla_gpu_ctx* ctx, double* out, int cap);
+
+/* Learned first-attempt delta for Mode::StaticRegularized (no reference
+ * counterpart; the reference starts every factorization's escalation from
+ * the same delta, solver.hpp:328-417). A multilayer perceptron maps
+ * SYMLA_MLP_INPUTS standardised per-front statistics to log10 of the
+ * front's first-attempt delta (symla_regularize_opts.front_delta), trained
+ * on the GPU from the deltas the escalation loop itself accepted; on an
+ * inertia failure the plain escalation runs as before. FP64; parameters in
+ * the order W1 (H x IN, row-major), b1 (H), W2 (H x H), b2 (H), w3 (H), b3. */
+#define SYMLA_MLP_INPUTS 8
+#define SYMLA_MLP_HIDDEN 32
+#define SYMLA_MLP_PARAMS (SYMLA_MLP_HIDDEN * SYMLA_MLP_INPUTS + SYMLA_MLP_HIDDEN + SYMLA_MLP_HIDDEN * SYMLA_MLP_HIDDEN + \
+                          SYMLA_MLP_HIDDEN + SYMLA_MLP_HIDDEN + 1)
+typedef struct symla_mlp symla_mlp;
+int symla_mlp_create(int device, const double* params, symla_mlp** out);
+void symla_mlp_destroy(symla_mlp* mlp);
+int symla_mlp_get_params(symla_mlp* mlp, double* params_out);
+/* Y[s] = network(X[s, :]) for B samples (X row-major B x SYMLA_MLP_INPUTS, host). */
+int symla_mlp_predict(symla_mlp* mlp, const double* X, int B, double* Y);
+/* Gradient of the mean squared error (1/B) sum (Y - T)^2 w.r.t. the
+ * parameters, and that error, at the current parameters. */
+int symla_mlp_gradient(symla_mlp* mlp, const double* X, const double* T, int B, double* grad, double* loss);
+/* Adam (beta 0.9 / 0.999) over `epochs` passes of minibatches (<= 0: full
+ * batch); final_loss (optional) = mean squared error after training. */
+int symla_mlp_train(symla_mlp* mlp, const double* X, const double* T, int B, int epochs, int minibatch, double lr,
+                    double* final_loss);
 
 /* Relative residual ||B - A X||_inf / (||A||_inf ||X||_inf + ||B||_inf) of
  * a device-resident candidate solution X against device-resident B

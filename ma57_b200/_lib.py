@@ -95,11 +95,25 @@ _SIGS = {
     "symla_gpu_phase_ms": (_i, [_p, _pf, _i]),
     "symla_gpu_plan_stats": (_i, [_p, _pd, _i]),
     "symla_gpu_set_profiling": (_i, [_p, _i]),
+    "symla_gpu_set_graph": (_i, [_p, _i]),
+    "symla_gpu_level_info": (_i, [_p, _i, _pi]),
+    "symla_gpu_set_level_schedule": (_i, [_p, _i, _i, _i]),
+    "symla_gpu_graph_stats": (_i, [_p, _pi, _pi]),
     "symla_gpu_kernel_stats": (_i, [_p, _i, _pd]),
     "symla_gpu_reset_kernel_stats": (None, [_p]),
     "symla_gpu_launch_count": (C.c_longlong, [_p]),
     "symla_gpu_relative_residual_noalloc": (_i, [_p, _p, _i, _p, _i, _i, _pd]),
+    "symla_mlp_create": (_i, [_i, _pd, C.POINTER(_p)]),
+    "symla_mlp_destroy": (None, [_p]),
+    "symla_mlp_get_params": (_i, [_p, _pd]),
+    "symla_mlp_predict": (_i, [_p, _pd, _i, _pd]),
+    "symla_mlp_gradient": (_i, [_p, _pd, _pd, _i, _pd, _pd]),
+    "symla_mlp_train": (_i, [_p, _pd, _pd, _i, _i, _i, _d, _pd]),
 }
+
+MLP_INPUTS = 8
+MLP_HIDDEN = 32
+MLP_PARAMS = MLP_HIDDEN * MLP_INPUTS + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_HIDDEN + 1
 
 NOALLOC_RESIDUAL_MAX_ENTRIES = 1 << 20
 

@@ -662,7 +662,8 @@ void timed(symla_gpu_ctx* c, int kind, double flops, double bytes, F&& launch);
 void collect_pending(symla_gpu_ctx* c);
 
 KernelOpts make_kernel_opts(symla_gpu_ctx* c, const symla_factor_opts* o) {
-  KernelOpts k{};
+  KernelOpts k;
+  std::memset(&k, 0, sizeof k);  // padding too: graph reuse compares the bytes
   k.mode = o->mode;
   k.precision = o->precision;
   k.zero_tol = o->zero_tolerance;
@@ -686,7 +687,7 @@ void launch_panel_iteration(symla_gpu_ctx* c, const LevelLists& L, int level, co
   timed(c, SYMLA_KERNEL_PANEL, 0.0, 0.0, [&] {
     if (c->use_cluster_panel && cluster_size_for(L.large_max_m, nl) > 0) {
       CK(launch_cluster_panel(c->d_desc, c->d_state, d_large, nl, L.large_max_m, kPanelWidth, ko, c->d_glob, level,
-                              dynamic, st));
+                              dynamic, st, L.cluster_ctas));
     } else {
       launch_panel(c->d_desc, c->d_state, d_large, nl, L.large_max_m, kPanelWidth, ko, c->d_glob, level, dynamic,
                    st);
@@ -718,22 +719,42 @@ void launch_panel_iteration(symla_gpu_ctx* c, const LevelLists& L, int level, co
   }
 }
 
-void launch_level(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
-                  const int* d_small, const int* d_large, const int* d_tasks) {
+// The level's kernels with `iters` panel iterations, no host synchronisation
+// (the part a graph launch captures).
+void launch_level_planned(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
+                          const int* d_small, const int* d_large, const int* d_tasks, int iters) {
   cudaStream_t st = c->stream;
   if (!L.small.empty())
     timed(c, SYMLA_KERNEL_SMALL, L.small_flops, 0.0, [&] {
       launch_factor_small(c->d_desc, c->d_links, c->d_state, d_small, static_cast<int>(L.small.size()),
-                          L.small_max_m, c->d_a_colptr, ko, c->d_glob, level, dynamic, st);
+                          L.small_max_m, c->d_a_colptr, ko, c->d_glob, level, dynamic, st, L.small_threads);
     });
   if (!L.large.empty()) {
     timed(c, SYMLA_KERNEL_ASSEMBLE, 0.0, L.assemble_bytes, [&] {
       launch_assemble(c->d_desc, c->d_links, c->d_state, d_tasks, static_cast<int>(L.tasks.size() / 2),
                       c->d_a_colptr, ko, c->d_glob, level, dynamic, st);
     });
-    for (int it = 0; it < L.panels; ++it) launch_panel_iteration(c, L, level, ko, dynamic, d_large);
-    // Flushes (a partner beyond the outer block) and 2x2 pivots can leave a
-    // front unfinished after the planned iterations: run more until done.
+    for (int it = 0; it < iters; ++it) launch_panel_iteration(c, L, level, ko, dynamic, d_large);
+  }
+}
+
+void complete_level(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
+                    const int* d_large);
+
+void launch_level(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
+                  const int* d_small, const int* d_large, const int* d_tasks) {
+  launch_level_planned(c, L, level, ko, dynamic, d_small, d_large, d_tasks, L.panels);
+  if (!L.large.empty()) complete_level(c, L, level, ko, dynamic, d_large);
+  CK(cudaGetLastError());
+}
+
+// Flushes (a partner beyond the outer block), 2x2 pivots and speculative
+// panels that stop at a failing pivot can leave a front unfinished after
+// the planned iterations: run more until done.
+void complete_level(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
+                    const int* d_large) {
+  cudaStream_t st = c->stream;
+  {
     const int nl = static_cast<int>(L.large.size());
     int guard = 0;
     for (;;) {
@@ -751,6 +772,42 @@ void launch_level(symla_gpu_ctx* c, const LevelLists& L, int level, const Kernel
     }
   }
   CK(cudaGetLastError());
+}
+
+// Graph launch of the static pass: every level with its planned panel
+// iterations plus slack, each level marking itself if a front is still
+// unfinished (the later levels then return at once). Captured once per set
+// of kernel options and replayed; no host synchronisation inside.
+int graph_iters(const LevelLists& L) { return L.panels + L.panels / 4 + 2; }
+
+void run_static_pass_graph(symla_gpu_ctx* c, const KernelOpts& ko) {
+  cudaStream_t st = c->stream;
+  const bool same = c->graph_exec && std::memcmp(&c->graph_ko, &ko, sizeof ko) == 0;
+  if (!same) {
+    if (c->graph_exec) {
+      cudaGraphExecDestroy(c->graph_exec);
+      c->graph_exec = nullptr;
+    }
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    for (int l = 0; l < c->numLevels; ++l) {
+      const LevelLists& L = c->levels[l];
+      launch_level_planned(c, L, l, ko, 0, L.d_small, L.d_large, L.d_tasks, graph_iters(L));
+      if (!L.large.empty())
+        launch_mark_unfinished(c->d_state, L.d_large, static_cast<int>(L.large.size()), c->d_glob, l, st);
+    }
+    const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+    if (ec != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      CK(ec);
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&c->graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    CK(ei);
+    c->graph_ko = ko;
+    ++c->graph_captures;
+  }
+  CK(cudaGraphLaunch(c->graph_exec, st));
 }
 
 // Re-plan front s whose children delayed columns (multifrontal.hpp:453-479)
@@ -866,7 +923,7 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
   reset_to_static(c);
   const KernelOpts ko = make_kernel_opts(c, o);
   CK(cudaMemsetAsync(c->d_state, 0, c->numSN * sizeof(FrontState), st));
-  FactorGlobals g0{INT_MAX, 0, -1, 0, 0.0, 0.0, 0.0, 0, 0, 0, 0};
+  FactorGlobals g0{INT_MAX, 0, -1, INT_MAX, 0.0, 0.0, 0.0, 0, 0, 0, 0};
   CK(cudaMemcpyAsync(c->d_glob, &g0, sizeof g0, cudaMemcpyHostToDevice, st));
   const bool mixed = o->precision == SYMLA_PREC_MIXED;
   if (mixed) {
@@ -875,9 +932,28 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
     launch_absmax(c->d_values, c->nnz, &c->d_glob->amax, st);  // scale of the growth guard
   }
   CK(cudaEventRecord(c->ev[0], st));
-  for (int l = 0; l < c->numLevels; ++l) {
-    const LevelLists& L = c->levels[l];
-    launch_level(c, L, l, ko, 0, L.d_small, L.d_large, L.d_tasks);
+  if (c->use_graph && !c->profiling) {
+    run_static_pass_graph(c, ko);
+    FactorGlobals gg;
+    CK(cudaMemcpyAsync(&gg, c->d_glob, sizeof gg, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (gg.unfinished_level != INT_MAX && gg.unfinished_level <= gg.delay_level) {
+      // resume on the host: finish that level, then run the later ones
+      const int u = gg.unfinished_level;
+      const int none = INT_MAX;
+      CK(cudaMemcpyAsync(&c->d_glob->unfinished_level, &none, sizeof none, cudaMemcpyHostToDevice, st));
+      ++c->graph_resumes;
+      complete_level(c, c->levels[u], u, ko, 0, c->levels[u].d_large);
+      for (int l = u + 1; l < c->numLevels; ++l) {
+        const LevelLists& L = c->levels[l];
+        launch_level(c, L, l, ko, 0, L.d_small, L.d_large, L.d_tasks);
+      }
+    }
+  } else {
+    for (int l = 0; l < c->numLevels; ++l) {
+      const LevelLists& L = c->levels[l];
+      launch_level(c, L, l, ko, 0, L.d_small, L.d_large, L.d_tasks);
+    }
   }
   FactorGlobals g;
   CK(cudaMemcpyAsync(&g, c->d_glob, sizeof g, cudaMemcpyDeviceToHost, st));
@@ -1244,6 +1320,7 @@ extern "C" int symla_gpu_create(const symla_symbolic* sym, int n, const int* col
 extern "C" void symla_gpu_destroy(symla_gpu_ctx* c) {
   if (!c) return;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   free_dynamic(c);
   for (auto& L : c->levels) free_level_device(L);
   void* ptrs[] = {c->d_arena, c->d_fidx, c->d_lperm, c->d_lpos, c->d_Dd, c->d_Do, c->d_pk, c->d_maps, c->d_desc, c->d_links, c->d_state,
@@ -1610,6 +1687,48 @@ extern "C" int symla_gpu_plan_stats(symla_gpu_ctx* c, double* out, int cap) {
   for (int i = 0; i < 4; ++i) v[7 + i] = c->panel_counts[i];
   for (int i = 0; i < cap && i < 11; ++i) out[i] = v[i];
   return 11;
+}
+
+extern "C" int symla_gpu_level_info(symla_gpu_ctx* c, int level, int* out6) {
+  if (!c || level < 0 || level >= c->numLevels || !out6) return set_error(SYMLA_ERR_INVALID, "bad arguments");
+  const auto& L = c->levels[level];
+  out6[0] = static_cast<int>(L.small.size());
+  out6[1] = L.small_max_m;
+  out6[2] = static_cast<int>(L.large.size());
+  out6[3] = L.large_max_m;
+  out6[4] = L.small_threads;
+  out6[5] = L.cluster_ctas;
+  return SYMLA_OK;
+}
+
+extern "C" int symla_gpu_set_level_schedule(symla_gpu_ctx* c, int level, int small_threads, int cluster_ctas) {
+  if (!c || level < 0 || level >= c->numLevels) return set_error(SYMLA_ERR_INVALID, "level out of range");
+  if ((small_threads != 0 && small_threads != 128 && small_threads != 256) ||
+      (cluster_ctas != 0 && cluster_ctas != 8 && cluster_ctas != 16))
+    return set_error(SYMLA_ERR_INVALID, "symla_gpu_set_level_schedule: small_threads in {0,128,256}, cluster_ctas in {0,8,16}");
+  auto& L = c->levels[level];
+  if (L.small_threads != small_threads || L.cluster_ctas != cluster_ctas) {
+    L.small_threads = small_threads;
+    L.cluster_ctas = cluster_ctas;
+    if (c->graph_exec) {  // the captured launches used the old shapes
+      cudaGraphExecDestroy(c->graph_exec);
+      c->graph_exec = nullptr;
+    }
+  }
+  return SYMLA_OK;
+}
+
+extern "C" int symla_gpu_set_graph(symla_gpu_ctx* c, int enable) {
+  if (!c) return set_error(SYMLA_ERR_INVALID, "null context");
+  c->use_graph = enable != 0;
+  return SYMLA_OK;
+}
+
+extern "C" int symla_gpu_graph_stats(symla_gpu_ctx* c, int* captures, int* resumes) {
+  if (!c) return set_error(SYMLA_ERR_INVALID, "null context");
+  if (captures) *captures = c->graph_captures;
+  if (resumes) *resumes = c->graph_resumes;
+  return SYMLA_OK;
 }
 
 extern "C" int symla_gpu_set_profiling(symla_gpu_ctx* c, int enable) {

@@ -83,7 +83,7 @@ struct FactorGlobals {
   int delay_level;     // lowest level that produced a delayed column, or INT_MAX
   int error;           // nonzero: internal error code
   int err_front;
-  int pad;
+  int unfinished_level;  // graph launches: lowest level left unfinished after its planned iterations
   double flops_near;   // algorithmic flops of the near (in-block) updates
   double flops_far;    // algorithmic flops of the far (deferred) updates
   double amax;         // max |a_ij| of the matrix being factorized (mixed precision only)
@@ -91,6 +91,14 @@ struct FactorGlobals {
   // whole panel / a prefix / failed at its first pivot; whole sequential panels
   int spec_full, spec_partial, spec_failed, seq_panels;
 };
+
+// Kernels of a level return at once when an earlier level stopped the
+// planned (static) pass: a delayed pivot (delay_level) or, in a graph
+// launch, a level whose planned panel iterations did not finish it
+// (unfinished_level). The host then continues from there.
+__device__ __forceinline__ bool level_skipped(const FactorGlobals* g, int level, int dynamic) {
+  return !dynamic && min(g->delay_level, g->unfinished_level) < level;
+}
 
 // Options visible to kernels.
 struct KernelOpts {

@@ -31,6 +31,8 @@ struct LevelLists {
   int small_max_m = 0;
   std::vector<int> large;      // other fronts
   int large_max_m = 0;
+  int small_threads = 0;       // tile schedule (autotuner): small-front kernel width, 0 = by size
+  int cluster_ctas = 0;        // panel cluster size, 0 = by size
   int panels = 0;              // panel iterations needed
   int trailing_grid = 0;
   std::vector<int> tasks;      // assembly tasks (front, column block) for large fronts
@@ -177,6 +179,12 @@ struct symla_gpu_ctx {
 
   // panel kernel choice (the cluster kernel unless SYMLA_PANEL=single)
   bool use_cluster_panel = true;
+
+  // graph launch of the factorization's static pass
+  bool use_graph = false;
+  cudaGraphExec_t graph_exec = nullptr;
+  symla_gpu::KernelOpts graph_ko{};
+  int graph_captures = 0, graph_resumes = 0;
 
   // instrumentation
   bool profiling = false;

@@ -29,7 +29,7 @@ namespace {
 constexpr double kAlpha = 0.64038820320220756;  // (1 + sqrt(17)) / 8
 
 __device__ __forceinline__ bool level_aborted(const FactorGlobals* g, int level, int dynamic) {
-  return !dynamic && g->delay_level < level;
+  return level_skipped(g, level, dynamic);
 }
 
 // Child contribution to parent entry (i, j) (i >= j in the parent's local
@@ -61,22 +61,74 @@ __device__ __forceinline__ int a_local_row(int pos, int ncols, int nextra) {
 // Assembly of large fronts in global memory: one CTA per (front, 32-column
 // block). Every parent entry is written exactly once (gather form), so no
 // separate zero fill and no atomics; then the A entries of the block's own
-// columns are added.
+// columns are added. The children's map pointers, contribution-block
+// origins and their maps of the block's 32 columns are staged in shared
+// memory once; each thread then takes rows, reads a row's position in each
+// child once and issues the (independent) loads of all 32 columns, summing
+// over the children in their fixed order.
+namespace {
+constexpr int kAsmMaxChildren = 16;
+}
+
 __global__ void __launch_bounds__(256) assemble_kernel(const FrontDesc* __restrict__ fronts,
                                                        const ChildLink* __restrict__ links,
                                                        FrontState* st, const int* __restrict__ tasks,
                                                        const int* __restrict__ a_colptr, KernelOpts o,
                                                        const FactorGlobals* __restrict__ g, int level, int dynamic) {
   if (level_aborted(g, level, dynamic)) return;
+  __shared__ const int* s_inv[kAsmMaxChildren];
+  __shared__ const double* s_cb[kAsmMaxChildren];
+  __shared__ int64_t s_ld[kAsmMaxChildren];
+  __shared__ int s_b[kAsmMaxChildren][32];
   const int s = tasks[2 * blockIdx.x];
   const int j0 = tasks[2 * blockIdx.x + 1];
   const FrontDesc f = fronts[s];
-  const int j1 = min(j0 + 32, f.m);
-  if (threadIdx.x < j1 - j0) f.lperm[j0 + threadIdx.x] = j0 + threadIdx.x;
-  for (int j = j0; j < j1; ++j) {
-    double* col = f.F + static_cast<int64_t>(j) * f.ld;
-    for (int i = j + threadIdx.x; i < f.m; i += blockDim.x)
-      col[i] = gather_children(fronts, links, st, f.ch_begin, f.ch_end, i, j);
+  const int j1 = min(j0 + 32, f.m), nj = j1 - j0;
+  const int nch = f.ch_end - f.ch_begin;
+  if (threadIdx.x < nj) f.lperm[j0 + threadIdx.x] = j0 + threadIdx.x;
+  if (nch <= kAsmMaxChildren) {
+    if (threadIdx.x < nch) {
+      const ChildLink L = links[f.ch_begin + threadIdx.x];
+      const FrontDesc& cf = fronts[L.child];
+      const int np = st[L.child].npiv;
+      s_inv[threadIdx.x] = L.invmap;
+      s_cb[threadIdx.x] = cf.F + static_cast<int64_t>(np) * cf.ld + np;  // contribution block origin
+      s_ld[threadIdx.x] = cf.ld;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nch * 32; t += blockDim.x) {
+      const int c = t / 32, jj = t % 32;
+      s_b[c][jj] = (jj < nj) ? s_inv[c][j0 + jj] : -1;
+    }
+    __syncthreads();
+    for (int i = j0 + threadIdx.x; i < f.m; i += blockDim.x) {
+      double acc[32];
+#pragma unroll
+      for (int jj = 0; jj < 32; ++jj) acc[jj] = 0.0;
+      for (int c = 0; c < nch; ++c) {
+        const int a = s_inv[c][i];
+        if (a < 0) continue;
+        const double* cb = s_cb[c];
+        const int64_t cld = s_ld[c];
+#pragma unroll
+        for (int jj = 0; jj < 32; ++jj) {
+          const int b = s_b[c][jj];
+          if (b >= 0 && j0 + jj <= i) {
+            const int r = a > b ? a : b, cc = a > b ? b : a;
+            acc[jj] += cb[static_cast<int64_t>(cc) * cld + r];
+          }
+        }
+      }
+#pragma unroll
+      for (int jj = 0; jj < 32; ++jj)
+        if (jj < nj && j0 + jj <= i) f.F[static_cast<int64_t>(j0 + jj) * f.ld + i] = acc[jj];
+    }
+  } else {
+    for (int j = j0; j < j1; ++j) {
+      double* col = f.F + static_cast<int64_t>(j) * f.ld;
+      for (int i = j + threadIdx.x; i < f.m; i += blockDim.x)
+        col[i] = gather_children(fronts, links, st, f.ch_begin, f.ch_end, i, j);
+    }
   }
   __syncthreads();
   if (j0 < f.ncols) {
@@ -1020,10 +1072,10 @@ size_t small_front_smem(int m) {
 
 void launch_factor_small(const FrontDesc* fronts, const ChildLink* links, FrontState* st, const int* list, int count,
                          int max_m, const int* a_colptr, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
-                         cudaStream_t stream) {
+                         cudaStream_t stream, int threads) {
   if (count <= 0) return;
   const size_t sm = small_front_smem(max_m);
-  if (max_m <= 48) {
+  if (threads == 128 || (threads == 0 && max_m <= 48)) {
     factor_small_kernel<128><<<count, 128, sm, stream>>>(fronts, links, st, list, a_colptr, o, g, level, dynamic);
   } else {
     factor_small_kernel<256><<<count, 256, sm, stream>>>(fronts, links, st, list, a_colptr, o, g, level, dynamic);
@@ -1050,6 +1102,24 @@ __global__ void count_unfinished_kernel(const FrontState* __restrict__ st, const
 void launch_count_unfinished(const FrontState* st, const int* list, int count, int* out, cudaStream_t stream) {
   if (count <= 0) return;
   count_unfinished_kernel<<<1, 256, 0, stream>>>(st, list, count, out);
+}
+
+// Graph launches: a level with an unfinished front after its planned
+// iterations marks itself, so the later levels of the graph return at once.
+__global__ void mark_unfinished_kernel(const FrontState* __restrict__ st, const int* __restrict__ list, int count,
+                                       FactorGlobals* g, int level) {
+  if (level_skipped(g, level, 0)) return;
+  int c = 0;
+  for (int t = threadIdx.x; t < count; t += blockDim.x)
+    if (!(st[list[t]].flags & kFlagDone)) ++c;
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicMin(&g->unfinished_level, level);
+}
+
+void launch_mark_unfinished(const FrontState* st, const int* list, int count, FactorGlobals* g, int level,
+                            cudaStream_t stream) {
+  if (count <= 0) return;
+  mark_unfinished_kernel<<<1, 256, 0, stream>>>(st, list, count, g, level);
 }
 
 void launch_update(bool far, const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,

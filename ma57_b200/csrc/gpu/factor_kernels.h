@@ -21,16 +21,19 @@ void launch_assemble(const FrontDesc* fronts, const ChildLink* links, FrontState
                      int dynamic, cudaStream_t stream);
 void launch_factor_small(const FrontDesc* fronts, const ChildLink* links, FrontState* st, const int* list, int count,
                          int max_m, const int* a_colptr, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
-                         cudaStream_t stream);
+                         cudaStream_t stream, int threads = 0);  // threads: 128, 256, or 0 (by front size)
 void launch_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m, int nb,
                   const KernelOpts& o, FactorGlobals* g, int level, int dynamic, cudaStream_t stream);
 // Cluster panel (panel_cluster.cu): returns 0 from cluster_size_for when a
 // front is too large for it (the single-CTA panel kernel then runs).
 int cluster_size_for(int max_m, int count);
+// whether a cluster of cs CTAs (8 or 16) can hold fronts of max_m rows
+bool cluster_size_fits(int max_m, int cs);
 cudaError_t configure_cluster_panel();
+// cs: 8 or 16, or 0 for cluster_size_for's choice
 cudaError_t launch_cluster_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m,
                                  int nb, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
-                                 cudaStream_t stream);
+                                 cudaStream_t stream, int cs = 0);
 // Mixed-precision far update (schur_tc.cu): TF32x3 tcgen05 GEMM fed by TMA.
 size_t tc_far_smem();
 cudaError_t configure_tc_far();
@@ -42,6 +45,10 @@ void launch_tc_far(const FrontDesc* fronts, FrontState* st, const int* list, int
                    const double* guard, int grid, FactorGlobals* g, int level, int dynamic, int* err,
                    cudaStream_t stream);
 
+// graph launches: atomicMin(g->unfinished_level, level) if a front of the
+// list is not finished
+void launch_mark_unfinished(const FrontState* st, const int* list, int count, FactorGlobals* g, int level,
+                            cudaStream_t stream);
 // *out += number of fronts in list not yet finished (flag kFlagDone unset)
 void launch_count_unfinished(const FrontState* st, const int* list, int count, int* out, cudaStream_t stream);
 // near (far = false) / far (far = true) Schur-complement update, FP64. With

@@ -96,7 +96,7 @@ template <int CS>
 __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
                                                             const int* __restrict__ front_list, int nb, int R,
                                                             KernelOpts o, FactorGlobals* g, int level, int dynamic) {
-  if (!dynamic && g->delay_level < level) return;
+  if (level_skipped(g, level, dynamic)) return;
   cg::cluster_group cluster = cg::this_cluster();
   const int q = static_cast<int>(cluster.block_rank());
   const int s = front_list[blockIdx.x / CS];
@@ -798,6 +798,12 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
   cluster.sync();
 }
 
+bool cluster_size_fits(int max_m, int cs) {
+  const size_t limit = 184 * 1024;
+  return (cs == 8 || cs == 16) &&
+         static_cast<size_t>((max_m + cs - 1) / cs) * (kPanelWidth + 4) * sizeof(double) <= limit;
+}
+
 int cluster_size_for(int max_m, int count) {
   const size_t limit = 184 * 1024;  // + the static ClusterShared (~38 KB) <= 227 KB
   const bool fits8 = static_cast<size_t>((max_m + 7) / 8) * (kPanelWidth + 4) * sizeof(double) <= limit;
@@ -825,9 +831,9 @@ cudaError_t configure_cluster_panel() {
 
 cudaError_t launch_cluster_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m,
                                  int nb, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
-                                 cudaStream_t stream) {
+                                 cudaStream_t stream, int cs_choice) {
   if (count <= 0) return cudaSuccess;
-  const int cs = cluster_size_for(max_m, count);
+  const int cs = cluster_size_fits(max_m, cs_choice) ? cs_choice : cluster_size_for(max_m, count);
   const int R = (max_m + cs - 1) / cs;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cs * count);

@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(256) tc_split_kernel(const FrontDesc* __restri
                                                        const int* __restrict__ list, int count,
                                                        float* const* __restrict__ ws, double* guard,
                                                        const FactorGlobals* g, int level, int dynamic) {
-  if (!dynamic && g->delay_level < level) return;
+  if (level_skipped(g, level, dynamic)) return;
   __shared__ float tile[4][kSplitRows][kTcKpad + 1];
   __shared__ double red[8];
   const int fi = blockIdx.y;
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_far_update_kernel(const FrontD
                                                                      const double* __restrict__ guard,
                                                                      FactorGlobals* g, int level, int dynamic,
                                                                      int* err) {
-  if (!dynamic && g->delay_level < level) return;
+  if (level_skipped(g, level, dynamic)) return;
   extern __shared__ __align__(1024) unsigned char tsm_raw[];
   // 1024-byte aligned stage ring (128B swizzle atoms)
   unsigned char* ring =

@@ -1,0 +1,145 @@
+"""Learned first-attempt delta for Mode::StaticRegularized.
+
+The reference's StaticRegularized mode (solver.hpp:328-417) factors with one
+static-pivot delta, checks the inertia against the expected sign pattern and,
+on failure, multiplies delta by a growth factor and factors again. Along an
+interior-point sequence the delta that finally passes drifts with the
+barrier parameter, and every failed attempt costs a full factorization.
+
+`DeltaModel` predicts log10 of the first-attempt delta of every front from
+statistics of that front of the matrix being factorized (diagonal
+magnitudes, expected-sign counts, column norms, sizes), with a small
+multilayer perceptron trained and evaluated on the GPU by the library's own
+kernels (symla_mlp_*). Training targets are the deltas the escalation loop
+itself accepted on earlier matrices of the sequence. The prediction goes in
+as `symla_regularize_opts.front_delta`; when it fails the inertia check the
+plain escalation continues as before, so correctness never depends on the
+model.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib as L
+
+NFEAT = L.MLP_INPUTS
+_TINY = 1e-300
+
+
+def front_features(sym, A_lower, expected_sign=None) -> np.ndarray:
+    """Per-front statistics (one row per supernode of `sym`, a SymbolicFactor):
+    log10 max / min / mean |a_jj| over the front's pivot columns, the fraction
+    of those columns whose expected sign is negative, log10 of the largest
+    column 2-norm, log10 m, log10 of the pivot-column count, and log10
+    max |a_ij| of the whole matrix. A_lower: the stored lower triangle."""
+    A = sp.csc_matrix(A_lower)
+    full = (A + sp.tril(A, -1).T).tocsc()
+    perm = np.asarray(sym.perm)
+    n = A.shape[0]
+    d = np.abs(full.diagonal())[perm]
+    colnorm = np.sqrt(np.asarray(full.multiply(full).sum(axis=0)).ravel())[perm]
+    sign = np.zeros(n) if expected_sign is None else np.asarray(expected_sign, dtype=np.float64)[perm]
+    amax = max(float(np.abs(A.data).max()) if A.nnz else 0.0, _TINY)
+    rows = []
+    for s in sym.supernodes:
+        c0, c1 = s.firstCol, s.firstCol + s.ncols
+        dc = d[c0:c1]
+        rows.append([
+            math.log10(dc.max() + _TINY), math.log10(dc.min() + _TINY), math.log10(dc.mean() + _TINY),
+            float(np.mean(sign[c0:c1] < 0)), math.log10(colnorm[c0:c1].max() + _TINY),
+            math.log10(len(s.rowPattern)), math.log10(s.ncols), math.log10(amax),
+        ])
+    return np.asarray(rows, dtype=np.float64)
+
+
+def init_params(seed: int) -> np.ndarray:
+    """Deterministic uniform (Glorot) initialisation, biases zero."""
+    rng = np.random.default_rng(seed)
+    h, i = L.MLP_HIDDEN, L.MLP_INPUTS
+    W1 = rng.uniform(-1, 1, (h, i)) * math.sqrt(6.0 / (i + h))
+    W2 = rng.uniform(-1, 1, (h, h)) * math.sqrt(6.0 / (2 * h))
+    w3 = rng.uniform(-1, 1, h) * math.sqrt(6.0 / (h + 1))
+    return np.concatenate([W1.ravel(), np.zeros(h), W2.ravel(), np.zeros(h), w3, [0.0]])
+
+
+class Network:
+    """The device-resident network (symla_mlp_*): predict, gradient, train."""
+
+    def __init__(self, params: np.ndarray, device: int = 0):
+        self._lib = L.load()
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        if p.size != L.MLP_PARAMS:
+            raise ValueError(f"expected {L.MLP_PARAMS} parameters, got {p.size}")
+        h = C.c_void_p()
+        rc = self._lib.symla_mlp_create(device, L.ptr_d(p), C.byref(h))
+        if rc != L.SYMLA_OK:
+            raise RuntimeError(L.last_error())
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self._lib.symla_mlp_destroy(self.h)
+            self.h = None
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(L.MLP_PARAMS)
+        self._check(self._lib.symla_mlp_get_params(self.h, L.ptr_d(out)))
+        return out
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        y = np.zeros(X.shape[0])
+        self._check(self._lib.symla_mlp_predict(self.h, L.ptr_d(X), X.shape[0], L.ptr_d(y)))
+        return y
+
+    def gradient(self, X: np.ndarray, T: np.ndarray):
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        g = np.zeros(L.MLP_PARAMS)
+        loss = C.c_double()
+        self._check(self._lib.symla_mlp_gradient(self.h, L.ptr_d(X), L.ptr_d(T), X.shape[0], L.ptr_d(g),
+                                                 C.byref(loss)))
+        return loss.value, g
+
+    def train(self, X: np.ndarray, T: np.ndarray, epochs: int, lr: float, minibatch: int = 0) -> float:
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        loss = C.c_double()
+        self._check(self._lib.symla_mlp_train(self.h, L.ptr_d(X), L.ptr_d(T), X.shape[0], epochs, minibatch, lr,
+                                              C.byref(loss)))
+        return loss.value
+
+    @staticmethod
+    def _check(rc):
+        if rc != L.SYMLA_OK:
+            raise RuntimeError(L.last_error())
+
+
+class DeltaModel:
+    """Standardised front features -> log10 first-attempt delta.
+
+    `margin` (decades) is added to the prediction: an under-predicted delta
+    costs a whole failed factorization, an over-predicted one only a
+    slightly larger perturbation for refinement to remove."""
+
+    def __init__(self, seed: int = 0, device: int = 0, margin: float = 0.5):
+        self.net = Network(init_params(seed), device)
+        self.mean = np.zeros(NFEAT)
+        self.std = np.ones(NFEAT)
+        self.margin = margin
+
+    def fit(self, X: np.ndarray, T: np.ndarray, epochs: int = 400, lr: float = 3e-3, minibatch: int = 4096) -> float:
+        self.mean = X.mean(axis=0)
+        self.std = X.std(axis=0)
+        self.std[self.std < 1e-12] = 1.0
+        return self.net.train((X - self.mean) / self.std, T, epochs, lr, minibatch)
+
+    def predict_log10(self, X: np.ndarray) -> np.ndarray:
+        return self.net.predict((X - self.mean) / self.std)
+
+    def front_deltas(self, X: np.ndarray) -> np.ndarray:
+        return 10.0 ** (self.predict_log10(X) + self.margin)

@@ -189,8 +189,14 @@ class InteriorPointSequence:
     x log-uniform in [1e-8, 1e2] with multiplicative exp(N(0, 0.3)) drift per
     step, mu_k = 10^(-9 k / (steps - 1))."""
 
-    def __init__(self, k: int = 20, steps: int = 500):
+    def __init__(self, k: int = 20, steps: int = 500, curvature_shift: float = 0.0):
+        """curvature_shift c > 0 gives the nonconvex variant E_k = L7 - c I +
+        diag(mu_k / x^2): for small mu_k, E_k has negative curvature, K_k is no
+        longer quasi-definite and StaticRegularized must perturb wrongly signed
+        pivots (c = 0 is the configuration as specified, which is
+        quasi-definite for every k)."""
         self.st = Stream(SEED_BASE + 5)
+        self.shift = curvature_shift
         self.n1 = k ** 3
         self.n2 = self.n1 // 2
         self.steps = steps
@@ -206,7 +212,7 @@ class InteriorPointSequence:
             self.logx = self.logx + 0.3 * self.st.normal(self.n1)
             self.logx = np.clip(self.logx, math.log(1e-8), math.log(1e2))
         x2 = np.exp(2.0 * self.logx)
-        E = self.L + sp.diags(mu / x2)
+        E = self.L + sp.diags(mu / x2 - self.shift)
         F = (mu * 1e-6) * sp.identity(self.n2)
         return kkt(E, F, self.A), mu
 

@@ -262,6 +262,7 @@ class SymLDLT:
         self.last_info = L.FactorInfo()
         self.last_reg_info = L.RegularizeInfo()
         self.front_delta_ = None
+        self.graph_launch_ = False
         self._analysis = None
         self._ctx = None
         self._singular_cols = []
@@ -343,7 +344,21 @@ class SymLDLT:
     def _context(self, cp, ri):
         if self._ctx is None or not self._ctx.same_pattern(cp, ri):
             self._ctx = Context(self._analysis, cp, ri, self.device)
+            L.load().symla_gpu_set_graph(self._ctx.h, int(self.graph_launch_))
         return self._ctx
+
+    # --- B200 extension: graph launch of the factorization (no reference
+    # counterpart; results are those of the ordinary launch path) ---
+    def setGraphLaunch(self, enable: bool):
+        self.graph_launch_ = bool(enable)
+        if self._ctx is not None:
+            L.load().symla_gpu_set_graph(self._ctx.h, int(self.graph_launch_))
+
+    def graphStats(self):
+        cap, res = C.c_int(), C.c_int()
+        if self._ctx is not None:
+            L.load().symla_gpu_graph_stats(self._ctx.h, C.byref(cap), C.byref(res))
+        return {"captures": cap.value, "resumes": res.value}
 
     def factorize(self, A):
         if not self.pattern_analyzed_:

@@ -1,0 +1,84 @@
+"""Graph launch of the factorization, the batched solver over many
+independent systems (config 4's shape, fewer systems), and the measured
+tile schedule: none of them may change a result."""
+import numpy as np
+import pytest
+
+from ma57_b200 import OrderingType, SymLDLT, autotune
+from ma57_b200 import matrices as M
+from ma57_b200.batch import BatchedSolver
+
+pytestmark = pytest.mark.gpu
+
+
+def backward_error(A, X, B):
+    Af = M.sym_full(A)
+    R = B - Af @ X
+    normA = abs(A).sum(axis=1).max()
+    return np.abs(R).max() / (normA * np.abs(X).max() + np.abs(B).max())
+
+
+@pytest.mark.parametrize("k", [12, 20])
+def test_graph_launch_matches_stream_launch_bitwise(k):
+    A, b = M.config1(k)
+    xs = []
+    for graph in (False, True):
+        s = SymLDLT()
+        s.setGraphLaunch(graph)
+        s.analyzePattern(A)
+        s.factorize(A)
+        s.refactorize(A)  # second factorization replays the captured graph
+        xs.append((s.inertia().as_tuple(), s.solve(b), s.graphStats()))
+    assert xs[0][0] == xs[1][0]
+    np.testing.assert_array_equal(xs[0][1], xs[1][1])
+    assert xs[1][2]["captures"] == 1
+    assert xs[0][2]["captures"] == 0
+
+
+def test_graph_launch_with_delayed_pivots_continues_on_host():
+    K, b, n1, n2 = M.config2(grid=30, n2=300)
+    ref = SymLDLT()
+    ref.analyzePattern(K)
+    ref.factorize(K)
+    s = SymLDLT()
+    s.setGraphLaunch(True)
+    s.analyzePattern(K)
+    s.factorize(K)
+    s.refactorize(K)
+    assert s.inertia().as_tuple() == ref.inertia().as_tuple() == (n2, n1, 0)
+    np.testing.assert_array_equal(s.solve(b), ref.solve(b))
+
+
+def test_batched_systems_match_individual_solves():
+    systems = [M.config4_system(i) for i in range(24)]
+    mats = [A for A, _, _, _ in systems]
+    rng = np.random.default_rng(9)
+    Bs = [rng.standard_normal((A.shape[0], 8)) for A in mats]
+    bs = BatchedSolver(mats)
+    bs.factorize()
+    bs.factorize()
+    Xs = bs.solve(Bs)
+    assert bs.solver.graphStats()["captures"] == 1
+    for A, B, X in zip(mats, Bs, Xs):
+        s = SymLDLT()
+        s.analyzePattern(A)
+        s.factorize(A)
+        Xi = s.solve(B)
+        assert backward_error(A, X, B) <= 1e-12
+        assert np.abs(X - Xi).max() <= 1e-10 * max(1.0, np.abs(Xi).max())
+
+
+def test_autotuned_schedule_keeps_results():
+    A, B = M.config3(20, nrhs=2)
+    s = SymLDLT()
+    s.setOrdering(OrderingType.Metis)
+    s.analyzePattern(A)
+    s.factorize(A)
+    inertia, X0 = s.inertia().as_tuple(), s.solve(B)
+    schedule, base, best = autotune.tune(s, A, reps=1)
+    assert best <= base
+    s.factorize(A)
+    assert s.inertia().as_tuple() == inertia
+    assert backward_error(A, s.solve(B), B) <= 10 * max(backward_error(A, X0, B), 1e-16)
+    info = autotune.level_info(s)
+    assert any(i["small_threads"] or i["cluster_ctas"] for i in info) or schedule == {"small": {}, "large": {}}
