@@ -228,7 +228,9 @@ int symla_gpu_phase_ms(symla_gpu_ctx* ctx, float* ms, int cap);
 /* Kernel instrumentation. When enabled, every launch of the library's
  * kernels is bracketed by CUDA events on the context's stream; per kernel
  * kind the launch count, summed device time and algorithmic work are kept
- * until reset. Kinds: 0 far (deferred, outer-block) Schur-complement update,
+ * until reset. Kinds: 0 far (deferred, outer-block) Schur-complement update
+ * (with FP64 precision the near updates run in the same launch and count
+ * here),
  * 1 panel factorization, 2 small-front kernel, 3 assembly, 4 forward solve,
  * 5 backward solve, 6 residual, 7 near (in-block) Schur-complement update.
  * out[0] launches, out[1] total ms, out[2] algorithmic flops, out[3]

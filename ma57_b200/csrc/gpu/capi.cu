@@ -693,6 +693,14 @@ void launch_panel_iteration(symla_gpu_ctx* c, const LevelLists& L, int level, co
                    st);
     }
   });
+  if (ko.precision != SYMLA_PREC_MIXED) {
+    // FP64: near and far updates in one launch (disjoint column ranges);
+    // timed as the far (Schur-complement) kind
+    timed(c, SYMLA_KERNEL_TRAILING, 0.0, 0.0, [&] {
+      launch_update_both(c->d_desc, c->d_state, d_large, nl, L.trailing_grid, c->d_glob, level, dynamic, st);
+    });
+    return;
+  }
   timed(c, SYMLA_KERNEL_NEAR, 0.0, 0.0, [&] {
     launch_update(false, c->d_desc, c->d_state, d_large, nl, L.trailing_grid, c->d_glob, level, dynamic, st);
   });
@@ -995,8 +1003,12 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
   if (c->profiling) {
     FactorGlobals gf;
     CK(cudaMemcpy(&gf, c->d_glob, sizeof gf, cudaMemcpyDeviceToHost));
-    c->kstat[SYMLA_KERNEL_TRAILING].flops += gf.flops_far;
-    c->kstat[SYMLA_KERNEL_NEAR].flops += gf.flops_near;
+    if (o->precision == SYMLA_PREC_MIXED) {
+      c->kstat[SYMLA_KERNEL_TRAILING].flops += gf.flops_far;
+      c->kstat[SYMLA_KERNEL_NEAR].flops += gf.flops_near;
+    } else {  // one launch does both (timed as the far kind)
+      c->kstat[SYMLA_KERNEL_TRAILING].flops += gf.flops_far + gf.flops_near;
+    }
   }
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));

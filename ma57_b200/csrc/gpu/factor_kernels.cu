@@ -913,7 +913,9 @@ __device__ __forceinline__ int update_tiles(int m, int c0, int c1) {
   return n;
 }
 
-template <bool FAR>
+// MODE 0: near updates, 1: far updates, 2: both in one tile space (their
+// column ranges are disjoint and read only finished L columns).
+template <int MODE>
 __global__ void __launch_bounds__(kTThreads) update_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
                                                            const int* __restrict__ front_list, int count,
                                                            FactorGlobals* g, int level, int dynamic,
@@ -927,28 +929,32 @@ __global__ void __launch_bounds__(kTThreads) update_kernel(const FrontDesc* __re
   double* Wj = usm + (4 * kKC + 4) * kTT;
   __shared__ double dd[kKC], dlo[kKC], dhi[kKC];
   __shared__ int8_t kk[kKC];
-  __shared__ int tile_end[kMaxUpdateFronts];
-  // one tile space over every front of the launch, so idle fronts do not
-  // leave CTAs without work
-  for (int t = threadIdx.x; t < count; t += kTThreads) {
-    const int sf = front_list[t];
+  __shared__ int tile_end[2 * kMaxUpdateFronts];
+  // one tile space over every front (and, in MODE 2, both ranges) of the
+  // launch, so idle fronts do not leave CTAs without work; entry e is front
+  // e % count, its far range when e >= count in MODE 2
+  const int nent = (MODE == 2) ? 2 * count : count;
+  auto entry_far = [&](int e) { return MODE == 1 || (MODE == 2 && e >= count); };
+  for (int t = threadIdx.x; t < nent; t += kTThreads) {
+    const int sf = front_list[t % count];
+    const bool far = entry_far(t);
     int c0, c1, q0, q1;
     const FrontState S = st[sf];
-    bool use = update_range(S, fronts[sf].m, FAR, c0, c1, q0, q1);
-    if (FAR && use && tc_guard && tc_block_ok(q1 - q0, tc_guard[2 * t], tc_guard[2 * t + 1], g->amax))
+    bool use = update_range(S, fronts[sf].m, far, c0, c1, q0, q1);
+    if (far && use && tc_guard && tc_block_ok(q1 - q0, tc_guard[2 * t], tc_guard[2 * t + 1], g->amax))
       use = false;  // the tensor-core kernel applied this block
     tile_end[t] = use ? update_tiles(fronts[sf].m, c0, c1) : 0;
     if (blockIdx.x == 0 && tile_end[t] > 0) {
       const double nc = c1 - c0, mm = fronts[sf].m;
       const double entries = nc * mm - (static_cast<double>(c0) + c1 - 1) * nc / 2.0;
-      atomicAdd(FAR ? &g->flops_far : &g->flops_near, 2.0 * (q1 - q0) * entries);
+      atomicAdd(far ? &g->flops_far : &g->flops_near, 2.0 * (q1 - q0) * entries);
     }
   }
   __syncthreads();
   if (threadIdx.x == 0)
-    for (int t = 1; t < count; ++t) tile_end[t] += tile_end[t - 1];
+    for (int t = 1; t < nent; ++t) tile_end[t] += tile_end[t - 1];
   __syncthreads();
-  const int total = count > 0 ? tile_end[count - 1] : 0;
+  const int total = nent > 0 ? tile_end[nent - 1] : 0;
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
   double tmax = 0.0;
   int cur = -1, s = -1;
@@ -965,11 +971,11 @@ __global__ void __launch_bounds__(kTThreads) update_kernel(const FrontDesc* __re
         tmax = 0.0;
       }
       cur = fi;
-      s = front_list[fi];
+      s = front_list[fi % count];
       f = fronts[s];
       m = f.m;
       ld = f.ld;
-      update_range(st[s], m, FAR, c0, c1, q0, q1);
+      update_range(st[s], m, entry_far(fi), c0, c1, q0, q1);
       nchunks = (q1 - q0 + kKC - 1) / kKC;
     }
     int rem = tile - (fi > 0 ? tile_end[fi - 1] : 0);
@@ -1057,6 +1063,202 @@ __global__ void __launch_bounds__(kTThreads) update_kernel(const FrontDesc* __re
 }
 
 // ---------------------------------------------------------------------------
+// The same near / far updates on the FP64 tensor path: mma.sync m8n8k4 .f64
+// (DMMA; the 5th-gen tcgen05 MMA has no FP64 kind). 128 x 128 tiles, 8 warps
+// of 64 x 32 (8 x 4 MMA tiles, 2 accumulators each per lane). A chunk of 32
+// pivots of the A rows (L(i, q)) and of the B rows (L(j, q) with one halo
+// column each side, for D's 2 x 2 blocks) is staged row-major with a 36-double
+// row stride (conflict-free fragment loads), double-buffered by cp.async;
+// W(j, q) = (L D)(j, q) is formed once per chunk in shared memory; the
+// negated L fragment accumulates onto the C tile held in registers.
+namespace {
+constexpr int kMS = 36;  // row stride of the staged tiles (doubles)
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// A rows i (pivots kc .. kc + kn) and B rows j (pivots kc - 1 .. kc + kn,
+// valid inside [q0, q1)) into row-major tiles, zero-filled outside.
+__device__ __forceinline__ void mma_stage(const FrontDesc& f, int q0, int q1, int kc, int kn, int i0, int j0,
+                                          double* As, double* Bs) {
+  const int64_t ld = f.ld;
+  const int m = f.m;
+  for (int t = threadIdx.x; t < kKC * kTT; t += kTThreads) {
+    const int k = t / kTT, r = t % kTT;
+    const int gi = i0 + r;
+    const bool ok = k < kn && gi < m;
+    cp_async8(As + r * kMS + k, f.F + (ok ? (kc + k) * ld + gi : 0), ok);
+  }
+  for (int t = threadIdx.x; t < (kKC + 2) * kTT; t += kTThreads) {
+    const int kp = t / kTT, r = t % kTT;
+    const int pq = kc + kp - 1;
+    const int gj = j0 + r;
+    const bool ok = gj < m && pq >= q0 && pq < q1 && kp <= kn + 1;  // halo: 2 x 2 partners either side
+    cp_async8(Bs + r * kMS + kp, f.F + (ok ? pq * ld + gj : 0), ok);
+  }
+}
+}  // namespace
+
+template <int MODE>
+__global__ void __launch_bounds__(kTThreads, 1) update_mma_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
+                                                               const int* __restrict__ front_list, int count,
+                                                               FactorGlobals* g, int level, int dynamic,
+                                                               const double* __restrict__ tc_guard) {
+  if (level_aborted(g, level, dynamic)) return;
+  extern __shared__ double usm[];
+  double* AsBuf[2] = {usm, usm + kTT * kMS};
+  double* BsBuf[2] = {usm + 2 * kTT * kMS, usm + 3 * kTT * kMS};
+  double* Ws = usm + 4 * kTT * kMS;
+  __shared__ double dd[kKC], dlo[kKC], dhi[kKC];
+  __shared__ int8_t kk[kKC];
+  __shared__ int tile_end[2 * kMaxUpdateFronts];
+  const int nent = (MODE == 2) ? 2 * count : count;
+  auto entry_far = [&](int e) { return MODE == 1 || (MODE == 2 && e >= count); };
+  for (int t = threadIdx.x; t < nent; t += kTThreads) {
+    const int sf = front_list[t % count];
+    const bool far = entry_far(t);
+    int c0, c1, q0, q1;
+    const FrontState S = st[sf];
+    bool use = update_range(S, fronts[sf].m, far, c0, c1, q0, q1);
+    if (far && use && tc_guard && tc_block_ok(q1 - q0, tc_guard[2 * t], tc_guard[2 * t + 1], g->amax))
+      use = false;  // the tensor-core kernel applied this block
+    tile_end[t] = use ? update_tiles(fronts[sf].m, c0, c1) : 0;
+    if (blockIdx.x == 0 && tile_end[t] > 0) {
+      const double nc = c1 - c0, mm = fronts[sf].m;
+      const double entries = nc * mm - (static_cast<double>(c0) + c1 - 1) * nc / 2.0;
+      atomicAdd(far ? &g->flops_far : &g->flops_near, 2.0 * (q1 - q0) * entries);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int t = 1; t < nent; ++t) tile_end[t] += tile_end[t - 1];
+  __syncthreads();
+  const int total = nent > 0 ? tile_end[nent - 1] : 0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wr = warp >> 2, wc = warp & 3;          // warp's 64 x 32 sub-tile
+  const int lr = lane >> 2, lk = lane & 3;          // fragment coordinates
+  double tmax = 0.0;
+  int cur = -1, s = -1;
+  FrontDesc f;
+  int m = 0, c0 = 0, c1 = 0, q0 = 0, q1 = 0, nchunks = 0;
+  int64_t ld = 0;
+  for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
+    int fi = 0;
+    while (tile >= tile_end[fi]) ++fi;
+    if (fi != cur) {
+      if (cur >= 0) {
+        tmax = warp_max(tmax);
+        if (lane == 0) atomic_max_nonneg(&st[s].running_max, tmax);
+        tmax = 0.0;
+      }
+      cur = fi;
+      s = front_list[fi % count];
+      f = fronts[s];
+      m = f.m;
+      ld = f.ld;
+      update_range(st[s], m, entry_far(fi), c0, c1, q0, q1);
+      nchunks = (q1 - q0 + kKC - 1) / kKC;
+    }
+    int rem = tile - (fi > 0 ? tile_end[fi - 1] : 0);
+    int tj = 0;
+    for (;;) {
+      const int nr = (m - (c0 + tj * kTT) + kTT - 1) / kTT;
+      if (rem < nr) break;
+      rem -= nr;
+      ++tj;
+    }
+    const int j0 = c0 + tj * kTT, i0 = j0 + rem * kTT;
+    __syncthreads();  // previous tile done with the buffers
+    mma_stage(f, q0, q1, q0, min(kKC, q1 - q0), i0, j0, AsBuf[0], BsBuf[0]);
+    cp_async_commit();
+    // C tile into the accumulators (lane holds rows gi0 + 8 rt, columns
+    // gj0 + 8 ct + e)
+    const int gi0 = i0 + wr * 64 + lr, gj0 = j0 + wc * 32 + 2 * lk;
+    double acc[8][4][2];
+#pragma unroll
+    for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int gj = gj0 + ct * 8 + e;
+        const double* colp = f.F + static_cast<int64_t>(gj < c1 ? gj : 0) * ld;
+#pragma unroll
+        for (int rt = 0; rt < 8; ++rt) {
+          const int gi = gi0 + rt * 8;
+          acc[rt][ct][e] = (gj < c1 && gi < m && gi >= gj) ? colp[gi] : 0.0;
+        }
+      }
+    for (int c = 0; c < nchunks; ++c) {
+      const int kc = q0 + c * kKC, kn = min(kKC, q1 - kc);
+      if (c + 1 < nchunks) {
+        const int kc2 = kc + kKC;
+        mma_stage(f, q0, q1, kc2, min(kKC, q1 - kc2), i0, j0, AsBuf[(c + 1) & 1], BsBuf[(c + 1) & 1]);
+      }
+      cp_async_commit();
+      if (threadIdx.x < kn) {
+        const int pq = kc + threadIdx.x;
+        const int8_t kind = f.pk[pq];
+        kk[threadIdx.x] = kind;
+        dd[threadIdx.x] = f.Dd[pq];
+        dlo[threadIdx.x] = (kind == 2) ? f.Do[pq - 1] : 0.0;
+        dhi[threadIdx.x] = (kind == 1) ? f.Do[pq] : 0.0;
+      }
+      cp_async_wait<1>();
+      __syncthreads();
+      const double* As = AsBuf[c & 1];
+      const double* Bs = BsBuf[c & 1];
+      // W(j, q) = (L D)(j, q); zero past the chunk (the MMAs run over 4-pivot steps)
+      const int kn4 = (kn + 3) & ~3;
+      for (int t = threadIdx.x; t < kn4 * kTT; t += kTThreads) {
+        const int q = t / kTT, r = t % kTT;
+        double w = 0.0;
+        if (q < kn) {
+          const double* row = Bs + r * kMS + q + 1;
+          w = dd[q] * row[0];
+          if (kk[q] == 1) w += dhi[q] * row[1];
+          if (kk[q] == 2) w += dlo[q] * row[-1];
+        }
+        Ws[r * kMS + q] = w;
+      }
+      __syncthreads();
+      for (int k0 = 0; k0 < kn4; k0 += 4) {
+        double a[8], b[4];
+#pragma unroll
+        for (int rt = 0; rt < 8; ++rt) a[rt] = -As[(wr * 64 + rt * 8 + lr) * kMS + k0 + lk];
+#pragma unroll
+        for (int ct = 0; ct < 4; ++ct) b[ct] = Ws[(wc * 32 + ct * 8 + lr) * kMS + k0 + lk];
+#pragma unroll
+        for (int rt = 0; rt < 8; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 4; ++ct) dmma(acc[rt][ct][0], acc[rt][ct][1], a[rt], b[ct]);
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int gj = gj0 + ct * 8 + e;
+        double* colp = f.F + static_cast<int64_t>(gj < c1 ? gj : 0) * ld;
+#pragma unroll
+        for (int rt = 0; rt < 8; ++rt) {
+          const int gi = gi0 + rt * 8;
+          if (gj < c1 && gi < m && gi >= gj) {
+            colp[gi] = acc[rt][ct][e];
+            tmax = fmax(tmax, fabs(acc[rt][ct][e]));
+          }
+        }
+      }
+  }
+  if (cur >= 0) {
+    tmax = warp_max(tmax);
+    if (lane == 0) atomic_max_nonneg(&st[s].running_max, tmax);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Host launchers
 
 void launch_assemble(const FrontDesc* fronts, const ChildLink* links, FrontState* st, const int* tasks,
@@ -1125,14 +1327,25 @@ void launch_mark_unfinished(const FrontState* st, const int* list, int count, Fa
 void launch_update(bool far, const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
                    FactorGlobals* g, int level, int dynamic, cudaStream_t stream, const double* tc_guard) {
   if (count <= 0 || grid_x <= 0) return;
-  const size_t sm = static_cast<size_t>(5 * kKC + 4) * kTT * sizeof(double);
+  const size_t sm = static_cast<size_t>(5) * kTT * kMS * sizeof(double);
   for (int b = 0; b < count; b += kMaxUpdateFronts) {
     const int cnt = count - b < kMaxUpdateFronts ? count - b : kMaxUpdateFronts;
     if (far)
-      update_kernel<true><<<grid_x, kTThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic,
-                                                             tc_guard ? tc_guard + 2 * b : nullptr);
+      update_mma_kernel<1><<<grid_x, kTThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic,
+                                                              tc_guard ? tc_guard + 2 * b : nullptr);
     else
-      update_kernel<false><<<grid_x, kTThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic, nullptr);
+      update_mma_kernel<0><<<grid_x, kTThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic,
+                                                              nullptr);
+  }
+}
+
+void launch_update_both(const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
+                        FactorGlobals* g, int level, int dynamic, cudaStream_t stream) {
+  if (count <= 0 || grid_x <= 0) return;
+  const size_t sm = static_cast<size_t>(5) * kTT * kMS * sizeof(double);
+  for (int b = 0; b < count; b += kMaxUpdateFronts) {
+    const int cnt = count - b < kMaxUpdateFronts ? count - b : kMaxUpdateFronts;
+    update_mma_kernel<2><<<grid_x, kTThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic, nullptr);
   }
 }
 
@@ -1144,9 +1357,16 @@ cudaError_t configure_factor_kernels() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  e = cudaFuncSetAttribute(update_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(update_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  e = cudaFuncSetAttribute(update_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(update_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (e != cudaSuccess) return e;
+  for (auto fn : {update_mma_kernel<0>, update_mma_kernel<1>, update_mma_kernel<2>}) {
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 5 * kTT * kMS * sizeof(double));
+    if (e != cudaSuccess) return e;
+  }
   return e;
 }
 

@@ -56,6 +56,9 @@ void launch_count_unfinished(const FrontState* st, const int* list, int count, i
 // applies just the blocks that tc_block_ok sends away from the tensor cores.
 void launch_update(bool far, const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
                    FactorGlobals* g, int level, int dynamic, cudaStream_t stream, const double* tc_guard = nullptr);
+// near and far updates of every front in one launch (FP64 path)
+void launch_update_both(const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
+                        FactorGlobals* g, int level, int dynamic, cudaStream_t stream);
 
 // Solve
 void launch_permute_in(int n, int nrhs, const int* perm, const double* B, int ldb, double* Bp, cudaStream_t stream);

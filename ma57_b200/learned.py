@@ -34,8 +34,9 @@ def front_features(sym, A_lower, expected_sign=None) -> np.ndarray:
     """Per-front statistics (one row per supernode of `sym`, a SymbolicFactor):
     log10 max / min / mean |a_jj| over the front's pivot columns, the fraction
     of those columns whose expected sign is negative, log10 of the largest
-    column 2-norm, log10 m, log10 of the pivot-column count, and log10
-    max |a_ij| of the whole matrix. A_lower: the stored lower triangle."""
+    column 2-norm, log10 m, and two statistics of the whole matrix (log10 of
+    the median |a_jj| and of max |a_ij|), which carry the scale the sequence
+    is at. A_lower: the stored lower triangle."""
     A = sp.csc_matrix(A_lower)
     full = (A + sp.tril(A, -1).T).tocsc()
     perm = np.asarray(sym.perm)
@@ -44,6 +45,7 @@ def front_features(sym, A_lower, expected_sign=None) -> np.ndarray:
     colnorm = np.sqrt(np.asarray(full.multiply(full).sum(axis=0)).ravel())[perm]
     sign = np.zeros(n) if expected_sign is None else np.asarray(expected_sign, dtype=np.float64)[perm]
     amax = max(float(np.abs(A.data).max()) if A.nnz else 0.0, _TINY)
+    dmed = math.log10(float(np.median(d)) + _TINY)
     rows = []
     for s in sym.supernodes:
         c0, c1 = s.firstCol, s.firstCol + s.ncols
@@ -51,7 +53,7 @@ def front_features(sym, A_lower, expected_sign=None) -> np.ndarray:
         rows.append([
             math.log10(dc.max() + _TINY), math.log10(dc.min() + _TINY), math.log10(dc.mean() + _TINY),
             float(np.mean(sign[c0:c1] < 0)), math.log10(colnorm[c0:c1].max() + _TINY),
-            math.log10(len(s.rowPattern)), math.log10(s.ncols), math.log10(amax),
+            math.log10(len(s.rowPattern)), dmed, math.log10(amax),
         ])
     return np.asarray(rows, dtype=np.float64)
 
@@ -122,24 +124,61 @@ class Network:
 class DeltaModel:
     """Standardised front features -> log10 first-attempt delta.
 
-    `margin` (decades) is added to the prediction: an under-predicted delta
-    costs a whole failed factorization, an over-predicted one only a
-    slightly larger perturbation for refinement to remove."""
+    A front's delta is its prediction, but never below the median prediction
+    over the matrix's fronts, plus a margin in decades: an under-predicted
+    delta costs a whole failed factorization, an over-predicted one only a
+    larger perturbation for refinement to remove. `fit` chooses the margin
+    as the smallest that would have covered `coverage` of the training
+    matrices (their median prediction plus margin at or above the delta
+    escalation accepted), unless a margin is given."""
 
-    def __init__(self, seed: int = 0, device: int = 0, margin: float = 0.5):
+    def __init__(self, seed: int = 0, device: int = 0, margin: float | None = None, coverage: float = 0.9):
         self.net = Network(init_params(seed), device)
         self.mean = np.zeros(NFEAT)
         self.std = np.ones(NFEAT)
         self.margin = margin
+        self.coverage = coverage
 
-    def fit(self, X: np.ndarray, T: np.ndarray, epochs: int = 400, lr: float = 3e-3, minibatch: int = 4096) -> float:
+    def fit(self, X: np.ndarray, T: np.ndarray, groups=None, epochs: int = 400, lr: float = 3e-3,
+            minibatch: int = 4096) -> float:
+        """X: front features, T: log10 accepted delta of each front's matrix,
+        groups: the matrix index of each row (for the margin)."""
         self.mean = X.mean(axis=0)
         self.std = X.std(axis=0)
         self.std[self.std < 1e-12] = 1.0
-        return self.net.train((X - self.mean) / self.std, T, epochs, lr, minibatch)
+        loss = self.net.train((X - self.mean) / self.std, T, epochs, lr, minibatch)
+        if self.margin is None:
+            if groups is None:
+                self.margin = 0.5
+            else:
+                pred = self.predict_log10(X)
+                groups = np.asarray(groups)
+                short = [float(T[groups == g][0] - np.median(pred[groups == g])) for g in np.unique(groups)]
+                self.margin = max(0.0, float(np.quantile(short, self.coverage)))
+        return loss
+
+    def update(self, X: np.ndarray, T: np.ndarray, window: int = 20, epochs: int = 20, lr: float = 1e-3,
+               minibatch: int = 4096) -> float:
+        """Online step along a sequence: add one matrix's fronts with the
+        delta escalation accepted for it, fine-tune on the last `window`
+        matrices (same standardisation) and refit the margin on them."""
+        self._buf = getattr(self, "_buf", [])
+        self._buf.append((np.asarray(X, dtype=np.float64), np.asarray(T, dtype=np.float64)))
+        self._buf = self._buf[-window:]
+        Xb = np.vstack([x for x, _ in self._buf])
+        Tb = np.concatenate([t for _, t in self._buf])
+        loss = self.net.train((Xb - self.mean) / self.std, Tb, epochs, lr, minibatch)
+        pred = self.predict_log10(Xb)
+        short, off = [], 0
+        for x, t in self._buf:
+            short.append(float(t[0] - np.median(pred[off:off + len(t)])))
+            off += len(t)
+        self.margin = max(0.0, float(np.quantile(short, self.coverage)))
+        return loss
 
     def predict_log10(self, X: np.ndarray) -> np.ndarray:
         return self.net.predict((X - self.mean) / self.std)
 
     def front_deltas(self, X: np.ndarray) -> np.ndarray:
-        return 10.0 ** (self.predict_log10(X) + self.margin)
+        p = self.predict_log10(X)
+        return 10.0 ** (np.maximum(p, np.median(p)) + (self.margin or 0.0))

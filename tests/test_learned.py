@@ -88,8 +88,9 @@ def test_learned_delta_cuts_retries_on_nonconvex_sequence():
     first attempt for the next 30."""
     seq = M.InteriorPointSequence(k=10, steps=60, curvature_shift=6.0)
     _, _, feats, targets = _run(seq, range(0, 30))
-    model = learned.DeltaModel(seed=3, margin=0.5)
-    model.fit(np.vstack(feats), np.concatenate(targets), epochs=300, lr=3e-3, minibatch=2048)
+    model = learned.DeltaModel(seed=3)
+    groups = np.concatenate([np.full(len(t), i) for i, t in enumerate(targets)])
+    model.fit(np.vstack(feats), np.concatenate(targets), groups, epochs=300, lr=3e-3, minibatch=2048)
     state = (seq.logx.copy(), seq.st.pos)
     plain, plain_res, _, _ = _run(seq, range(30, 60))
     seq.logx, seq.st.pos = state
