@@ -313,8 +313,8 @@ def run_learned(args):
     accepted deltas train the network on the GPU; the remaining matrices are
     then run twice from the same state of the sequence, with plain
     escalation and with the network's first-attempt deltas (the network
-    fine-tuned after every matrix on the deltas accepted for the last 20,
-    its training time included). Reported: mean retries and total time
+    fine-tuned, after every matrix whose first attempt failed, on the deltas
+    accepted for the last 20, its training time included). Reported: mean retries and total time
     (factorize + refinement towards 1e-10)."""
     import math
     import numpy as np
@@ -338,13 +338,14 @@ def run_learned(args):
                 sym = s.symbolicFactor()
             F = learned.front_features(sym, K, signs)
             t0 = time.perf_counter()
-            s.setInitialRegularizationDelta(1e-14 * abs(K.data).max())
-            s.setFrontDeltas(None if model is None else model.front_deltas(F))
+            base = 1e-14 * abs(K.data).max()
+            s.setInitialRegularizationDelta(base)
+            s.setFrontDeltas(None if model is None else model.front_deltas(F, base))
             s.factorize(K)
             r = s.solveWithRefinement(K, seq.b, RefinementOptions(max_iterations=30, tolerance=1e-10))
-            T = np.full(F.shape[0], math.log10(s.lastRegularizationDelta()))
-            if online:
-                model.update(F, T)  # the sequence's own retry history keeps the model current
+            T = np.full(F.shape[0], math.log10(s.lastRegularizationDelta() / base))
+            if online:  # the sequence's own retry history keeps the model current
+                model.update(F, T, retries=s.regularizationRetriesUsed())
             out["ms"].append(1e3 * (time.perf_counter() - t0))
             out["retries"].append(s.regularizationRetriesUsed())
             out["resid"].append(r.diagnostics.final_relative_residual)
@@ -550,7 +551,8 @@ def run_ours(args):
                    "l2": "inputs larger than L2 (fronts 11 GB)", "inertia": [info.n_pos, info.n_neg, info.n_zero],
                    "backward_error": bw, "refine_iterations": rinfo.iterations,
                    "analyze_s": t_analyze, "factor_flops": stats.get("factor_flops"),
-                   "kernel_ms_per_step": {k: v[1] / max(1, args.steps) for k, v in kstats.items()}},
+                   "kernel_ms_per_step": {k: v[1] / max(1, args.steps) for k, v in kstats.items()},
+                   "panels": {k: v for k, v in stats.items() if k.startswith("panels_")}},
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(8 * (2 * len(vals) + n * nrhs)),
                 "d2h_bytes_per_step": int(8 * n * nrhs)},
         "gpu_launches": launches,

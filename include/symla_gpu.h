@@ -167,7 +167,9 @@ typedef struct {
   const int* expected_sign;     /* original index space, or NULL */
   int kkt_n1, kkt_n2;           /* used when expected_sign is NULL and kkt_n1 >= 0 */
   int precision;
-  const double* front_delta;    /* optional per-supernode first-attempt deltas (learned) */
+  const double* front_delta;    /* optional per-supernode first-attempt deltas (learned); when
+                                   that attempt fails, the escalation resumes one growth step
+                                   above max(initial delta, smallest front delta) */
 } symla_regularize_opts;
 
 void symla_regularize_opts_default(symla_regularize_opts* o);
@@ -276,10 +278,11 @@ int symla_gpu_plan_stats(symla_gpu_ctx* ctx, double* out, int cap);
 /* Learned first-attempt delta for Mode::StaticRegularized (no reference
  * counterpart; the reference starts every factorization's escalation from
  * the same delta, solver.hpp:328-417). A multilayer perceptron maps
- * SYMLA_MLP_INPUTS standardised per-front statistics to log10 of the
- * front's first-attempt delta (symla_regularize_opts.front_delta), trained
- * on the GPU from the deltas the escalation loop itself accepted; on an
- * inertia failure the plain escalation runs as before. FP64; parameters in
+ * SYMLA_MLP_INPUTS standardised per-front statistics to the front's
+ * first-attempt delta in decades above the plain first attempt
+ * (symla_regularize_opts.front_delta), trained on the GPU from the deltas
+ * the escalation loop itself accepted; on an inertia failure the plain
+ * escalation resumes above the failed attempt. FP64; parameters in
  * the order W1 (H x IN, row-major), b1 (H), W2 (H x H), b2 (H), w3 (H), b3. */
 #define SYMLA_MLP_INPUTS 8
 #define SYMLA_MLP_HIDDEN 32

@@ -1498,6 +1498,13 @@ extern "C" int symla_gpu_factorize_regularized(symla_gpu_ctx* c, const double* v
                delta);
       return set_error(SYMLA_ERR_RETRY_EXHAUSTED, buf);
     }
+    if (attempt == 0 && ro->front_delta && c->numSN > 0) {
+      // every front had at least its smallest per-front delta and the
+      // inertia still failed: no uniform delta below that is worth a pass
+      double dmin = ro->front_delta[0];
+      for (int s = 1; s < c->numSN; ++s) dmin = std::min(dmin, ro->front_delta[s]);
+      delta = std::max(delta, dmin);
+    }
     delta *= ro->growth;
   }
   return SYMLA_OK;

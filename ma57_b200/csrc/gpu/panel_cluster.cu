@@ -48,6 +48,7 @@ constexpr int kCT = 256;                           // threads per CTA
 constexpr int kNBMax = 34;                         // panel width + 2
 constexpr int kSpecMax = 32;                       // pivots per speculative panel (= panel width)
 constexpr int kSpecRetry = 2;                      // consecutive failures before a whole sequential panel
+constexpr int kSeqFinish = 12;                     // pivots left that the sequential path finishes in-launch
 
 struct ClusterShared {
   double w[kNBMax];     // D * L(k, :)^T for the current pivot row
@@ -264,6 +265,7 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
   int spec = S.spec;
   int seq_limit = 1 << 30;  // sequential decisions allowed in this panel
   bool run_seq = true;
+  int spec_kind = 0;  // 0 no speculation, 1 all accepted, 2 a prefix, 3 none
   const int np = pe - ps;
   if (np > 0 && spec < kSpecRetry) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -341,39 +343,40 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
       sh.rmd[c] = rv;
     }
     // rows below the block, left-looking: the raw panel columns of this
-    // CTA's rows are staged in Lr, then each thread walks its rows pivot by
-    // pivot (two rows interleaved), touching only its own rows, so no
-    // synchronisation is needed between pivots. Lr receives the current
-    // values a_ic = raw_ic - sum_t a_it L_ct (L = a_ic / d_c on write-back).
+    // CTA's rows are staged in Lr, then each thread takes one row at a time
+    // into registers and walks it pivot by pivot, touching only its own
+    // rows, so no synchronisation is needed between pivots; the L(c, t) are
+    // warp-uniform (broadcast) shared loads. Lr receives the current values
+    // a_ic = raw_ic - sum_t a_it L_ct (L = a_ic / d_c on write-back). Columns
+    // past np compute unused values (column c depends on columns t < c only).
     for (int c = 0; c < np; ++c)
       for (int i = r0 + threadIdx.x; i < rend; i += kCT)
         cp_async8(Lr + c * R + (i - base), F + static_cast<int64_t>(ps + c) * ld + i);
     cp_async_wait_all();
     __syncthreads();
-    for (int i0 = r0 + threadIdx.x; i0 < rend; i0 += 2 * kCT) {
-      const int i1 = i0 + kCT;
-      const bool two = i1 < rend;
-      const int l0 = i0 - base, l1 = two ? i1 - base : l0;
-      for (int c = 0; c < np; ++c) {
-        // sum_t L_it d_t L_ct = sum_t a_it L_ct (a_it = L_it d_t), two
-        // partial sums per row
-        double a0 = 0.0, b0 = 0.0, a1 = 0.0, b1 = 0.0;
-        int t = 0;
-        for (; t + 2 <= c; t += 2) {
-          const double x = sh.db[c][t], y = sh.db[c][t + 1];
-          a0 = fma(Lr[t * R + l0], x, a0);
-          b0 = fma(Lr[(t + 1) * R + l0], y, b0);
-          a1 = fma(Lr[t * R + l1], x, a1);
-          b1 = fma(Lr[(t + 1) * R + l1], y, b1);
+    for (int i = r0 + threadIdx.x; i < rend; i += kCT) {
+      const int li = i - base;
+      double a[kSpecMax];
+#pragma unroll
+      for (int c = 0; c < kSpecMax; ++c) a[c] = (c < np) ? Lr[c * R + li] : 0.0;
+#pragma unroll
+      for (int c = 1; c < kSpecMax; ++c) {
+        // sum_t L_it d_t L_ct = sum_t a_it L_ct (a_it = L_it d_t): even and
+        // odd t in two partial sums
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int t = 0; t < c; ++t) {
+          if (t & 1)
+            s1 = fma(a[t], sh.db[c][t], s1);
+          else
+            s0 = fma(a[t], sh.db[c][t], s0);
         }
-        if (t < c) {
-          const double x = sh.db[c][t];
-          a0 = fma(Lr[t * R + l0], x, a0);
-          a1 = fma(Lr[t * R + l1], x, a1);
-        }
-        Lr[c * R + l0] -= a0 + b0;
-        if (two) Lr[c * R + l1] -= a1 + b1;
+        a[c] -= s0 + s1;
+        asm volatile("" ::: "memory");  // keep the next pivot's loads from being hoisted (registers)
       }
+#pragma unroll
+      for (int c = 0; c < kSpecMax; ++c)
+        if (c < np) Lr[c * R + li] = a[c];
     }
     __syncthreads();
     // per pivot and warp: lambda part (eligible rows) and running-max part
@@ -453,9 +456,34 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
       k = ps + kstar;
       run_seq = false;
       spec = 0;
+      spec_kind = kstar == np ? 1 : 2;
+      if (kstar < np) {
+        // Continue in this launch from the failing pivot with the sequential
+        // path, which needs for the accepted pivots: L of this CTA's rows in
+        // Lr (below the block: a / d as written to F; block rows: sh.db), D
+        // in sh.Dd/Do/pk, and w = D L(k, :)^T of the next row (sh.wv[kstar]).
+        for (int c = 0; c < kstar; ++c) {
+          const double iv = sh.iv[c];
+          for (int i = r0 + threadIdx.x; i < rend; i += kCT) Lr[c * R + (i - base)] *= iv;
+          for (int i = max(base, ps + c + 1) + threadIdx.x; i < min(rend, pe); i += kCT)
+            Lr[c * R + (i - base)] = sh.db[i - ps][c];
+        }
+        if (threadIdx.x < kstar) {
+          sh.Dd[threadIdx.x] = sh.dv[threadIdx.x];
+          sh.Do[threadIdx.x] = 0.0;
+          sh.pk[threadIdx.x] = 0;
+          sh.w[threadIdx.x] = sh.wv[kstar][threadIdx.x];
+        }
+        __syncthreads();
+        run_seq = true;
+        // finish the panel here when little of it is left, else take the
+        // failing pivot's decision and speculate again in the next launch
+        seq_limit = (np - kstar <= kSeqFinish) ? np - kstar : 1;
+      }
     } else {
-      seq_limit = 1;  // the first pivot needs the sequential decision
+      seq_limit = (np <= kSeqFinish) ? np : 1;  // the first pivot needs the sequential decision
       spec += 1;
+      spec_kind = 3;
     }
   }
   int decisions = 0, nontrivial = 0;
@@ -775,10 +803,11 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     // a whole sequential panel without interchanges or 2x2 pivots: try
     // speculation again next time
     W.spec = (spec >= kSpecRetry && run_seq && nontrivial == 0) ? 0 : spec;
-    if (!run_seq)
-      atomicAdd(k - ps == np ? &g->spec_full : &g->spec_partial, 1);
-    else
-      atomicAdd(seq_limit == 1 ? &g->spec_failed : &g->seq_panels, 1);
+    int* counter = spec_kind == 1 ? &g->spec_full
+                   : spec_kind == 2 ? &g->spec_partial
+                   : spec_kind == 3 ? &g->spec_failed
+                                    : &g->seq_panels;
+    atomicAdd(counter, 1);
     int flags = flush ? kFlagFlush : 0;
     if (done) {
       flags |= kFlagDone;

@@ -6,15 +6,19 @@ on failure, multiplies delta by a growth factor and factors again. Along an
 interior-point sequence the delta that finally passes drifts with the
 barrier parameter, and every failed attempt costs a full factorization.
 
-`DeltaModel` predicts log10 of the first-attempt delta of every front from
+`DeltaModel` predicts the first-attempt delta of every front from
 statistics of that front of the matrix being factorized (diagonal
 magnitudes, expected-sign counts, column norms, sizes), with a small
 multilayer perceptron trained and evaluated on the GPU by the library's own
-kernels (symla_mlp_*). Training targets are the deltas the escalation loop
-itself accepted on earlier matrices of the sequence. The prediction goes in
-as `symla_regularize_opts.front_delta`; when it fails the inertia check the
-plain escalation continues as before, so correctness never depends on the
-model.
+kernels (symla_mlp_*). The prediction is in decades above a base delta, the
+plain escalation's first attempt (a fixed fraction of max|K|), so that it
+is the number of escalation steps to skip: a quantity that stays in the
+training range while the matrix scale drifts along the sequence. Training
+targets are log10(accepted / base) of the deltas the escalation loop itself
+accepted on earlier matrices of the sequence. The prediction goes in as
+`symla_regularize_opts.front_delta`; when it fails the inertia check the
+plain escalation takes over, one growth step above the smallest delta the
+failed attempt used, so correctness never depends on the model.
 """
 from __future__ import annotations
 
@@ -122,7 +126,8 @@ class Network:
 
 
 class DeltaModel:
-    """Standardised front features -> log10 first-attempt delta.
+    """Standardised front features -> first-attempt delta, in decades above
+    the base delta.
 
     A front's delta is its prediction, but never below the median prediction
     over the matrix's fronts, plus a margin in decades: an under-predicted
@@ -141,8 +146,9 @@ class DeltaModel:
 
     def fit(self, X: np.ndarray, T: np.ndarray, groups=None, epochs: int = 400, lr: float = 3e-3,
             minibatch: int = 4096) -> float:
-        """X: front features, T: log10 accepted delta of each front's matrix,
-        groups: the matrix index of each row (for the margin)."""
+        """X: front features, T: log10(accepted delta / base delta) of each
+        front's matrix, groups: the matrix index of each row (for the
+        margin)."""
         self.mean = X.mean(axis=0)
         self.std = X.std(axis=0)
         self.std[self.std < 1e-12] = 1.0
@@ -157,14 +163,19 @@ class DeltaModel:
                 self.margin = max(0.0, float(np.quantile(short, self.coverage)))
         return loss
 
-    def update(self, X: np.ndarray, T: np.ndarray, window: int = 20, epochs: int = 20, lr: float = 1e-3,
-               minibatch: int = 4096) -> float:
+    def update(self, X: np.ndarray, T: np.ndarray, retries: int | None = None, window: int = 20, epochs: int = 20,
+               lr: float = 1e-3, minibatch: int = 4096) -> float | None:
         """Online step along a sequence: add one matrix's fronts with the
-        delta escalation accepted for it, fine-tune on the last `window`
-        matrices (same standardisation) and refit the margin on them."""
+        delta escalation accepted for it to the last `window` matrices and,
+        unless the first attempt passed (`retries` == 0: the model was right
+        and nothing new is learned), fine-tune on them (same
+        standardisation) and refit the margin. Returns the training loss,
+        or None when no training ran."""
         self._buf = getattr(self, "_buf", [])
         self._buf.append((np.asarray(X, dtype=np.float64), np.asarray(T, dtype=np.float64)))
         self._buf = self._buf[-window:]
+        if retries == 0:
+            return None
         Xb = np.vstack([x for x, _ in self._buf])
         Tb = np.concatenate([t for _, t in self._buf])
         loss = self.net.train((Xb - self.mean) / self.std, Tb, epochs, lr, minibatch)
@@ -179,6 +190,9 @@ class DeltaModel:
     def predict_log10(self, X: np.ndarray) -> np.ndarray:
         return self.net.predict((X - self.mean) / self.std)
 
-    def front_deltas(self, X: np.ndarray) -> np.ndarray:
+    def front_deltas(self, X: np.ndarray, base: float) -> np.ndarray:
+        """Per-front first-attempt deltas for a matrix whose plain first
+        attempt is `base`: never below it (a smaller delta than plain
+        escalation's first one gains nothing)."""
         p = self.predict_log10(X)
-        return 10.0 ** (np.maximum(p, np.median(p)) + (self.margin or 0.0))
+        return base * 10.0 ** np.maximum(0.0, np.maximum(p, np.median(p)) + (self.margin or 0.0))

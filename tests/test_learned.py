@@ -45,7 +45,7 @@ def _run(seq, steps, model=None, initial=1e-14):
     """Factorize each step in StaticRegularized mode from a small first delta
     (plain escalation x10 on a failed inertia check), refine towards 1e-10.
     Returns retries and refined residuals per step, feature rows and the
-    accepted deltas (training targets)."""
+    accepted deltas in decades above the first attempt (training targets)."""
     s = SymLDLT()
     s.setMode(Mode.StaticRegularized)
     s.setOrdering(OrderingType.AMD)
@@ -59,15 +59,16 @@ def _run(seq, steps, model=None, initial=1e-14):
         if sym is None:
             s.analyzePattern(K)
             sym = s.symbolicFactor()
-        s.setInitialRegularizationDelta(initial * abs(K.data).max())
+        base = initial * abs(K.data).max()
+        s.setInitialRegularizationDelta(base)
         F = learned.front_features(sym, K, signs)
-        s.setFrontDeltas(None if model is None else model.front_deltas(F))
+        s.setFrontDeltas(None if model is None else model.front_deltas(F, base))
         s.factorize(K)
         r = s.solveWithRefinement(K, seq.b, RefinementOptions(max_iterations=30, tolerance=1e-10))
         retries.append(s.regularizationRetriesUsed())
         resid.append(r.diagnostics.final_relative_residual)
         feats.append(F)
-        targets.append(np.full(F.shape[0], math.log10(s.lastRegularizationDelta())))
+        targets.append(np.full(F.shape[0], math.log10(s.lastRegularizationDelta() / base)))
     return retries, resid, feats, targets
 
 
