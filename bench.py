@@ -528,10 +528,24 @@ def run_ours(args):
     launches_k, ms_k, flops_k, bytes_k = kstats[dom]
     if dom in ("far_update", "near_update", "small"):
         achieved = (flops_k / (ms_k * 1e-3)) / 1e12 if ms_k > 0 else 0.0
-        peak = peaks.get("bf16_tflops")
-        roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "peak_source": f"dense bf16 tensor, {peak_kind}",
-                    "algorithmic_flops_per_launch": flops_k / max(1, launches_k)}
+        bf16 = peaks.get("bf16_tflops")
+        if prec == L.PREC_FP64 and dom != "small":
+            # FP64 on the DMMA tensor path: the bf16 figure is no denominator
+            # for it; measure the FP64 tensor peak of this GPU the same way
+            # (register-only MMA loop), and give the bf16 fraction beside it
+            fp64 = C.c_double()
+            check(lib.symla_gpu_measure_fp64_tensor_peak(local, C.byref(fp64)))
+            peak = fp64.value
+            roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                        "peak_source": "FP64 DMMA (mma.sync .f64) register-only loop, measured live on this GPU; "
+                                       "no FP64 figure in MEASURED_PEAKS.json",
+                        "frac_of_bf16_peak": achieved / bf16 if bf16 else None,
+                        "algorithmic_flops_per_launch": flops_k / max(1, launches_k)}
+        else:
+            peak = bf16
+            roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                        "peak_source": f"dense bf16 tensor, {peak_kind}",
+                        "algorithmic_flops_per_launch": flops_k / max(1, launches_k)}
     else:
         achieved = (bytes_k / (ms_k * 1e-3)) / 1e9 if ms_k > 0 else 0.0
         peak = peaks.get("hbm_gbs")

@@ -256,7 +256,7 @@ int symla_gpu_set_graph(symla_gpu_ctx* ctx, int enable);
  * autotuner in ma57_b200/autotune.py). level_info: out6 = {small fronts,
  * their max m, large fronts, their max m, small-front kernel threads, panel
  * cluster CTAs}. set_level_schedule: small-front kernel threads in {128,
- * 256} and panel cluster size in {8, 16}, 0 = chosen by front size; a
+ * 256} and panel cluster size in {2, 4, 8, 16}, 0 = chosen by front size; a
  * cluster size too small for the level's fronts falls back to the default. */
 int symla_gpu_level_info(symla_gpu_ctx* ctx, int level, int* out6);
 int symla_gpu_set_level_schedule(symla_gpu_ctx* ctx, int level, int small_threads, int cluster_ctas);
@@ -301,6 +301,12 @@ int symla_mlp_gradient(symla_mlp* mlp, const double* X, const double* T, int B, 
  * batch); final_loss (optional) = mean squared error after training. */
 int symla_mlp_train(symla_mlp* mlp, const double* X, const double* T, int B, int epochs, int minibatch, double lr,
                     double* final_loss);
+
+/* Diagnostic (no reference counterpart): the FP64 tensor-path (DMMA) peak
+ * of `device` in TFLOP/s, measured with a register-only loop of independent
+ * mma.sync .f64 instructions on every SM (best of three timed launches);
+ * the roofline denominator of the FP64 Schur update. */
+int symla_gpu_measure_fp64_tensor_peak(int device, double* tflops);
 
 /* Relative residual ||B - A X||_inf / (||A||_inf ||X||_inf + ||B||_inf) of
  * a device-resident candidate solution X against device-resident B

@@ -2,8 +2,8 @@
 
 Two launch shapes depend on front size and have no single best value:
 the width of the small-front kernel (128 or 256 threads per front) and the
-number of CTAs in the panel cluster of the large fronts (8 or 16; more CTAs
-hold fewer rows each but occupy more SMs). The tree levels are bucketed by
+number of CTAs in the panel cluster of the large fronts (2, 4, 8 or 16; more
+CTAs hold fewer rows each but occupy more SMs). The tree levels are bucketed by
 the largest front they hold, and a coordinate search times the actual
 factorization (CUDA events around the numeric factorization) for each
 candidate shape of one bucket at a time, keeping the fastest. The result is
@@ -73,7 +73,7 @@ def tune(solver, A, reps: int = 2):
     apply(solver, schedule)
     base = _factor_ms(solver, A, reps)
     best = base
-    for kind, buckets, cands in (("small", small_b, (128, 256)), ("large", large_b, (8, 16))):
+    for kind, buckets, cands in (("small", small_b, (128, 256)), ("large", large_b, (2, 4, 8, 16))):
         for b in buckets:
             for cand in cands:
                 trial = {"small": dict(schedule["small"]), "large": dict(schedule["large"])}

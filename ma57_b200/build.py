@@ -23,7 +23,7 @@ NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 HOST_SRCS = ["host/symbolic.cpp", "host/amd.cpp", "host/metis_order.cpp"]
-CUDA_SRCS = ["gpu/capi.cu", "gpu/factor_kernels.cu", "gpu/solve_kernels.cu", "gpu/panel_cluster.cu", "gpu/schur_tc.cu", "gpu/noalloc.cu", "gpu/mlp.cu"]
+CUDA_SRCS = ["gpu/capi.cu", "gpu/factor_kernels.cu", "gpu/solve_kernels.cu", "gpu/panel_cluster.cu", "gpu/schur_tc.cu", "gpu/noalloc.cu", "gpu/mlp.cu", "gpu/peak.cu"]
 
 
 def _run(cmd: list[str]) -> None:

@@ -266,6 +266,8 @@ void build_level_lists(symla_gpu_ctx* c, const std::vector<int>& frontsOfLevel, 
       for (int j0 = 0; j0 < f.m; j0 += 32) {
         L.tasks.push_back(s);
         L.tasks.push_back(j0);
+        L.tasks.push_back(j0);
+        L.tasks.push_back(-1);
       }
       double cbsum = 0.0;
       for (int ch : f.children) {
@@ -277,6 +279,21 @@ void build_level_lists(symla_gpu_ctx* c, const std::vector<int>& frontsOfLevel, 
       const int nt = (mt + 127) / 128;
       tiles = std::max(tiles, nt * (nt + 1) / 2);
     }
+  }
+  if (!L.large.empty() && L.tasks.size() / 4 < 2 * 148) {
+    // too few (front, 32 columns) assembly tasks to fill the GPU: split
+    // their rows into chunks
+    std::vector<int> split;
+    for (size_t t = 0; t < L.tasks.size(); t += 4) {
+      const int s = L.tasks[t], j0 = L.tasks[t + 1], m = c->fronts[s].m;
+      for (int i0 = j0; i0 < m; i0 += kAsmRows) {
+        split.push_back(s);
+        split.push_back(j0);
+        split.push_back(i0);
+        split.push_back(i0 + kAsmRows >= m ? -1 : i0 + kAsmRows);
+      }
+    }
+    L.tasks.swap(split);
   }
   if (!L.large.empty()) {
     // one grid over the tiles of every front of the level (one CTA per SM)
@@ -739,7 +756,7 @@ void launch_level_planned(symla_gpu_ctx* c, const LevelLists& L, int level, cons
     });
   if (!L.large.empty()) {
     timed(c, SYMLA_KERNEL_ASSEMBLE, 0.0, L.assemble_bytes, [&] {
-      launch_assemble(c->d_desc, c->d_links, c->d_state, d_tasks, static_cast<int>(L.tasks.size() / 2),
+      launch_assemble(c->d_desc, c->d_links, c->d_state, d_tasks, static_cast<int>(L.tasks.size() / 4),
                       c->d_a_colptr, ko, c->d_glob, level, dynamic, st);
     });
     for (int it = 0; it < iters; ++it) launch_panel_iteration(c, L, level, ko, dynamic, d_large);
@@ -1723,8 +1740,9 @@ extern "C" int symla_gpu_level_info(symla_gpu_ctx* c, int level, int* out6) {
 extern "C" int symla_gpu_set_level_schedule(symla_gpu_ctx* c, int level, int small_threads, int cluster_ctas) {
   if (!c || level < 0 || level >= c->numLevels) return set_error(SYMLA_ERR_INVALID, "level out of range");
   if ((small_threads != 0 && small_threads != 128 && small_threads != 256) ||
-      (cluster_ctas != 0 && cluster_ctas != 8 && cluster_ctas != 16))
-    return set_error(SYMLA_ERR_INVALID, "symla_gpu_set_level_schedule: small_threads in {0,128,256}, cluster_ctas in {0,8,16}");
+      (cluster_ctas != 0 && cluster_ctas != 2 && cluster_ctas != 4 && cluster_ctas != 8 && cluster_ctas != 16))
+    return set_error(SYMLA_ERR_INVALID,
+                     "symla_gpu_set_level_schedule: small_threads in {0,128,256}, cluster_ctas in {0,2,4,8,16}");
   auto& L = c->levels[level];
   if (L.small_threads != small_threads || L.cluster_ctas != cluster_ctas) {
     L.small_threads = small_threads;

@@ -59,9 +59,10 @@ __device__ __forceinline__ int a_local_row(int pos, int ncols, int nextra) {
 
 // ---------------------------------------------------------------------------
 // Assembly of large fronts in global memory: one CTA per (front, 32-column
-// block). Every parent entry is written exactly once (gather form), so no
-// separate zero fill and no atomics; then the A entries of the block's own
-// columns are added. The children's map pointers, contribution-block
+// block, row range); levels with few large fronts split the rows into
+// chunks so that they still fill the GPU. Every parent entry is written exactly once (gather
+// form), so no separate zero fill and no atomics; then the A entries of the
+// block's own columns and rows are added. The children's map pointers, contribution-block
 // origins and their maps of the block's 32 columns are staged in shared
 // memory once; each thread then takes rows, reads a row's position in each
 // child once and issues the (independent) loads of all 32 columns, summing
@@ -80,12 +81,13 @@ __global__ void __launch_bounds__(256) assemble_kernel(const FrontDesc* __restri
   __shared__ const double* s_cb[kAsmMaxChildren];
   __shared__ int64_t s_ld[kAsmMaxChildren];
   __shared__ int s_b[kAsmMaxChildren][32];
-  const int s = tasks[2 * blockIdx.x];
-  const int j0 = tasks[2 * blockIdx.x + 1];
+  const int4 task = reinterpret_cast<const int4*>(tasks)[blockIdx.x];
+  const int s = task.x, j0 = task.y, i0 = task.z;  // i0 >= j0
   const FrontDesc f = fronts[s];
   const int j1 = min(j0 + 32, f.m), nj = j1 - j0;
+  const int iend = task.w < 0 ? f.m : min(task.w, f.m);
   const int nch = f.ch_end - f.ch_begin;
-  if (threadIdx.x < nj) f.lperm[j0 + threadIdx.x] = j0 + threadIdx.x;
+  if (i0 == j0 && threadIdx.x < nj) f.lperm[j0 + threadIdx.x] = j0 + threadIdx.x;
   if (nch <= kAsmMaxChildren) {
     if (threadIdx.x < nch) {
       const ChildLink L = links[f.ch_begin + threadIdx.x];
@@ -101,7 +103,7 @@ __global__ void __launch_bounds__(256) assemble_kernel(const FrontDesc* __restri
       s_b[c][jj] = (jj < nj) ? s_inv[c][j0 + jj] : -1;
     }
     __syncthreads();
-    for (int i = j0 + threadIdx.x; i < f.m; i += blockDim.x) {
+    for (int i = i0 + threadIdx.x; i < iend; i += blockDim.x) {
       double acc[32];
 #pragma unroll
       for (int jj = 0; jj < 32; ++jj) acc[jj] = 0.0;
@@ -126,7 +128,7 @@ __global__ void __launch_bounds__(256) assemble_kernel(const FrontDesc* __restri
   } else {
     for (int j = j0; j < j1; ++j) {
       double* col = f.F + static_cast<int64_t>(j) * f.ld;
-      for (int i = j + threadIdx.x; i < f.m; i += blockDim.x)
+      for (int i = max(j, i0) + threadIdx.x; i < iend; i += blockDim.x)
         col[i] = gather_children(fronts, links, st, f.ch_begin, f.ch_end, i, j);
     }
   }
@@ -137,7 +139,7 @@ __global__ void __launch_bounds__(256) assemble_kernel(const FrontDesc* __restri
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
       const int j = o.a_j[e];
       const int i = a_local_row(o.a_pos[e], f.ncols, f.nextra);
-      f.F[static_cast<int64_t>(j) * f.ld + i] += o.values[o.a_idx[e]];
+      if (i >= i0 && i < iend) f.F[static_cast<int64_t>(j) * f.ld + i] += o.values[o.a_idx[e]];
     }
   }
   // max |entry| of the assembled front (dense_kernel.hpp:413), folded here
@@ -146,7 +148,7 @@ __global__ void __launch_bounds__(256) assemble_kernel(const FrontDesc* __restri
   double tmax = 0.0;
   for (int j = j0; j < j1; ++j) {
     const double* col = f.F + static_cast<int64_t>(j) * f.ld;
-    for (int i = j + threadIdx.x; i < f.m; i += blockDim.x) tmax = fmax(tmax, fabs(col[i]));
+    for (int i = max(j, i0) + threadIdx.x; i < iend; i += blockDim.x) tmax = fmax(tmax, fabs(col[i]));
   }
   tmax = warp_max(tmax);
   if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&st[s].orig_max, tmax);
@@ -843,14 +845,11 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* _
 //        pivots [ps, k1) of the panel;
 //   far  (after an outer block, a flush or the last panel): columns
 //        [max(ob_end, k1), m), pivots [ob, k1) of the whole block.
-// C(i, j) -= sum_q L(i, q) (L D)(j, q) for i >= j. 128 x 128 tiles, 256
-// threads, 8 x 8 register blocks (rows tx + 16u, columns ty + 16v, so a
-// half-warp touches 16 consecutive rows of a column); the K range is staged
-// in shared memory 32 pivots at a time. The tile's C values are loaded
-// before the staging so their latency overlaps it.
+// C(i, j) -= sum_q L(i, q) (L D)(j, q) for i >= j, over 128 x 128 tiles of
+// every front of the level (one tile space), the K range staged 32 pivots
+// at a time.
 namespace {
 constexpr int kTT = 128;        // tile edge
-constexpr int kTThreads = 256;  // 16 x 16 threads, 8 x 8 outputs each
 constexpr int kKC = 32;         // K chunk
 constexpr int kMaxUpdateFronts = 1024;  // fronts per update launch
 }  // namespace
@@ -883,28 +882,6 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// Stage pivots [kc, kc + kn) of rows i0.. (A side) and rows j0.. (B side,
-// with one halo column on each side for the 2x2 blocks of D) into smem.
-__device__ __forceinline__ void update_stage(const FrontDesc& f, int q0, int q1, int kc, int kn, int i0, int j0,
-                                             double* Ls, double* Lj) {
-  const int64_t ld = f.ld;
-  const int m = f.m;
-  for (int t = threadIdx.x; t < kn * kTT; t += kTThreads) {
-    const int q = t / kTT, r = t % kTT;
-    const int gi = i0 + r;
-    const double* src = f.F + (kc + q) * ld + (gi < m ? gi : 0);
-    cp_async8(Ls + q * kTT + r, src, gi < m);
-  }
-  for (int t = threadIdx.x; t < (kn + 2) * kTT; t += kTThreads) {
-    const int q = t / kTT - 1, r = t % kTT;
-    const int pq = kc + q;
-    const int gj = j0 + r;
-    const bool ok = gj < m && pq >= q0 && pq < q1;
-    const double* src = f.F + (ok ? pq * ld + gj : 0);
-    cp_async8(Lj + (q + 1) * kTT + r, src, ok);
-  }
-}
-
 // Tiles of front s's update region: column tiles over [c0, c1), each with
 // row tiles from its diagonal down to m.
 __device__ __forceinline__ int update_tiles(int m, int c0, int c1) {
@@ -913,211 +890,68 @@ __device__ __forceinline__ int update_tiles(int m, int c0, int c1) {
   return n;
 }
 
-// MODE 0: near updates, 1: far updates, 2: both in one tile space (their
-// column ranges are disjoint and read only finished L columns).
-template <int MODE>
-__global__ void __launch_bounds__(kTThreads) update_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
-                                                           const int* __restrict__ front_list, int count,
-                                                           FactorGlobals* g, int level, int dynamic,
-                                                           const double* __restrict__ tc_guard) {
-  if (level_aborted(g, level, dynamic)) return;
-  // two stages of {A rows (kKC x kTT), B rows with halo ((kKC+2) x kTT)} and
-  // one (L D) buffer (kKC x kTT)
-  extern __shared__ double usm[];
-  double* LsBuf[2] = {usm, usm + (2 * kKC + 2) * kTT};
-  double* LjBuf[2] = {usm + kKC * kTT, usm + (3 * kKC + 2) * kTT};
-  double* Wj = usm + (4 * kKC + 4) * kTT;
-  __shared__ double dd[kKC], dlo[kKC], dhi[kKC];
-  __shared__ int8_t kk[kKC];
-  __shared__ int tile_end[2 * kMaxUpdateFronts];
-  // one tile space over every front (and, in MODE 2, both ranges) of the
-  // launch, so idle fronts do not leave CTAs without work; entry e is front
-  // e % count, its far range when e >= count in MODE 2
-  const int nent = (MODE == 2) ? 2 * count : count;
-  auto entry_far = [&](int e) { return MODE == 1 || (MODE == 2 && e >= count); };
-  for (int t = threadIdx.x; t < nent; t += kTThreads) {
-    const int sf = front_list[t % count];
-    const bool far = entry_far(t);
-    int c0, c1, q0, q1;
-    const FrontState S = st[sf];
-    bool use = update_range(S, fronts[sf].m, far, c0, c1, q0, q1);
-    if (far && use && tc_guard && tc_block_ok(q1 - q0, tc_guard[2 * t], tc_guard[2 * t + 1], g->amax))
-      use = false;  // the tensor-core kernel applied this block
-    tile_end[t] = use ? update_tiles(fronts[sf].m, c0, c1) : 0;
-    if (blockIdx.x == 0 && tile_end[t] > 0) {
-      const double nc = c1 - c0, mm = fronts[sf].m;
-      const double entries = nc * mm - (static_cast<double>(c0) + c1 - 1) * nc / 2.0;
-      atomicAdd(far ? &g->flops_far : &g->flops_near, 2.0 * (q1 - q0) * entries);
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0)
-    for (int t = 1; t < nent; ++t) tile_end[t] += tile_end[t - 1];
-  __syncthreads();
-  const int total = nent > 0 ? tile_end[nent - 1] : 0;
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  double tmax = 0.0;
-  int cur = -1, s = -1;
-  FrontDesc f;
-  int m = 0, c0 = 0, c1 = 0, q0 = 0, q1 = 0, nchunks = 0;
-  int64_t ld = 0;
-  for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
-    int fi = 0;
-    while (tile >= tile_end[fi]) ++fi;
-    if (fi != cur) {
-      if (cur >= 0) {
-        tmax = warp_max(tmax);
-        if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&st[s].running_max, tmax);
-        tmax = 0.0;
-      }
-      cur = fi;
-      s = front_list[fi % count];
-      f = fronts[s];
-      m = f.m;
-      ld = f.ld;
-      update_range(st[s], m, entry_far(fi), c0, c1, q0, q1);
-      nchunks = (q1 - q0 + kKC - 1) / kKC;
-    }
-    int rem = tile - (fi > 0 ? tile_end[fi - 1] : 0);
-    int tj = 0;
-    for (;;) {
-      const int nr = (m - (c0 + tj * kTT) + kTT - 1) / kTT;
-      if (rem < nr) break;
-      rem -= nr;
-      ++tj;
-    }
-    const int j0 = c0 + tj * kTT, i0 = j0 + rem * kTT;
-    __syncthreads();  // previous tile done with the buffers
-    update_stage(f, q0, q1, q0, min(kKC, q1 - q0), i0, j0, LsBuf[0], LjBuf[0]);
-    cp_async_commit();
-    double acc[8][8];
-#pragma unroll
-    for (int v = 0; v < 8; ++v) {
-      const int gj = j0 + ty + 16 * v;
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int gi = i0 + tx + 16 * u;
-        acc[u][v] = (gj < c1 && gi < m && gi >= gj) ? f.F[gj * ld + gi] : 0.0;
-      }
-    }
-    for (int c = 0; c < nchunks; ++c) {
-      const int kc = q0 + c * kKC, kn = min(kKC, q1 - kc);
-      if (c + 1 < nchunks) {
-        const int kc2 = kc + kKC;
-        update_stage(f, q0, q1, kc2, min(kKC, q1 - kc2), i0, j0, LsBuf[(c + 1) & 1], LjBuf[(c + 1) & 1]);
-      }
-      cp_async_commit();
-      if (threadIdx.x < kn) {
-        const int pq = kc + threadIdx.x;
-        const int8_t kind = f.pk[pq];
-        kk[threadIdx.x] = kind;
-        dd[threadIdx.x] = f.Dd[pq];
-        dlo[threadIdx.x] = (kind == 2) ? f.Do[pq - 1] : 0.0;
-        dhi[threadIdx.x] = (kind == 1) ? f.Do[pq] : 0.0;
-      }
-      cp_async_wait<1>();
-      __syncthreads();
-      const double* Ls = LsBuf[c & 1];
-      const double* Lj = LjBuf[c & 1];
-      // (L D)(j, q) from the staged L rows of the B side and D's blocks
-      for (int t = threadIdx.x; t < kn * kTT; t += kTThreads) {
-        const int q = t / kTT, r = t % kTT;
-        const double* col = Lj + (q + 1) * kTT + r;
-        double w = dd[q] * col[0];
-        if (kk[q] == 1) w += dhi[q] * col[kTT];
-        if (kk[q] == 2) w += dlo[q] * col[-kTT];
-        Wj[q * kTT + r] = w;
-      }
-      __syncthreads();
-      for (int q = 0; q < kn; ++q) {
-        double a[8], b[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          a[u] = Ls[q * kTT + tx + 16 * u];
-          b[u] = Wj[q * kTT + ty + 16 * u];
-        }
-#pragma unroll
-        for (int u = 0; u < 8; ++u)
-#pragma unroll
-          for (int v = 0; v < 8; ++v) acc[u][v] = fma(-a[u], b[v], acc[u][v]);
-      }
-      __syncthreads();
-    }
-#pragma unroll
-    for (int v = 0; v < 8; ++v) {
-      const int gj = j0 + ty + 16 * v;
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int gi = i0 + tx + 16 * u;
-        if (gj < c1 && gi < m && gi >= gj) {
-          f.F[gj * ld + gi] = acc[u][v];
-          tmax = fmax(tmax, fabs(acc[u][v]));
-        }
-      }
-    }
-  }
-  if (cur >= 0) {
-    tmax = warp_max(tmax);
-    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&st[s].running_max, tmax);
-  }
-}
-
 // ---------------------------------------------------------------------------
-// The same near / far updates on the FP64 tensor path: mma.sync m8n8k4 .f64
-// (DMMA; the 5th-gen tcgen05 MMA has no FP64 kind). 128 x 128 tiles, 8 warps
-// of 64 x 32 (8 x 4 MMA tiles, 2 accumulators each per lane). A chunk of 32
+// The near / far updates on the FP64 tensor path: mma.sync m16n8k8 .f64
+// (DMMA; the 5th-gen tcgen05 MMA has no FP64 kind). 128 x 128 tiles, 16 warps
+// of 32 x 32 (2 x 4 MMA tiles, 4 accumulators each per lane; four warps per
+// scheduler hide the shared-memory fragment loads). A chunk of 32
 // pivots of the A rows (L(i, q)) and of the B rows (L(j, q) with one halo
-// column each side, for D's 2 x 2 blocks) is staged row-major with a 36-double
-// row stride (conflict-free fragment loads), double-buffered by cp.async;
-// W(j, q) = (L D)(j, q) is formed once per chunk in shared memory; the
-// negated L fragment accumulates onto the C tile held in registers.
+// column each side, for D's 2 x 2 blocks) is staged pivot-major as in the
+// front (coalesced, conflict-free cp.async) with a 132-double stride, which
+// also makes the fragment loads conflict-free (lanes 0-15 of a 64-bit load
+// hit 16 distinct bank pairs); double-buffered. W(j, q) = -(L D)(j, q) is
+// formed once per chunk in shared memory and the L fragment accumulates onto
+// the C tile held in registers.
 namespace {
-constexpr int kMS = 36;  // row stride of the staged tiles (doubles)
+constexpr int kAS = 132;  // pivot-major stride of the staged tiles (doubles)
+constexpr int kMThreads = 512;  // 16 warps of 32 x 32
+constexpr size_t kMmaSmem = static_cast<size_t>(2 * kKC + 2 * (kKC + 2) + kKC) * kAS * sizeof(double);
 
-__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-               : "+d"(c0), "+d"(c1)
-               : "d"(a), "d"(b));
+// c (16 x 8) += a (16 x 8) * b (8 x 8); lane (g, t) = (lane >> 2, lane & 3):
+// a_r = A(g + 8 (r & 1), t + 4 (r >> 1)), b_r = B(t + 4 r, g),
+// c_e = C(g + 8 (e >> 1), 2 t + (e & 1))
+__device__ __forceinline__ void dmma16x8x8(double* c, const double* a, const double* b) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+               : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+               : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
 // A rows i (pivots kc .. kc + kn) and B rows j (pivots kc - 1 .. kc + kn,
-// valid inside [q0, q1)) into row-major tiles, zero-filled outside.
-__device__ __forceinline__ void mma_stage(const FrontDesc& f, int q0, int q1, int kc, int kn, int i0, int j0,
-                                          double* As, double* Bs) {
-  const int64_t ld = f.ld;
-  const int m = f.m;
-  for (int t = threadIdx.x; t < kKC * kTT; t += kTThreads) {
+// valid inside [q0, q1)) into pivot-major tiles, zero-filled outside.
+__device__ __forceinline__ void mma_stage(const double* F, int64_t ld, int m, int q0, int q1, int kc, int kn, int i0,
+                                          int j0, double* As, double* Bs) {
+  for (int t = threadIdx.x; t < kKC * kTT; t += kMThreads) {
     const int k = t / kTT, r = t % kTT;
     const int gi = i0 + r;
     const bool ok = k < kn && gi < m;
-    cp_async8(As + r * kMS + k, f.F + (ok ? (kc + k) * ld + gi : 0), ok);
+    cp_async8(As + k * kAS + r, F + (ok ? (kc + k) * ld + gi : 0), ok);
   }
-  for (int t = threadIdx.x; t < (kKC + 2) * kTT; t += kTThreads) {
+  for (int t = threadIdx.x; t < (kKC + 2) * kTT; t += kMThreads) {
     const int kp = t / kTT, r = t % kTT;
     const int pq = kc + kp - 1;
     const int gj = j0 + r;
     const bool ok = gj < m && pq >= q0 && pq < q1 && kp <= kn + 1;  // halo: 2 x 2 partners either side
-    cp_async8(Bs + r * kMS + kp, f.F + (ok ? pq * ld + gj : 0), ok);
+    cp_async8(Bs + kp * kAS + r, F + (ok ? pq * ld + gj : 0), ok);
   }
 }
 }  // namespace
 
 template <int MODE>
-__global__ void __launch_bounds__(kTThreads, 1) update_mma_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
+__global__ void __launch_bounds__(kMThreads, 1) update_mma_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
                                                                const int* __restrict__ front_list, int count,
                                                                FactorGlobals* g, int level, int dynamic,
                                                                const double* __restrict__ tc_guard) {
   if (level_aborted(g, level, dynamic)) return;
   extern __shared__ double usm[];
-  double* AsBuf[2] = {usm, usm + kTT * kMS};
-  double* BsBuf[2] = {usm + 2 * kTT * kMS, usm + 3 * kTT * kMS};
-  double* Ws = usm + 4 * kTT * kMS;
+  double* AsBuf[2] = {usm, usm + kKC * kAS};
+  double* BsBuf[2] = {usm + 2 * kKC * kAS, usm + (3 * kKC + 2) * kAS};
+  double* Ws = usm + (4 * kKC + 4) * kAS;
   __shared__ double dd[kKC], dlo[kKC], dhi[kKC];
   __shared__ int8_t kk[kKC];
   __shared__ int tile_end[2 * kMaxUpdateFronts];
   const int nent = (MODE == 2) ? 2 * count : count;
   auto entry_far = [&](int e) { return MODE == 1 || (MODE == 2 && e >= count); };
-  for (int t = threadIdx.x; t < nent; t += kTThreads) {
+  for (int t = threadIdx.x; t < nent; t += kMThreads) {
     const int sf = front_list[t % count];
     const bool far = entry_far(t);
     int c0, c1, q0, q1;
@@ -1138,11 +972,11 @@ __global__ void __launch_bounds__(kTThreads, 1) update_mma_kernel(const FrontDes
   __syncthreads();
   const int total = nent > 0 ? tile_end[nent - 1] : 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wr = warp >> 2, wc = warp & 3;          // warp's 64 x 32 sub-tile
-  const int lr = lane >> 2, lk = lane & 3;          // fragment coordinates
+  const int wr = warp >> 2, wc = warp & 3;          // warp's 32 x 32 sub-tile
+  const int lg = lane >> 2, lt = lane & 3;          // fragment coordinates
   double tmax = 0.0;
   int cur = -1, s = -1;
-  FrontDesc f;
+  double* Fp = nullptr;
   int m = 0, c0 = 0, c1 = 0, q0 = 0, q1 = 0, nchunks = 0;
   int64_t ld = 0;
   for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
@@ -1156,9 +990,9 @@ __global__ void __launch_bounds__(kTThreads, 1) update_mma_kernel(const FrontDes
       }
       cur = fi;
       s = front_list[fi % count];
-      f = fronts[s];
-      m = f.m;
-      ld = f.ld;
+      Fp = fronts[s].F;
+      m = fronts[s].m;
+      ld = fronts[s].ld;
       update_range(st[s], m, entry_far(fi), c0, c1, q0, q1);
       nchunks = (q1 - q0 + kKC - 1) / kKC;
     }
@@ -1172,84 +1006,94 @@ __global__ void __launch_bounds__(kTThreads, 1) update_mma_kernel(const FrontDes
     }
     const int j0 = c0 + tj * kTT, i0 = j0 + rem * kTT;
     __syncthreads();  // previous tile done with the buffers
-    mma_stage(f, q0, q1, q0, min(kKC, q1 - q0), i0, j0, AsBuf[0], BsBuf[0]);
+    mma_stage(Fp, ld, m, q0, q1, q0, min(kKC, q1 - q0), i0, j0, AsBuf[0], BsBuf[0]);
     cp_async_commit();
-    // C tile into the accumulators (lane holds rows gi0 + 8 rt, columns
-    // gj0 + 8 ct + e)
-    const int gi0 = i0 + wr * 64 + lr, gj0 = j0 + wc * 32 + 2 * lk;
-    double acc[8][4][2];
+    // C tile into the accumulators (lane holds rows gi0 + 16 rt + 8 v,
+    // columns gj0 + 8 ct + h as acc[rt][ct][2 v + h])
+    const int gi0 = i0 + wr * 32 + lg, gj0 = j0 + wc * 32 + 2 * lt;
+    double acc[2][4][4];
 #pragma unroll
     for (int ct = 0; ct < 4; ++ct)
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int gj = gj0 + ct * 8 + e;
-        const double* colp = f.F + static_cast<int64_t>(gj < c1 ? gj : 0) * ld;
+      for (int h = 0; h < 2; ++h) {
+        const int gj = gj0 + ct * 8 + h;
+        const double* colp = Fp + static_cast<int64_t>(gj < c1 ? gj : 0) * ld;
 #pragma unroll
-        for (int rt = 0; rt < 8; ++rt) {
-          const int gi = gi0 + rt * 8;
-          acc[rt][ct][e] = (gj < c1 && gi < m && gi >= gj) ? colp[gi] : 0.0;
-        }
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int v = 0; v < 2; ++v) {
+            const int gi = gi0 + rt * 16 + 8 * v;
+            acc[rt][ct][2 * v + h] = (gj < c1 && gi < m && gi >= gj) ? colp[gi] : 0.0;
+          }
       }
     for (int c = 0; c < nchunks; ++c) {
       const int kc = q0 + c * kKC, kn = min(kKC, q1 - kc);
       if (c + 1 < nchunks) {
         const int kc2 = kc + kKC;
-        mma_stage(f, q0, q1, kc2, min(kKC, q1 - kc2), i0, j0, AsBuf[(c + 1) & 1], BsBuf[(c + 1) & 1]);
+        mma_stage(Fp, ld, m, q0, q1, kc2, min(kKC, q1 - kc2), i0, j0, AsBuf[(c + 1) & 1], BsBuf[(c + 1) & 1]);
       }
       cp_async_commit();
       if (threadIdx.x < kn) {
         const int pq = kc + threadIdx.x;
-        const int8_t kind = f.pk[pq];
+        const FrontDesc& fd = fronts[s];
+        const int8_t kind = fd.pk[pq];
         kk[threadIdx.x] = kind;
-        dd[threadIdx.x] = f.Dd[pq];
-        dlo[threadIdx.x] = (kind == 2) ? f.Do[pq - 1] : 0.0;
-        dhi[threadIdx.x] = (kind == 1) ? f.Do[pq] : 0.0;
+        dd[threadIdx.x] = fd.Dd[pq];
+        dlo[threadIdx.x] = (kind == 2) ? fd.Do[pq - 1] : 0.0;
+        dhi[threadIdx.x] = (kind == 1) ? fd.Do[pq] : 0.0;
       }
       cp_async_wait<1>();
       __syncthreads();
       const double* As = AsBuf[c & 1];
       const double* Bs = BsBuf[c & 1];
-      // W(j, q) = (L D)(j, q); zero past the chunk (the MMAs run over 4-pivot steps)
-      const int kn4 = (kn + 3) & ~3;
-      for (int t = threadIdx.x; t < kn4 * kTT; t += kTThreads) {
+      // W(j, q) = -(L D)(j, q); zero past the chunk (the MMAs run over
+      // 8-pivot steps; A is zero-filled past kn)
+      const int kn8 = (kn + 7) & ~7;
+      for (int t = threadIdx.x; t < kn8 * kTT; t += kMThreads) {
         const int q = t / kTT, r = t % kTT;
         double w = 0.0;
         if (q < kn) {
-          const double* row = Bs + r * kMS + q + 1;
-          w = dd[q] * row[0];
-          if (kk[q] == 1) w += dhi[q] * row[1];
-          if (kk[q] == 2) w += dlo[q] * row[-1];
+          const double* col = Bs + (q + 1) * kAS + r;
+          w = dd[q] * col[0];
+          if (kk[q] == 1) w += dhi[q] * col[kAS];
+          if (kk[q] == 2) w += dlo[q] * col[-kAS];
         }
-        Ws[r * kMS + q] = w;
+        Ws[q * kAS + r] = -w;
       }
       __syncthreads();
-      for (int k0 = 0; k0 < kn4; k0 += 4) {
-        double a[8], b[4];
+      for (int k0 = 0; k0 < kn8; k0 += 8) {
+        double b[4][2];
 #pragma unroll
-        for (int rt = 0; rt < 8; ++rt) a[rt] = -As[(wr * 64 + rt * 8 + lr) * kMS + k0 + lk];
+        for (int ct = 0; ct < 4; ++ct)
 #pragma unroll
-        for (int ct = 0; ct < 4; ++ct) b[ct] = Ws[(wc * 32 + ct * 8 + lr) * kMS + k0 + lk];
+          for (int r = 0; r < 2; ++r) b[ct][r] = Ws[(k0 + lt + 4 * r) * kAS + wc * 32 + ct * 8 + lg];
 #pragma unroll
-        for (int rt = 0; rt < 8; ++rt)
+        for (int rt = 0; rt < 2; ++rt) {
+          double a[4];
 #pragma unroll
-          for (int ct = 0; ct < 4; ++ct) dmma(acc[rt][ct][0], acc[rt][ct][1], a[rt], b[ct]);
+          for (int r = 0; r < 4; ++r) a[r] = As[(k0 + lt + 4 * (r >> 1)) * kAS + wr * 32 + rt * 16 + lg + 8 * (r & 1)];
+#pragma unroll
+          for (int ct = 0; ct < 4; ++ct) dmma16x8x8(acc[rt][ct], a, b[ct]);
+        }
       }
       __syncthreads();
     }
 #pragma unroll
     for (int ct = 0; ct < 4; ++ct)
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int gj = gj0 + ct * 8 + e;
-        double* colp = f.F + static_cast<int64_t>(gj < c1 ? gj : 0) * ld;
+      for (int h = 0; h < 2; ++h) {
+        const int gj = gj0 + ct * 8 + h;
+        double* colp = Fp + static_cast<int64_t>(gj < c1 ? gj : 0) * ld;
 #pragma unroll
-        for (int rt = 0; rt < 8; ++rt) {
-          const int gi = gi0 + rt * 8;
-          if (gj < c1 && gi < m && gi >= gj) {
-            colp[gi] = acc[rt][ct][e];
-            tmax = fmax(tmax, fabs(acc[rt][ct][e]));
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int v = 0; v < 2; ++v) {
+            const int gi = gi0 + rt * 16 + 8 * v;
+            if (gj < c1 && gi < m && gi >= gj) {
+              colp[gi] = acc[rt][ct][2 * v + h];
+              tmax = fmax(tmax, fabs(acc[rt][ct][2 * v + h]));
+            }
           }
-        }
       }
   }
   if (cur >= 0) {
@@ -1327,14 +1171,14 @@ void launch_mark_unfinished(const FrontState* st, const int* list, int count, Fa
 void launch_update(bool far, const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
                    FactorGlobals* g, int level, int dynamic, cudaStream_t stream, const double* tc_guard) {
   if (count <= 0 || grid_x <= 0) return;
-  const size_t sm = static_cast<size_t>(5) * kTT * kMS * sizeof(double);
+  const size_t sm = kMmaSmem;
   for (int b = 0; b < count; b += kMaxUpdateFronts) {
     const int cnt = count - b < kMaxUpdateFronts ? count - b : kMaxUpdateFronts;
     if (far)
-      update_mma_kernel<1><<<grid_x, kTThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic,
+      update_mma_kernel<1><<<grid_x, kMThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic,
                                                               tc_guard ? tc_guard + 2 * b : nullptr);
     else
-      update_mma_kernel<0><<<grid_x, kTThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic,
+      update_mma_kernel<0><<<grid_x, kMThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic,
                                                               nullptr);
   }
 }
@@ -1342,10 +1186,10 @@ void launch_update(bool far, const FrontDesc* fronts, FrontState* st, const int*
 void launch_update_both(const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
                         FactorGlobals* g, int level, int dynamic, cudaStream_t stream) {
   if (count <= 0 || grid_x <= 0) return;
-  const size_t sm = static_cast<size_t>(5) * kTT * kMS * sizeof(double);
+  const size_t sm = kMmaSmem;
   for (int b = 0; b < count; b += kMaxUpdateFronts) {
     const int cnt = count - b < kMaxUpdateFronts ? count - b : kMaxUpdateFronts;
-    update_mma_kernel<2><<<grid_x, kTThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic, nullptr);
+    update_mma_kernel<2><<<grid_x, kMThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic, nullptr);
   }
 }
 
@@ -1357,14 +1201,8 @@ cudaError_t configure_factor_kernels() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(update_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(update_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(update_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  if (e != cudaSuccess) return e;
   for (auto fn : {update_mma_kernel<0>, update_mma_kernel<1>, update_mma_kernel<2>}) {
-    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 5 * kTT * kMS * sizeof(double));
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMmaSmem);
     if (e != cudaSuccess) return e;
   }
   return e;

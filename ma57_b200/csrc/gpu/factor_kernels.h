@@ -12,10 +12,14 @@ namespace symla_gpu {
 constexpr int kSmallFrontMax = 128;
 // Panel width of the large-front path.
 constexpr int kPanelWidth = 32;
+// Rows of one assembly task when a level's (front, 32 columns) tasks are
+// too few to fill the GPU (they are then split into row chunks).
+constexpr int kAsmRows = 1024;
 
 cudaError_t configure_factor_kernels();
 size_t small_front_smem(int m);
 
+// tasks: (front, first column, first row, end row or -1 for the front's m)
 void launch_assemble(const FrontDesc* fronts, const ChildLink* links, FrontState* st, const int* tasks,
                      int ntasks, const int* a_colptr, const KernelOpts& o, const FactorGlobals* g, int level,
                      int dynamic, cudaStream_t stream);
@@ -27,10 +31,10 @@ void launch_panel(const FrontDesc* fronts, FrontState* st, const int* list, int 
 // Cluster panel (panel_cluster.cu): returns 0 from cluster_size_for when a
 // front is too large for it (the single-CTA panel kernel then runs).
 int cluster_size_for(int max_m, int count);
-// whether a cluster of cs CTAs (8 or 16) can hold fronts of max_m rows
+// whether a cluster of cs CTAs (2, 4, 8 or 16) can hold fronts of max_m rows
 bool cluster_size_fits(int max_m, int cs);
 cudaError_t configure_cluster_panel();
-// cs: 8 or 16, or 0 for cluster_size_for's choice
+// cs: 2, 4, 8 or 16, or 0 for cluster_size_for's choice
 cudaError_t launch_cluster_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m,
                                  int nb, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
                                  cudaStream_t stream, int cs = 0);

@@ -1,6 +1,6 @@
 // Panel factorization of large fronts by a thread-block cluster.
 //
-// One cluster of CS CTAs (8 or 16) factors up to NB pivots of one front.
+// One cluster of CS CTAs (2, 4, 8 or 16) factors up to NB pivots of one front.
 // The rows [ps, m) of the front are split into CS contiguous slices; CTA q
 // keeps, in its shared memory, the panel's L values of its rows (one column
 // per pivot of the panel) and the current values of the candidate columns.
@@ -828,21 +828,29 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
 }
 
 bool cluster_size_fits(int max_m, int cs) {
-  const size_t limit = 184 * 1024;
-  return (cs == 8 || cs == 16) &&
+  const size_t limit = 184 * 1024;  // + the static ClusterShared (~38 KB) <= 227 KB
+  return (cs == 2 || cs == 4 || cs == 8 || cs == 16) &&
          static_cast<size_t>((max_m + cs - 1) / cs) * (kPanelWidth + 4) * sizeof(double) <= limit;
 }
 
 int cluster_size_for(int max_m, int count) {
-  const size_t limit = 184 * 1024;  // + the static ClusterShared (~38 KB) <= 227 KB
-  const bool fits8 = static_cast<size_t>((max_m + 7) / 8) * (kPanelWidth + 4) * sizeof(double) <= limit;
-  const bool fits16 = static_cast<size_t>((max_m + 15) / 16) * (kPanelWidth + 4) * sizeof(double) <= limit;
-  // The panel is latency- and per-SM-traffic-bound: 16 CTAs halve each
-  // CTA's rows. Use them when every front of the launch still gets its
-  // cluster in one wave over the 148 SMs, and for fronts too tall for 8.
-  if (fits16 && (!fits8 || (max_m >= 768 && count * 16 <= 144))) return 16;
-  if (fits8) return 8;
-  return 0;  // too large for the cluster kernel
+  // The panel is latency-bound: a CTA costs a fixed ~8 us (the diagonal
+  // block's pivot chain, the exchanges) plus ~10 ns per row it holds, and
+  // one CTA runs per SM (200 registers x 256 threads). More CTAs per front
+  // shorten each CTA; fewer let more fronts run in one wave. Pick the
+  // cluster size with the smallest modelled time (waves x CTA time).
+  int best = 0;
+  double best_t = 0.0;
+  for (int cs : {2, 4, 8, 16}) {
+    if (!cluster_size_fits(max_m, cs)) continue;
+    const double waves = std::ceil(static_cast<double>(count) * cs / 148.0);
+    const double t = waves * (8.0 + 0.01 * ((max_m + cs - 1) / cs));
+    if (best == 0 || t < best_t) {
+      best = cs;
+      best_t = t;
+    }
+  }
+  return best;  // 0: too large for the cluster kernel
 }
 
 size_t cluster_panel_smem(int max_m, int nb, int cs) {
@@ -851,7 +859,11 @@ size_t cluster_panel_smem(int max_m, int nb, int cs) {
 }
 
 cudaError_t configure_cluster_panel() {
-  cudaError_t e = cudaFuncSetAttribute(cluster_panel_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 184 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(cluster_panel_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 184 * 1024);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(cluster_panel_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 184 * 1024);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(cluster_panel_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 184 * 1024);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(cluster_panel_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 184 * 1024);
   if (e != cudaSuccess) return e;
@@ -876,8 +888,16 @@ cudaError_t launch_cluster_panel(const FrontDesc* fronts, FrontState* st, const 
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (cs == 16) return cudaLaunchKernelEx(&cfg, cluster_panel_kernel<16>, fronts, st, list, nb, R, o, g, level, dynamic);
-  return cudaLaunchKernelEx(&cfg, cluster_panel_kernel<8>, fronts, st, list, nb, R, o, g, level, dynamic);
+  switch (cs) {
+    case 16:
+      return cudaLaunchKernelEx(&cfg, cluster_panel_kernel<16>, fronts, st, list, nb, R, o, g, level, dynamic);
+    case 8:
+      return cudaLaunchKernelEx(&cfg, cluster_panel_kernel<8>, fronts, st, list, nb, R, o, g, level, dynamic);
+    case 4:
+      return cudaLaunchKernelEx(&cfg, cluster_panel_kernel<4>, fronts, st, list, nb, R, o, g, level, dynamic);
+    default:
+      return cudaLaunchKernelEx(&cfg, cluster_panel_kernel<2>, fronts, st, list, nb, R, o, g, level, dynamic);
+  }
 }
 
 }  // namespace symla_gpu
