@@ -263,7 +263,8 @@ int symla_gpu_set_level_schedule(symla_gpu_ctx* ctx, int level, int small_thread
 int symla_gpu_graph_stats(symla_gpu_ctx* ctx, int* captures, int* resumes);
 int symla_gpu_kernel_stats(symla_gpu_ctx* ctx, int kind, double* out4);
 void symla_gpu_reset_kernel_stats(symla_gpu_ctx* ctx);
-/* Number of kernels the library launched since the last reset. */
+/* Number of kernels the library launched since the last reset (the kernel
+ * nodes of a replayed factorization graph count at every replay). */
 long long symla_gpu_launch_count(symla_gpu_ctx* ctx);
 
 /* Front-size statistics of the plan: [0] fronts, [1] levels, [2] max m,

@@ -593,6 +593,8 @@ void build_plan(symla_gpu_ctx* c, const symla_host::SymbolicFactor& sf, const in
   std::vector<std::vector<int>> byLevel(numLevels);
   for (int s = 0; s < numSN; ++s) byLevel[c->fronts[s].level].push_back(s);
   c->levels.assign(numLevels, LevelLists());
+  c->level_iters.assign(numLevels, 0);
+  c->graph_level_iters.clear();
   for (int l = 0; l < numLevels; ++l) {
     build_level_lists(c, byLevel[l], c->levels[l]);
     upload_level_lists(c->levels[l], c->stream);
@@ -764,12 +766,21 @@ void launch_level_planned(symla_gpu_ctx* c, const LevelLists& L, int level, cons
 }
 
 void complete_level(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
-                    const int* d_large);
+                    const int* d_large, int launched);
+
+// Panel iterations to launch for a level before checking it on the host:
+// the planned count, or the most an earlier factorization of the same plan
+// needed (the same pattern usually pivots alike).
+int level_plan_iters(const symla_gpu_ctx* c, const LevelLists& L, int level) {
+  const int seen = level < static_cast<int>(c->level_iters.size()) ? c->level_iters[level] : 0;
+  return std::max(L.panels, seen);
+}
 
 void launch_level(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
                   const int* d_small, const int* d_large, const int* d_tasks) {
-  launch_level_planned(c, L, level, ko, dynamic, d_small, d_large, d_tasks, L.panels);
-  if (!L.large.empty()) complete_level(c, L, level, ko, dynamic, d_large);
+  const int iters = level_plan_iters(c, L, level);
+  launch_level_planned(c, L, level, ko, dynamic, d_small, d_large, d_tasks, iters);
+  if (!L.large.empty()) complete_level(c, L, level, ko, dynamic, d_large, iters);
   CK(cudaGetLastError());
 }
 
@@ -777,7 +788,7 @@ void launch_level(symla_gpu_ctx* c, const LevelLists& L, int level, const Kernel
 // panels that stop at a failing pivot can leave a front unfinished after
 // the planned iterations: run more until done.
 void complete_level(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
-                    const int* d_large) {
+                    const int* d_large, int launched) {
   cudaStream_t st = c->stream;
   {
     const int nl = static_cast<int>(L.large.size());
@@ -794,30 +805,41 @@ void complete_level(symla_gpu_ctx* c, const LevelLists& L, int level, const Kern
       if (!dynamic && gl.delay_level < level) break;  // aborted level, re-run by the delay path
       if (++guard > 4 * L.panels + 64) throw SymlaError(SYMLA_ERR_INTERNAL, "large front did not finish");
       for (int it = 0; it < 4; ++it) launch_panel_iteration(c, L, level, ko, dynamic, d_large);
+      launched += 4;
     }
   }
+  if (level < static_cast<int>(c->level_iters.size()))
+    c->level_iters[level] = std::max(c->level_iters[level], std::min(launched, 4 * L.panels + 64));
   CK(cudaGetLastError());
 }
 
 // Graph launch of the static pass: every level with its planned panel
-// iterations plus slack, each level marking itself if a front is still
-// unfinished (the later levels then return at once). Captured once per set
-// of kernel options and replayed; no host synchronisation inside.
-int graph_iters(const LevelLists& L) { return L.panels + L.panels / 4 + 2; }
+// iterations (or the most an earlier factorization needed) plus slack, each
+// level marking itself if a front is still unfinished (the later levels then
+// return at once). Captured once per set of kernel options and iteration
+// counts and replayed; no host synchronisation inside. A level that ran past
+// its count raises it, so the next factorization recaptures with room.
+int graph_iters(const symla_gpu_ctx* c, const LevelLists& L, int level) {
+  const int n = level_plan_iters(c, L, level);
+  return n + n / 8 + 2;
+}
 
 void run_static_pass_graph(symla_gpu_ctx* c, const KernelOpts& ko) {
   cudaStream_t st = c->stream;
-  const bool same = c->graph_exec && std::memcmp(&c->graph_ko, &ko, sizeof ko) == 0;
+  std::vector<int> iters(c->numLevels);
+  for (int l = 0; l < c->numLevels; ++l) iters[l] = graph_iters(c, c->levels[l], l);
+  const bool same = c->graph_exec && std::memcmp(&c->graph_ko, &ko, sizeof ko) == 0 && iters == c->graph_level_iters;
   if (!same) {
     if (c->graph_exec) {
       cudaGraphExecDestroy(c->graph_exec);
       c->graph_exec = nullptr;
     }
     cudaGraph_t graph = nullptr;
+    const long long counted = c->launches;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     for (int l = 0; l < c->numLevels; ++l) {
       const LevelLists& L = c->levels[l];
-      launch_level_planned(c, L, l, ko, 0, L.d_small, L.d_large, L.d_tasks, graph_iters(L));
+      launch_level_planned(c, L, l, ko, 0, L.d_small, L.d_large, L.d_tasks, iters[l]);
       if (!L.large.empty())
         launch_mark_unfinished(c->d_state, L.d_large, static_cast<int>(L.large.size()), c->d_glob, l, st);
     }
@@ -826,13 +848,27 @@ void run_static_pass_graph(symla_gpu_ctx* c, const KernelOpts& ko) {
       if (graph) cudaGraphDestroy(graph);
       CK(ec);
     }
+    // the captured launches run at every replay, not at the capture
+    c->launches = counted;
+    size_t nodes = 0;
+    c->graph_kernels = 0;
+    if (cudaGraphGetNodes(graph, nullptr, &nodes) == cudaSuccess && nodes > 0) {
+      std::vector<cudaGraphNode_t> list(nodes);
+      if (cudaGraphGetNodes(graph, list.data(), &nodes) == cudaSuccess)
+        for (size_t i = 0; i < nodes; ++i) {
+          cudaGraphNodeType t;
+          if (cudaGraphNodeGetType(list[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++c->graph_kernels;
+        }
+    }
     const cudaError_t ei = cudaGraphInstantiate(&c->graph_exec, graph, 0);
     cudaGraphDestroy(graph);
     CK(ei);
     c->graph_ko = ko;
+    c->graph_level_iters = iters;
     ++c->graph_captures;
   }
   CK(cudaGraphLaunch(c->graph_exec, st));
+  c->launches += c->graph_kernels;
 }
 
 // Re-plan front s whose children delayed columns (multifrontal.hpp:453-479)
@@ -968,7 +1004,7 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
       const int none = INT_MAX;
       CK(cudaMemcpyAsync(&c->d_glob->unfinished_level, &none, sizeof none, cudaMemcpyHostToDevice, st));
       ++c->graph_resumes;
-      complete_level(c, c->levels[u], u, ko, 0, c->levels[u].d_large);
+      complete_level(c, c->levels[u], u, ko, 0, c->levels[u].d_large, c->graph_level_iters[u]);
       for (int l = u + 1; l < c->numLevels; ++l) {
         const LevelLists& L = c->levels[l];
         launch_level(c, L, l, ko, 0, L.d_small, L.d_large, L.d_tasks);

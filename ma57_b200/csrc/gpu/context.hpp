@@ -185,6 +185,10 @@ struct symla_gpu_ctx {
   cudaGraphExec_t graph_exec = nullptr;
   symla_gpu::KernelOpts graph_ko{};
   int graph_captures = 0, graph_resumes = 0;
+  long long graph_kernels = 0;  // kernel nodes of the captured graph (counted per replay)
+  // panel iterations per level: the most any factorization of this plan
+  // needed (0: within the plan), and the counts the captured graph holds
+  std::vector<int> level_iters, graph_level_iters;
 
   // instrumentation
   bool profiling = false;

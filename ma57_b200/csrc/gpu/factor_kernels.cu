@@ -14,6 +14,7 @@
 // both triangles and re-averages them after every update
 // (dense_kernel.hpp:269-297), which is a no-op for a computation that forms
 // each symmetric entry once.
+#include <algorithm>
 #include <cfloat>
 #include <climits>
 #include <cmath>
@@ -849,8 +850,7 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* _
 // every front of the level (one tile space), the K range staged 32 pivots
 // at a time.
 namespace {
-constexpr int kTT = 128;        // tile edge
-constexpr int kKC = 32;         // K chunk
+constexpr int kTT = 128;        // tile height (rows)
 constexpr int kMaxUpdateFronts = 1024;  // fronts per update launch
 }  // namespace
 
@@ -882,30 +882,34 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// Tiles of front s's update region: column tiles over [c0, c1), each with
-// row tiles from its diagonal down to m.
-__device__ __forceinline__ int update_tiles(int m, int c0, int c1) {
+// Tiles of front s's update region: column tiles of width tj over [c0, c1),
+// each with kTT-row tiles from its diagonal down to m.
+__device__ __forceinline__ int update_tiles(int m, int c0, int c1, int tj) {
   int n = 0;
-  for (int j = c0; j < c1; j += kTT) n += (m - j + kTT - 1) / kTT;
+  for (int j = c0; j < c1; j += tj) n += (m - j + kTT - 1) / kTT;
   return n;
 }
 
 // ---------------------------------------------------------------------------
 // The near / far updates on the FP64 tensor path: mma.sync m16n8k8 .f64
-// (DMMA; the 5th-gen tcgen05 MMA has no FP64 kind). 128 x 128 tiles, 16 warps
-// of 32 x 32 (2 x 4 MMA tiles, 4 accumulators each per lane; four warps per
-// scheduler hide the shared-memory fragment loads). A chunk of 32
-// pivots of the A rows (L(i, q)) and of the B rows (L(j, q) with one halo
-// column each side, for D's 2 x 2 blocks) is staged pivot-major as in the
-// front (coalesced, conflict-free cp.async) with a 132-double stride, which
-// also makes the fragment loads conflict-free (lanes 0-15 of a 64-bit load
-// hit 16 distinct bank pairs); double-buffered. W(j, q) = -(L D)(j, q) is
-// formed once per chunk in shared memory and the L fragment accumulates onto
-// the C tile held in registers.
+// (DMMA; the 5th-gen tcgen05 MMA has no FP64 kind). 128 x 64 tiles, 8 warps
+// of 32 x 32 (2 x 4 MMA tiles, 4 accumulators each per lane), two CTAs per
+// SM, so that one CTA's C load and store overlap the other's MMAs. A chunk
+// of 16 pivots of the A rows (L(i, q)) and of the B rows (L(j, q) with one
+// halo column each side, for D's 2 x 2 blocks) is staged pivot-major as in
+// the front (coalesced, conflict-free cp.async) with strides of 132 and 68
+// doubles, which also make the fragment loads conflict-free (lanes 0-15 of
+// a 64-bit load hit 16 distinct bank pairs); double-buffered.
+// W(j, q) = -(L D)(j, q) is formed once per chunk in shared memory and the L
+// fragment accumulates onto the C tile held in registers.
 namespace {
-constexpr int kAS = 132;  // pivot-major stride of the staged tiles (doubles)
-constexpr int kMThreads = 512;  // 16 warps of 32 x 32
-constexpr size_t kMmaSmem = static_cast<size_t>(2 * kKC + 2 * (kKC + 2) + kKC) * kAS * sizeof(double);
+constexpr int kTJ = 64;   // column tile width
+constexpr int kKM = 16;   // K chunk
+constexpr int kAS = 132;  // pivot-major stride of the staged A rows (doubles)
+constexpr int kBS = 68;   // pivot-major stride of the staged B rows and W
+constexpr int kMThreads = 256;  // 8 warps of 32 x 32
+constexpr size_t kMmaSmem =
+    static_cast<size_t>(2 * kKM * kAS + 2 * (kKM + 2) * kBS + kKM * kBS) * sizeof(double);
 
 // c (16 x 8) += a (16 x 8) * b (8 x 8); lane (g, t) = (lane >> 2, lane & 3):
 // a_r = A(g + 8 (r & 1), t + 4 (r >> 1)), b_r = B(t + 4 r, g),
@@ -920,34 +924,34 @@ __device__ __forceinline__ void dmma16x8x8(double* c, const double* a, const dou
 // valid inside [q0, q1)) into pivot-major tiles, zero-filled outside.
 __device__ __forceinline__ void mma_stage(const double* F, int64_t ld, int m, int q0, int q1, int kc, int kn, int i0,
                                           int j0, double* As, double* Bs) {
-  for (int t = threadIdx.x; t < kKC * kTT; t += kMThreads) {
+  for (int t = threadIdx.x; t < kKM * kTT; t += kMThreads) {
     const int k = t / kTT, r = t % kTT;
     const int gi = i0 + r;
     const bool ok = k < kn && gi < m;
     cp_async8(As + k * kAS + r, F + (ok ? (kc + k) * ld + gi : 0), ok);
   }
-  for (int t = threadIdx.x; t < (kKC + 2) * kTT; t += kMThreads) {
-    const int kp = t / kTT, r = t % kTT;
+  for (int t = threadIdx.x; t < (kKM + 2) * kTJ; t += kMThreads) {
+    const int kp = t / kTJ, r = t % kTJ;
     const int pq = kc + kp - 1;
     const int gj = j0 + r;
     const bool ok = gj < m && pq >= q0 && pq < q1 && kp <= kn + 1;  // halo: 2 x 2 partners either side
-    cp_async8(Bs + kp * kAS + r, F + (ok ? pq * ld + gj : 0), ok);
+    cp_async8(Bs + kp * kBS + r, F + (ok ? pq * ld + gj : 0), ok);
   }
 }
 }  // namespace
 
 template <int MODE>
-__global__ void __launch_bounds__(kMThreads, 1) update_mma_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
+__global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
                                                                const int* __restrict__ front_list, int count,
                                                                FactorGlobals* g, int level, int dynamic,
                                                                const double* __restrict__ tc_guard) {
   if (level_aborted(g, level, dynamic)) return;
   extern __shared__ double usm[];
-  double* AsBuf[2] = {usm, usm + kKC * kAS};
-  double* BsBuf[2] = {usm + 2 * kKC * kAS, usm + (3 * kKC + 2) * kAS};
-  double* Ws = usm + (4 * kKC + 4) * kAS;
-  __shared__ double dd[kKC], dlo[kKC], dhi[kKC];
-  __shared__ int8_t kk[kKC];
+  double* AsBuf[2] = {usm, usm + kKM * kAS};
+  double* BsBuf[2] = {usm + 2 * kKM * kAS, usm + 2 * kKM * kAS + (kKM + 2) * kBS};
+  double* Ws = usm + 2 * kKM * kAS + 2 * (kKM + 2) * kBS;
+  __shared__ double dd[kKM], dlo[kKM], dhi[kKM];
+  __shared__ int8_t kk[kKM];
   __shared__ int tile_end[2 * kMaxUpdateFronts];
   const int nent = (MODE == 2) ? 2 * count : count;
   auto entry_far = [&](int e) { return MODE == 1 || (MODE == 2 && e >= count); };
@@ -959,7 +963,7 @@ __global__ void __launch_bounds__(kMThreads, 1) update_mma_kernel(const FrontDes
     bool use = update_range(S, fronts[sf].m, far, c0, c1, q0, q1);
     if (far && use && tc_guard && tc_block_ok(q1 - q0, tc_guard[2 * t], tc_guard[2 * t + 1], g->amax))
       use = false;  // the tensor-core kernel applied this block
-    tile_end[t] = use ? update_tiles(fronts[sf].m, c0, c1) : 0;
+    tile_end[t] = use ? update_tiles(fronts[sf].m, c0, c1, kTJ) : 0;
     if (blockIdx.x == 0 && tile_end[t] > 0) {
       const double nc = c1 - c0, mm = fronts[sf].m;
       const double entries = nc * mm - (static_cast<double>(c0) + c1 - 1) * nc / 2.0;
@@ -972,7 +976,7 @@ __global__ void __launch_bounds__(kMThreads, 1) update_mma_kernel(const FrontDes
   __syncthreads();
   const int total = nent > 0 ? tile_end[nent - 1] : 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wr = warp >> 2, wc = warp & 3;          // warp's 32 x 32 sub-tile
+  const int wr = warp >> 1, wc = warp & 1;          // warp's 32 x 32 sub-tile
   const int lg = lane >> 2, lt = lane & 3;          // fragment coordinates
   double tmax = 0.0;
   int cur = -1, s = -1;
@@ -994,19 +998,19 @@ __global__ void __launch_bounds__(kMThreads, 1) update_mma_kernel(const FrontDes
       m = fronts[s].m;
       ld = fronts[s].ld;
       update_range(st[s], m, entry_far(fi), c0, c1, q0, q1);
-      nchunks = (q1 - q0 + kKC - 1) / kKC;
+      nchunks = (q1 - q0 + kKM - 1) / kKM;
     }
     int rem = tile - (fi > 0 ? tile_end[fi - 1] : 0);
     int tj = 0;
     for (;;) {
-      const int nr = (m - (c0 + tj * kTT) + kTT - 1) / kTT;
+      const int nr = (m - (c0 + tj * kTJ) + kTT - 1) / kTT;
       if (rem < nr) break;
       rem -= nr;
       ++tj;
     }
-    const int j0 = c0 + tj * kTT, i0 = j0 + rem * kTT;
+    const int j0 = c0 + tj * kTJ, i0 = j0 + rem * kTT;
     __syncthreads();  // previous tile done with the buffers
-    mma_stage(Fp, ld, m, q0, q1, q0, min(kKC, q1 - q0), i0, j0, AsBuf[0], BsBuf[0]);
+    mma_stage(Fp, ld, m, q0, q1, q0, min(kKM, q1 - q0), i0, j0, AsBuf[0], BsBuf[0]);
     cp_async_commit();
     // C tile into the accumulators (lane holds rows gi0 + 16 rt + 8 v,
     // columns gj0 + 8 ct + h as acc[rt][ct][2 v + h])
@@ -1027,10 +1031,10 @@ __global__ void __launch_bounds__(kMThreads, 1) update_mma_kernel(const FrontDes
           }
       }
     for (int c = 0; c < nchunks; ++c) {
-      const int kc = q0 + c * kKC, kn = min(kKC, q1 - kc);
+      const int kc = q0 + c * kKM, kn = min(kKM, q1 - kc);
       if (c + 1 < nchunks) {
-        const int kc2 = kc + kKC;
-        mma_stage(Fp, ld, m, q0, q1, kc2, min(kKC, q1 - kc2), i0, j0, AsBuf[(c + 1) & 1], BsBuf[(c + 1) & 1]);
+        const int kc2 = kc + kKM;
+        mma_stage(Fp, ld, m, q0, q1, kc2, min(kKM, q1 - kc2), i0, j0, AsBuf[(c + 1) & 1], BsBuf[(c + 1) & 1]);
       }
       cp_async_commit();
       if (threadIdx.x < kn) {
@@ -1049,16 +1053,16 @@ __global__ void __launch_bounds__(kMThreads, 1) update_mma_kernel(const FrontDes
       // W(j, q) = -(L D)(j, q); zero past the chunk (the MMAs run over
       // 8-pivot steps; A is zero-filled past kn)
       const int kn8 = (kn + 7) & ~7;
-      for (int t = threadIdx.x; t < kn8 * kTT; t += kMThreads) {
-        const int q = t / kTT, r = t % kTT;
+      for (int t = threadIdx.x; t < kn8 * kTJ; t += kMThreads) {
+        const int q = t / kTJ, r = t % kTJ;
         double w = 0.0;
         if (q < kn) {
-          const double* col = Bs + (q + 1) * kAS + r;
+          const double* col = Bs + (q + 1) * kBS + r;
           w = dd[q] * col[0];
-          if (kk[q] == 1) w += dhi[q] * col[kAS];
-          if (kk[q] == 2) w += dlo[q] * col[-kAS];
+          if (kk[q] == 1) w += dhi[q] * col[kBS];
+          if (kk[q] == 2) w += dlo[q] * col[-kBS];
         }
-        Ws[q * kAS + r] = -w;
+        Ws[q * kBS + r] = -w;
       }
       __syncthreads();
       for (int k0 = 0; k0 < kn8; k0 += 8) {
@@ -1066,7 +1070,7 @@ __global__ void __launch_bounds__(kMThreads, 1) update_mma_kernel(const FrontDes
 #pragma unroll
         for (int ct = 0; ct < 4; ++ct)
 #pragma unroll
-          for (int r = 0; r < 2; ++r) b[ct][r] = Ws[(k0 + lt + 4 * r) * kAS + wc * 32 + ct * 8 + lg];
+          for (int r = 0; r < 2; ++r) b[ct][r] = Ws[(k0 + lt + 4 * r) * kBS + wc * 32 + ct * 8 + lg];
 #pragma unroll
         for (int rt = 0; rt < 2; ++rt) {
           double a[4];
@@ -1172,6 +1176,7 @@ void launch_update(bool far, const FrontDesc* fronts, FrontState* st, const int*
                    FactorGlobals* g, int level, int dynamic, cudaStream_t stream, const double* tc_guard) {
   if (count <= 0 || grid_x <= 0) return;
   const size_t sm = kMmaSmem;
+  grid_x = std::min(2 * grid_x, 2 * 148);  // two 128 x 64 tiles per 128 x 128, two CTAs per SM
   for (int b = 0; b < count; b += kMaxUpdateFronts) {
     const int cnt = count - b < kMaxUpdateFronts ? count - b : kMaxUpdateFronts;
     if (far)
@@ -1187,6 +1192,7 @@ void launch_update_both(const FrontDesc* fronts, FrontState* st, const int* list
                         FactorGlobals* g, int level, int dynamic, cudaStream_t stream) {
   if (count <= 0 || grid_x <= 0) return;
   const size_t sm = kMmaSmem;
+  grid_x = std::min(2 * grid_x, 2 * 148);  // two 128 x 64 tiles per 128 x 128, two CTAs per SM
   for (int b = 0; b < count; b += kMaxUpdateFronts) {
     const int cnt = count - b < kMaxUpdateFronts ? count - b : kMaxUpdateFronts;
     update_mma_kernel<2><<<grid_x, kMThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic, nullptr);

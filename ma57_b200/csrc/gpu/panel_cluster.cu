@@ -26,9 +26,9 @@
 // for D and the L rows of the block), then its own rows below the block in
 // one pass with no per-pivot synchronisation; the per-pivot partial lambdas
 // cross the cluster once. The pivots before the first one that fails are
-// accepted (identical values and decisions to the sequential path); if the
-// very first pivot fails, the sequential path takes over for one decision
-// (or for the whole panel after repeated failures).
+// accepted (identical values and decisions to the sequential path), and
+// the same launch finishes the panel on the sequential path from the first
+// failing pivot (measured: cheaper than a new panel + update launch pair).
 #include <cooperative_groups.h>
 
 #include <cmath>
@@ -48,7 +48,6 @@ constexpr int kCT = 256;                           // threads per CTA
 constexpr int kNBMax = 34;                         // panel width + 2
 constexpr int kSpecMax = 32;                       // pivots per speculative panel (= panel width)
 constexpr int kSpecRetry = 2;                      // consecutive failures before a whole sequential panel
-constexpr int kSeqFinish = 12;                     // pivots left that the sequential path finishes in-launch
 
 struct ClusterShared {
   double w[kNBMax];     // D * L(k, :)^T for the current pivot row
@@ -263,7 +262,6 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
   // ---- speculative panel: 1x1 pivots at k, verified against lambda after
   // the fact (see the file comment)
   int spec = S.spec;
-  int seq_limit = 1 << 30;  // sequential decisions allowed in this panel
   bool run_seq = true;
   int spec_kind = 0;  // 0 no speculation, 1 all accepted, 2 a prefix, 3 none
   const int np = pe - ps;
@@ -475,18 +473,14 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
           sh.w[threadIdx.x] = sh.wv[kstar][threadIdx.x];
         }
         __syncthreads();
-        run_seq = true;
-        // finish the panel here when little of it is left, else take the
-        // failing pivot's decision and speculate again in the next launch
-        seq_limit = (np - kstar <= kSeqFinish) ? np - kstar : 1;
+        run_seq = true;  // finish the panel here
       }
     } else {
-      seq_limit = (np <= kSeqFinish) ? np : 1;  // the first pivot needs the sequential decision
-      spec += 1;
+      spec += 1;  // the whole panel on the sequential path
       spec_kind = 3;
     }
   }
-  int decisions = 0, nontrivial = 0;
+  int nontrivial = 0;
   // prefetched raw values of column k for this thread's rows
   constexpr int kPF = 4;
   double pf[kPF];
@@ -562,8 +556,6 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
   };
 
   while (run_seq && k < pe) {
-    if (decisions >= seq_limit) break;
-    ++decisions;
     const int p = k - ps;
     const int b = step & 1;
     ++step;

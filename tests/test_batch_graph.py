@@ -27,11 +27,17 @@ def test_graph_launch_matches_stream_launch_bitwise(k):
         s.setGraphLaunch(graph)
         s.analyzePattern(A)
         s.factorize(A)
-        s.refactorize(A)  # second factorization replays the captured graph
-        xs.append((s.inertia().as_tuple(), s.solve(b), s.graphStats()))
+        # a level that ran past its planned iterations raises its count, so
+        # the next factorization recaptures once; the one after replays
+        s.refactorize(A)
+        first = s.graphStats()
+        s.refactorize(A)
+        xs.append((s.inertia().as_tuple(), s.solve(b), s.graphStats(), first))
     assert xs[0][0] == xs[1][0]
     np.testing.assert_array_equal(xs[0][1], xs[1][1])
-    assert xs[1][2]["captures"] == 1
+    assert 1 <= xs[1][3]["captures"] <= 2
+    assert xs[1][2]["captures"] == xs[1][3]["captures"]  # replayed, not recaptured
+    assert xs[1][2]["resumes"] == xs[1][3]["resumes"]  # and ran within the graph
     assert xs[0][2]["captures"] == 0
 
 
