@@ -280,7 +280,7 @@ void build_level_lists(symla_gpu_ctx* c, const std::vector<int>& frontsOfLevel, 
       tiles = std::max(tiles, nt * (nt + 1) / 2);
     }
   }
-  if (!L.large.empty() && L.tasks.size() / 4 < 2 * 148) {
+  if (!L.large.empty() && L.tasks.size() / 4 < 4 * 148) {
     // too few (front, 32 columns) assembly tasks to fill the GPU: split
     // their rows into chunks
     std::vector<int> split;

@@ -66,13 +66,13 @@ __device__ __forceinline__ int a_local_row(int pos, int ncols, int nextra) {
 // block's own columns and rows are added. The children's map pointers, contribution-block
 // origins and their maps of the block's 32 columns are staged in shared
 // memory once; each thread then takes rows, reads a row's position in each
-// child once and issues the (independent) loads of all 32 columns, summing
-// over the children in their fixed order.
+// child once and issues the (independent) loads of 16 of the 32 columns,
+// summing over the children in their fixed order.
 namespace {
 constexpr int kAsmMaxChildren = 16;
 }
 
-__global__ void __launch_bounds__(256) assemble_kernel(const FrontDesc* __restrict__ fronts,
+__global__ void __launch_bounds__(256, 4) assemble_kernel(const FrontDesc* __restrict__ fronts,
                                                        const ChildLink* __restrict__ links,
                                                        FrontState* st, const int* __restrict__ tasks,
                                                        const int* __restrict__ a_colptr, KernelOpts o,
@@ -104,27 +104,32 @@ __global__ void __launch_bounds__(256) assemble_kernel(const FrontDesc* __restri
       s_b[c][jj] = (jj < nj) ? s_inv[c][j0 + jj] : -1;
     }
     __syncthreads();
-    for (int i = i0 + threadIdx.x; i < iend; i += blockDim.x) {
-      double acc[32];
+    // warp w takes columns j0 + 16 (w & 1) .. + 16 of rows 32 (w >> 1) + lane
+    // + 128 t: half a row's loads per thread keeps the registers low enough
+    // for four CTAs per SM (the gather is load-latency-bound)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int h0 = 16 * (warp & 1);
+    for (int i = i0 + 32 * (warp >> 1) + lane; i < iend; i += 128) {
+      double acc[16];
 #pragma unroll
-      for (int jj = 0; jj < 32; ++jj) acc[jj] = 0.0;
+      for (int jj = 0; jj < 16; ++jj) acc[jj] = 0.0;
       for (int c = 0; c < nch; ++c) {
         const int a = s_inv[c][i];
         if (a < 0) continue;
         const double* cb = s_cb[c];
         const int64_t cld = s_ld[c];
 #pragma unroll
-        for (int jj = 0; jj < 32; ++jj) {
-          const int b = s_b[c][jj];
-          if (b >= 0 && j0 + jj <= i) {
+        for (int jj = 0; jj < 16; ++jj) {
+          const int b = s_b[c][h0 + jj];
+          if (b >= 0 && j0 + h0 + jj <= i) {
             const int r = a > b ? a : b, cc = a > b ? b : a;
             acc[jj] += cb[static_cast<int64_t>(cc) * cld + r];
           }
         }
       }
 #pragma unroll
-      for (int jj = 0; jj < 32; ++jj)
-        if (jj < nj && j0 + jj <= i) f.F[static_cast<int64_t>(j0 + jj) * f.ld + i] = acc[jj];
+      for (int jj = 0; jj < 16; ++jj)
+        if (h0 + jj < nj && j0 + h0 + jj <= i) f.F[static_cast<int64_t>(j0 + h0 + jj) * f.ld + i] = acc[jj];
     }
   } else {
     for (int j = j0; j < j1; ++j) {
