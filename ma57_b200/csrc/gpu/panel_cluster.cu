@@ -89,6 +89,9 @@ __device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc) 
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// wait until at most the newest group of this thread's copies is in flight
+__device__ __forceinline__ void cp_async_wait_but_newest() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 }  // namespace
 
@@ -271,7 +274,14 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     // raw diagonal block (lower triangle)
     for (int j = 0; j < np; ++j)
       for (int i = j + threadIdx.x; i < np; i += kCT) cp_async8(&sh.db[i][j], F + static_cast<int64_t>(ps + j) * ld + ps + i);
-    cp_async_wait_all();
+    cp_async_commit();
+    // the raw panel columns of this CTA's rows below the block go to Lr
+    // while warp 0 factors the diagonal block
+    for (int c = 0; c < np; ++c)
+      for (int i = r0 + threadIdx.x; i < rend; i += kCT)
+        cp_async8(Lr + c * R + (i - base), F + static_cast<int64_t>(ps + c) * ld + i);
+    cp_async_commit();
+    cp_async_wait_but_newest();
     __syncthreads();
     // diagonal block, left-looking: warp 0 of every CTA, lane = row (the
     // row lives in sh.db, conflict-free with the odd row stride). The sums
@@ -341,15 +351,12 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
       sh.rmd[c] = rv;
     }
     // rows below the block, left-looking: the raw panel columns of this
-    // CTA's rows are staged in Lr, then each thread takes one row at a time
+    // CTA's rows are in Lr (staged above), then each thread takes one row at a time
     // into registers and walks it pivot by pivot, touching only its own
     // rows, so no synchronisation is needed between pivots; the L(c, t) are
     // warp-uniform (broadcast) shared loads. Lr receives the current values
     // a_ic = raw_ic - sum_t a_it L_ct (L = a_ic / d_c on write-back). Columns
     // past np compute unused values (column c depends on columns t < c only).
-    for (int c = 0; c < np; ++c)
-      for (int i = r0 + threadIdx.x; i < rend; i += kCT)
-        cp_async8(Lr + c * R + (i - base), F + static_cast<int64_t>(ps + c) * ld + i);
     cp_async_wait_all();
     __syncthreads();
     for (int i = r0 + threadIdx.x; i < rend; i += kCT) {

@@ -100,3 +100,33 @@ def test_learned_delta_cuts_retries_on_nonconvex_sequence():
     assert np.mean(with_model) <= 0.5 * np.mean(plain)
     for a, b in zip(model_res, plain_res):
         assert a <= max(10 * b, 1e-10)
+
+
+def test_failed_learned_attempt_resumes_escalation_above_it():
+    """A per-front first attempt that fails the inertia check costs one
+    attempt: the escalation resumes one growth step above the smallest
+    delta it used, not from the initial delta."""
+    seq = M.InteriorPointSequence(k=10, steps=60, curvature_shift=6.0)
+    K, _ = seq.matrix(0)
+    base = 1e-14 * abs(K.data).max()
+
+    def run(front):
+        s = SymLDLT()
+        s.setMode(Mode.StaticRegularized)
+        s.setOrdering(OrderingType.AMD)
+        s.setKKTBlockSizes(seq.n1, seq.n2)
+        s.setMaxRegularizationRetries(40)
+        s.analyzePattern(K)
+        s.setInitialRegularizationDelta(base)
+        if front is not None:
+            s.setFrontDeltas(np.full(len(s.symbolicFactor().supernodes), front))
+        s.factorize(K)
+        return s.regularizationRetriesUsed(), s.lastRegularizationDelta(), s.inertia().as_tuple()
+
+    plain_retries, plain_delta, inertia = run(None)
+    assert plain_retries >= 5
+    # first attempt three decades above the initial delta, still too small
+    retries, delta, inertia2 = run(base * 1e3)
+    assert inertia2 == inertia == (seq.n2, seq.n1, 0)
+    assert retries == plain_retries - 3
+    assert delta == pytest.approx(plain_delta, rel=1e-9)
