@@ -154,17 +154,18 @@ def panel_bytes(k):
     return b
 
 
-def profiled_traffic(kind):
-    """DRAM bytes per launch of a kernel kind from the committed ncu summary
-    (profiles/traffic.md: lines 'kind: <kind> dram_bytes_per_launch: <N>'),
-    or None."""
+def profiled_traffic(kind, units_per_launch):
+    """DRAM bytes per launch of a kernel kind, from the committed ncu summary
+    (profiles/traffic.md: lines 'kind: <kind> dram_bytes_per_unit: <r>', r =
+    measured DRAM bytes of the captured launch / its algorithmic units, flops
+    or bytes), scaled to this run's algorithmic units per launch; or None."""
     path = os.path.join(ROOT, "profiles", "traffic.md")
     try:
         with open(path) as f:
             for line in f:
                 parts = line.replace("`", "").split()
-                if len(parts) >= 4 and parts[0] == "kind:" and parts[1] == kind and parts[2] == "dram_bytes_per_launch:":
-                    return float(parts[3])
+                if len(parts) >= 4 and parts[0] == "kind:" and parts[1] == kind and parts[2] == "dram_bytes_per_unit:":
+                    return float(parts[3]) * units_per_launch
     except OSError:
         pass
     return None
@@ -552,7 +553,8 @@ def run_ours(args):
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "peak_source": f"HBM copy, {peak_kind}",
                     "algorithmic_bytes_per_launch": bytes_k / max(1, launches_k)}
-    roofline.update({"frac": achieved / peak if peak else None, "traffic": profiled_traffic(dom), "kernel": dom,
+    units = (flops_k if roofline["unit"] == "TFLOP/s" else bytes_k) / max(1, launches_k)
+    roofline.update({"frac": achieved / peak if peak else None, "traffic": profiled_traffic(dom, units), "kernel": dom,
                      "launches_per_step": launches_k / steps, "ms_per_step": ms_k / steps,
                      "avg_launch_us": 1e3 * ms_k / max(1, launches_k)})
 

@@ -124,9 +124,10 @@ def test_failed_learned_attempt_resumes_escalation_above_it():
         return s.regularizationRetriesUsed(), s.lastRegularizationDelta(), s.inertia().as_tuple()
 
     plain_retries, plain_delta, inertia = run(None)
-    assert plain_retries >= 5
-    # first attempt three decades above the initial delta, still too small
-    retries, delta, inertia2 = run(base * 1e3)
+    assert plain_retries >= 2
+    # a first attempt j decades above the initial delta, still too small
+    j = max(1, plain_retries - 2)
+    retries, delta, inertia2 = run(base * 10.0**j)
     assert inertia2 == inertia == (seq.n2, seq.n1, 0)
-    assert retries == plain_retries - 3
+    assert retries == plain_retries - j
     assert delta == pytest.approx(plain_delta, rel=1e-9)
