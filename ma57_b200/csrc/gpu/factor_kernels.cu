@@ -904,7 +904,8 @@ __device__ __forceinline__ int update_tiles(int m, int c0, int c1, int tj) {
 // halo column each side, for D's 2 x 2 blocks) is staged pivot-major as in
 // the front (coalesced, conflict-free cp.async) with strides of 132 and 68
 // doubles, which also make the fragment loads conflict-free (lanes 0-15 of
-// a 64-bit load hit 16 distinct bank pairs); double-buffered.
+// a 64-bit load hit 16 distinct bank pairs); a ring of three stages keeps
+// two chunks in flight.
 // W(j, q) = -(L D)(j, q) is formed once per chunk in shared memory and the L
 // fragment accumulates onto the C tile held in registers.
 namespace {
@@ -913,8 +914,9 @@ constexpr int kKM = 16;   // K chunk
 constexpr int kAS = 132;  // pivot-major stride of the staged A rows (doubles)
 constexpr int kBS = 68;   // pivot-major stride of the staged B rows and W
 constexpr int kMThreads = 256;  // 8 warps of 32 x 32
+constexpr int kMStages = 3;  // staging ring depth (two chunks in flight)
 constexpr size_t kMmaSmem =
-    static_cast<size_t>(2 * kKM * kAS + 2 * (kKM + 2) * kBS + kKM * kBS) * sizeof(double);
+    static_cast<size_t>(kMStages * (kKM * kAS + (kKM + 2) * kBS) + kKM * kBS) * sizeof(double);
 
 // c (16 x 8) += a (16 x 8) * b (8 x 8); lane (g, t) = (lane >> 2, lane & 3):
 // a_r = A(g + 8 (r & 1), t + 4 (r >> 1)), b_r = B(t + 4 r, g),
@@ -952,9 +954,10 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
                                                                const double* __restrict__ tc_guard) {
   if (level_aborted(g, level, dynamic)) return;
   extern __shared__ double usm[];
-  double* AsBuf[2] = {usm, usm + kKM * kAS};
-  double* BsBuf[2] = {usm + 2 * kKM * kAS, usm + 2 * kKM * kAS + (kKM + 2) * kBS};
-  double* Ws = usm + 2 * kKM * kAS + 2 * (kKM + 2) * kBS;
+  // stage b of the ring: A rows at As_of(b), B rows at Bs_of(b)
+  auto As_of = [&](int b) { return usm + b * kKM * kAS; };
+  auto Bs_of = [&](int b) { return usm + kMStages * kKM * kAS + b * (kKM + 2) * kBS; };
+  double* Ws = usm + kMStages * (kKM * kAS + (kKM + 2) * kBS);
   __shared__ double dd[kKM], dlo[kKM], dhi[kKM];
   __shared__ int8_t kk[kKM];
   __shared__ int tile_end[2 * kMaxUpdateFronts];
@@ -1015,7 +1018,9 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
     }
     const int j0 = c0 + tj * kTJ, i0 = j0 + rem * kTT;
     __syncthreads();  // previous tile done with the buffers
-    mma_stage(Fp, ld, m, q0, q1, q0, min(kKM, q1 - q0), i0, j0, AsBuf[0], BsBuf[0]);
+    mma_stage(Fp, ld, m, q0, q1, q0, min(kKM, q1 - q0), i0, j0, As_of(0), Bs_of(0));
+    cp_async_commit();
+    if (nchunks > 1) mma_stage(Fp, ld, m, q0, q1, q0 + kKM, min(kKM, q1 - q0 - kKM), i0, j0, As_of(1), Bs_of(1));
     cp_async_commit();
     // C tile into the accumulators (lane holds rows gi0 + 16 rt + 8 v,
     // columns gj0 + 8 ct + h as acc[rt][ct][2 v + h])
@@ -1037,11 +1042,12 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
       }
     for (int c = 0; c < nchunks; ++c) {
       const int kc = q0 + c * kKM, kn = min(kKM, q1 - kc);
-      if (c + 1 < nchunks) {
-        const int kc2 = kc + kKM;
-        mma_stage(Fp, ld, m, q0, q1, kc2, min(kKM, q1 - kc2), i0, j0, AsBuf[(c + 1) & 1], BsBuf[(c + 1) & 1]);
+      if (c + 2 < nchunks) {
+        const int kc2 = kc + 2 * kKM;
+        mma_stage(Fp, ld, m, q0, q1, kc2, min(kKM, q1 - kc2), i0, j0, As_of((c + 2) % kMStages),
+                  Bs_of((c + 2) % kMStages));
       }
-      cp_async_commit();
+      cp_async_commit();  // (possibly empty) group c + 2
       if (threadIdx.x < kn) {
         const int pq = kc + threadIdx.x;
         const FrontDesc& fd = fronts[s];
@@ -1051,10 +1057,10 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
         dlo[threadIdx.x] = (kind == 2) ? fd.Do[pq - 1] : 0.0;
         dhi[threadIdx.x] = (kind == 1) ? fd.Do[pq] : 0.0;
       }
-      cp_async_wait<1>();
+      cp_async_wait<2>();  // chunk c landed; c + 1 and c + 2 may be in flight
       __syncthreads();
-      const double* As = AsBuf[c & 1];
-      const double* Bs = BsBuf[c & 1];
+      const double* As = As_of(c % kMStages);
+      const double* Bs = Bs_of(c % kMStages);
       // W(j, q) = -(L D)(j, q); zero past the chunk (the MMAs run over
       // 8-pivot steps; A is zero-filled past kn)
       const int kn8 = (kn + 7) & ~7;
