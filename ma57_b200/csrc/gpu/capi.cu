@@ -296,7 +296,9 @@ void build_level_lists(symla_gpu_ctx* c, const std::vector<int>& frontsOfLevel, 
     L.tasks.swap(split);
   }
   if (!L.large.empty()) {
-    // one grid over the tiles of every front of the level (one CTA per SM)
+    // one grid over the tiles of every front of the level, in 128 x 128
+    // tiles up to one per SM (the update launchers double it: 128 x 64 tiles,
+    // two CTAs per SM)
     L.trailing_grid = std::max(1, std::min(tiles * static_cast<int>(L.large.size()), 148));
   } else {
     L.trailing_grid = 0;

@@ -851,9 +851,8 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* _
 //        pivots [ps, k1) of the panel;
 //   far  (after an outer block, a flush or the last panel): columns
 //        [max(ob_end, k1), m), pivots [ob, k1) of the whole block.
-// C(i, j) -= sum_q L(i, q) (L D)(j, q) for i >= j, over 128 x 128 tiles of
-// every front of the level (one tile space), the K range staged 32 pivots
-// at a time.
+// C(i, j) -= sum_q L(i, q) (L D)(j, q) for i >= j, over the tiles of every
+// front of the level (one tile space).
 namespace {
 constexpr int kTT = 128;        // tile height (rows)
 constexpr int kMaxUpdateFronts = 1024;  // fronts per update launch
