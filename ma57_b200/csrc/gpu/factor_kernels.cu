@@ -588,7 +588,7 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* _
   const FrontDesc f = fronts[s];
   FrontState S = st[s];
   if (S.flags & kFlagDone) {
-    // no panel this round: the updates that follow must do nothing
+    // no panel in this iteration: the updates that follow must do nothing
     if (threadIdx.x == 0) {
       st[s].panel_start = S.k;
       st[s].far = 0;
