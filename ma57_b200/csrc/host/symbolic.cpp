@@ -81,18 +81,10 @@ std::vector<int> computeOrdering(const CscPattern& sym, OrderingType type) {
   throw std::invalid_argument("symla::computeOrdering: unknown OrderingType");
 }
 
-EliminationTree buildEliminationTree(const CscPattern& P, std::vector<std::vector<int>>* rowPatterns) {
-  const int n = P.n;
-  EliminationTree tree;
-  tree.n = n;
-  tree.parent.assign(n, -1);
-  tree.colCount.assign(n, 0);
-  if (n == 0) {
-    if (rowPatterns) rowPatterns->clear();
-    return tree;
-  }
+std::vector<int> eliminationTreeParent(const CscPattern& P) {
   // elimination_tree.hpp:78-96 -- Liu's algorithm with path compression.
-  std::vector<int> ancestor(n, -1);
+  const int n = P.n;
+  std::vector<int> parent(n, -1), ancestor(n, -1);
   for (int j = 0; j < n; ++j) {
     for (int idx = P.colPtr[j]; idx < P.colPtr[j + 1]; ++idx) {
       const int i = P.rowIdx[idx];
@@ -105,14 +97,31 @@ EliminationTree buildEliminationTree(const CscPattern& P, std::vector<std::vecto
       }
       if (ancestor[r] == -1) {
         ancestor[r] = j;
-        tree.parent[r] = j;
+        parent[r] = j;
       }
     }
   }
-  // elimination_tree.hpp:98-131 -- Struct(L*j) = (Struct(A*j) ∩ {i>j}) ∪
-  // children's patterns minus the child itself. Computed with a marker array
-  // and one sort per column (the set is unique, so the result is identical
-  // to the reference's repeated set_union).
+  return parent;
+}
+
+EliminationTree columnStructure(const CscPattern& P, std::vector<Supernode>* fundamental,
+                                std::vector<Supernode>* groups) {
+  // Struct(L*j) = (Struct(A*j) ∩ {i>j}) ∪ children's structures minus the
+  // child itself (elimination_tree.hpp:98-131), formed by merging sorted
+  // lists: the column's own entries below
+  // the diagonal (sorted in P) and each child's structure without the child
+  // (sorted, all >= j). A column's structure lives only until its parent has
+  // consumed it; what the callers need of it is kept on the way:
+  //  - fundamental: the supernodes of symbolic.hpp:229-247 (column j
+  //    continues the previous one's iff parent[j-1] == j and colCount[j-1]
+  //    == colCount[j] + 1), each with its first column's structure;
+  //  - groups: for given contiguous column groups, the sorted union of their
+  //    columns' structures (symbolic.hpp:385-396) as each group's rowPattern.
+  const int n = P.n;
+  EliminationTree tree;
+  tree.n = n;
+  tree.parent = eliminationTreeParent(P);
+  tree.colCount.assign(n, 0);
   std::vector<int> headChild(n, -1), nextSib(n, -1);
   for (int j = n - 1; j >= 0; --j) {
     const int p = tree.parent[j];
@@ -121,36 +130,54 @@ EliminationTree buildEliminationTree(const CscPattern& P, std::vector<std::vecto
       headChild[p] = j;
     }
   }
+  if (fundamental) fundamental->clear();
   std::vector<std::vector<int>> pats(n);
-  std::vector<int> mark(n, -1);
-  std::vector<int> work;
+  std::vector<int> cur, tmp;
+  std::vector<int> mark(n, -1), gwork;
+  size_t g = 0;  // current group
   for (int j = 0; j < n; ++j) {
-    work.clear();
-    work.push_back(j);
-    mark[j] = j;
-    for (int idx = P.colPtr[j]; idx < P.colPtr[j + 1]; ++idx) {
-      const int i = P.rowIdx[idx];
-      if (i > j && mark[i] != j) {
-        mark[i] = j;
-        work.push_back(i);
-      }
+    cur.assign(1, j);
+    {
+      const int* b = P.rowIdx.data() + P.colPtr[j];
+      const int* e = P.rowIdx.data() + P.colPtr[j + 1];
+      cur.insert(cur.end(), std::upper_bound(b, e, j), e);
     }
     for (int c = headChild[j]; c != -1; c = nextSib[c]) {
       const auto& cp = pats[c];
-      for (size_t t = 1; t < cp.size(); ++t) {
-        const int i = cp[t];
-        if (mark[i] != j) {
-          mark[i] = j;
-          work.push_back(i);
-        }
-      }
-      if (!rowPatterns) std::vector<int>().swap(pats[c]);
+      tmp.clear();
+      std::set_union(cur.begin(), cur.end(), cp.begin() + 1, cp.end(), std::back_inserter(tmp));
+      cur.swap(tmp);
+      std::vector<int>().swap(pats[c]);
     }
-    std::sort(work.begin(), work.end());
-    tree.colCount[j] = static_cast<int>(work.size());
-    pats[j] = work;
+    tree.colCount[j] = static_cast<int>(cur.size());
+    if (fundamental) {
+      const bool continues = j > 0 && tree.parent[j - 1] == j && tree.colCount[j - 1] == tree.colCount[j] + 1;
+      if (continues) {
+        ++fundamental->back().ncols;
+      } else {
+        Supernode sn;
+        sn.firstCol = j;
+        sn.ncols = 1;
+        sn.rowPattern = cur;
+        fundamental->push_back(std::move(sn));
+      }
+    }
+    if (groups && g < groups->size()) {
+      Supernode& G = (*groups)[g];
+      for (int i : cur)
+        if (mark[i] != static_cast<int>(g)) {
+          mark[i] = static_cast<int>(g);
+          gwork.push_back(i);
+        }
+      if (j == G.firstCol + G.ncols - 1) {
+        std::sort(gwork.begin(), gwork.end());
+        G.rowPattern = gwork;
+        gwork.clear();
+        ++g;
+      }
+    }
+    if (tree.parent[j] != -1) pats[j].swap(cur);
   }
-  if (rowPatterns) *rowPatterns = std::move(pats);
   return tree;
 }
 
@@ -194,25 +221,6 @@ std::vector<int> postorder(const std::vector<int>& parent) {
 
 namespace {
 
-std::vector<Supernode> computeFundamentalSupernodes(const EliminationTree& t,
-                                                    const std::vector<std::vector<int>>& patterns) {
-  // symbolic.hpp:229-247
-  std::vector<Supernode> out;
-  const int nn = t.n;
-  int j = 0;
-  while (j < nn) {
-    const int start = j;
-    while (j + 1 < nn && t.parent[j] == j + 1 && t.colCount[j] == t.colCount[j + 1] + 1) ++j;
-    Supernode sn;
-    sn.firstCol = start;
-    sn.ncols = j - start + 1;
-    sn.rowPattern = patterns[start];
-    out.push_back(std::move(sn));
-    ++j;
-  }
-  return out;
-}
-
 std::int64_t storageNnzOf(int ncols, size_t m) {
   const std::int64_t k = ncols;
   const std::int64_t mm = static_cast<std::int64_t>(m);
@@ -239,20 +247,15 @@ SymbolicFactor analyze(int n, const int* colptr, const int* rowind, OrderingType
   CscPattern A0 = permutedSymmetricPattern(sym, newIndexOf);
 
   // Step 3 (symbolic.hpp:212-216)
-  EliminationTree tree0 = buildEliminationTree(A0, nullptr);
-  std::vector<int> postNodes = postorder(tree0.parent);
+  std::vector<int> postNodes = postorder(eliminationTreeParent(A0));
   std::vector<int> finalPerm(n);
   for (int k = 0; k < n; ++k) finalPerm[k] = perm0[postNodes[k]];
   for (int k = 0; k < n; ++k) newIndexOf[finalPerm[k]] = k;
   CscPattern A1 = permutedSymmetricPattern(sym, newIndexOf);
 
-  // Step 4 (symbolic.hpp:222-226)
-  std::vector<std::vector<int>> rowPatterns;
-  EliminationTree tree = buildEliminationTree(A1, &rowPatterns);
-
-  // Step 5
-  std::vector<Supernode> funda = computeFundamentalSupernodes(tree, rowPatterns);
-  std::vector<std::vector<int>>().swap(rowPatterns);
+  // Step 4-5 (symbolic.hpp:222-247)
+  std::vector<Supernode> funda;
+  EliminationTree tree = columnStructure(A1, &funda, nullptr);
   const int numFunda = static_cast<int>(funda.size());
 
   // Step 6a (symbolic.hpp:253-267)
@@ -353,29 +356,10 @@ SymbolicFactor analyze(int n, const int* colptr, const int* rowind, OrderingType
   for (int k = 0; k < n; ++k) combinedPerm[k] = finalPerm[newOrder[k]];
   for (int k = 0; k < n; ++k) newIndexOf[combinedPerm[k]] = k;
   CscPattern A2 = permutedSymmetricPattern(sym, newIndexOf);
-  std::vector<std::vector<int>> rowPatterns2;
-  EliminationTree tree2 = buildEliminationTree(A2, &rowPatterns2);
+  // and Step 6f (symbolic.hpp:385-396): each final supernode's pattern is the
+  // union of its member columns' patterns
+  sf.etree = columnStructure(A2, &sf.fundamentalSupernodes, &finalSupernodes);
   sf.perm = combinedPerm;
-  sf.etree = tree2;
-  sf.fundamentalSupernodes = computeFundamentalSupernodes(tree2, rowPatterns2);
-
-  // Step 6f (symbolic.hpp:385-396): union of member columns' patterns.
-  std::vector<int> mark(n, -1);
-  std::vector<int> work;
-  for (size_t s = 0; s < finalSupernodes.size(); ++s) {
-    auto& sn = finalSupernodes[s];
-    work.clear();
-    for (int c = sn.firstCol; c < sn.firstCol + sn.ncols; ++c) {
-      for (int i : rowPatterns2[c]) {
-        if (mark[i] != static_cast<int>(s)) {
-          mark[i] = static_cast<int>(s);
-          work.push_back(i);
-        }
-      }
-    }
-    std::sort(work.begin(), work.end());
-    sn.rowPattern = work;
-  }
   sf.supernodes = std::move(finalSupernodes);
   return sf;
 }

@@ -54,10 +54,8 @@ struct EliminationTree {
   int n = 0;
 };
 
-// Liu's etree (union-find with path compression) plus column counts by
-// explicit row-pattern union (elimination_tree.hpp:62-138). If rowPatterns is
-// non-null, Struct(L*j) (sorted, including j) is returned for every column.
-EliminationTree buildEliminationTree(const CscPattern& permutedSym, std::vector<std::vector<int>>* rowPatterns);
+// Liu's etree (union-find with path compression), elimination_tree.hpp:78-96.
+std::vector<int> eliminationTreeParent(const CscPattern& permutedSym);
 
 // Postorder of the forest given by parent[] with children visited in
 // increasing index order (symbolic.hpp:85-105). Iterative, same visit order.
@@ -73,6 +71,15 @@ struct Supernode {
     return k * m - k * (k - 1) / 2;
   }
 };
+
+// The elimination tree with its column counts (elimination_tree.hpp:62-138)
+// from the structures Struct(L*j), which live only until their parent's
+// structure is formed. Optionally returns the fundamental supernodes
+// (symbolic.hpp:229-247, each with its first column's structure), and fills
+// the rowPattern of each of the given contiguous column groups with the
+// sorted union of its columns' structures (symbolic.hpp:385-396).
+EliminationTree columnStructure(const CscPattern& permutedSym, std::vector<Supernode>* fundamental,
+                                std::vector<Supernode>* groups);
 
 struct SymbolicFactorOptions {
   int max_relax_size = 64;
