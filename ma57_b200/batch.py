@@ -15,24 +15,33 @@ from __future__ import annotations
 import numpy as np
 import scipy.sparse as sp
 
-from . import matrices as M
 from .solver import OrderingType, SymLDLT
 
 
 class BatchedSolver:
     def __init__(self, systems, ordering=OrderingType.AMD, device: int = 0, graph: bool = True):
         """systems: lower triangles (CSC) of the symmetric matrices."""
-        self.perms, blocks, self.offsets = [], [], [0]
+        self.perms, self.offsets = [], [0]
+        rows, cols, vals = [], [], []
         for A in systems:
             s = SymLDLT(device)
             s.setOrdering(ordering)
             s.analyzePattern(A)
-            perm = np.asarray(s.symbolicFactor().perm)
-            full = M.sym_full(A).tocsr()
-            blocks.append(sp.tril(full[perm][:, perm]).tocsc())
+            perm = np.asarray(s._analysis.perm())
+            # the permuted lower triangle: every stored entry (r >= c) moves to
+            # (max, min) of its new positions, shifted to the system's block
+            C = sp.tril(sp.csc_matrix(A)).tocoo()
+            inv = np.empty_like(perm)
+            inv[perm] = np.arange(len(perm), dtype=perm.dtype)
+            r, c = inv[C.row], inv[C.col]
+            o = self.offsets[-1]
+            rows.append(np.maximum(r, c) + o)
+            cols.append(np.minimum(r, c) + o)
+            vals.append(C.data)
             self.perms.append(perm)
-            self.offsets.append(self.offsets[-1] + A.shape[0])
-        self.A = sp.block_diag(blocks, format="csc")
+            self.offsets.append(o + A.shape[0])
+        n = self.offsets[-1]
+        self.A = sp.csc_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
         self.A.sort_indices()
         self.n = self.A.shape[0]
         self.solver = SymLDLT(device)

@@ -180,6 +180,16 @@ class Analysis:
         except Exception:
             pass
 
+    def perm(self) -> np.ndarray:
+        """The final ordering alone (new -> original index), without
+        building the supernode lists."""
+        if self._sf is not None:
+            return self._sf.perm
+        lib = L.load()
+        p = np.zeros(self.n, np.int32)
+        _check(lib.symla_symbolic_get(self.h, L.ptr_i(p), None, None, None, None, None, None))
+        return p
+
     def factor(self) -> SymbolicFactor:
         if self._sf is not None:
             return self._sf
