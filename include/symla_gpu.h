@@ -59,7 +59,14 @@ enum {
   SYMLA_ERR_INTERNAL = 11
 };
 
-enum { SYMLA_ORDER_AMD = 0, SYMLA_ORDER_METIS = 1, SYMLA_ORDER_NATURAL = 2 };
+/* Orderings (OrderingType, ordering.hpp:31-35). SYMLA_ORDER_METIS takes
+ * METIS_NodeND's first output array, which lists the original vertex placed
+ * at each new position: the nested-dissection pivot order. The reference
+ * takes the second array instead (ordering.hpp:130-141), which is the inverse
+ * of that permutation; SYMLA_ORDER_METIS_IPERM reproduces the reference's
+ * permutation exactly, for callers that need bit-identical symbolic results
+ * with it. The two agree on AMD and Natural. */
+enum { SYMLA_ORDER_AMD = 0, SYMLA_ORDER_METIS = 1, SYMLA_ORDER_NATURAL = 2, SYMLA_ORDER_METIS_IPERM = 3 };
 enum { SYMLA_MODE_THRESHOLD = 0, SYMLA_MODE_STATIC = 1 };
 /* Arithmetic of the Schur-complement (trailing) updates of large fronts.
  * Pivot tests, D, 2x2 inversion, L, the solves and the refinement residual
@@ -89,6 +96,11 @@ typedef struct {
 int symla_analyze(int n, const int* colptr, const int* rowind, int ordering, int max_relax_size,
                   double max_relax_fill_fraction, symla_symbolic** out);
 void symla_symbolic_destroy(symla_symbolic* sym);
+/* computeOrdering (ordering.hpp:84-149) alone: perm[k] = original index of
+ * the k-th pivot, before the elimination-tree postorder that symla_analyze
+ * applies on top of it (symbolic.hpp:207-218). Either triangle or both may be
+ * stored. */
+int symla_compute_ordering(int n, const int* colptr, const int* rowind, int ordering, int* perm);
 int symla_symbolic_get_info(const symla_symbolic* sym, symla_symbolic_info* info);
 /* Any output pointer may be NULL. perm/etree_parent/etree_colcount: n.
  * sn_first/sn_ncols: num_supernodes; sn_ptr: num_supernodes+1;

@@ -6,8 +6,8 @@ kernels behind the C ABI declared in ``include/symla_gpu.h``.
 """
 from .solver import (Inertia, InvalidArgument, LogicError, Mode, NumericFactor, OrderingType, Precision,
                      RefinedSolve, RefinementOptions, RefinementResult, SymbolicFactor, SymbolicFactorOptions,
-                     SymLDLT, as_csc)
+                     SymLDLT, as_csc, computeOrdering)
 
 __all__ = ["SymLDLT", "Mode", "OrderingType", "Precision", "Inertia", "SymbolicFactorOptions",
            "RefinementOptions", "RefinementResult", "RefinedSolve", "SymbolicFactor", "NumericFactor",
-           "LogicError", "InvalidArgument", "as_csc"]
+           "LogicError", "InvalidArgument", "as_csc", "computeOrdering"]

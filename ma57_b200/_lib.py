@@ -74,6 +74,7 @@ _SIGS = {
     "symla_last_error": (C.c_char_p, []),
     "symla_analyze": (_i, [_i, _pi, _pi, _i, _i, _d, C.POINTER(_p)]),
     "symla_symbolic_destroy": (None, [_p]),
+    "symla_compute_ordering": (_i, [_i, _pi, _pi, _i, _pi]),
     "symla_symbolic_get_info": (_i, [_p, C.POINTER(SymbolicInfo)]),
     "symla_symbolic_get": (_i, [_p, _pi, _pi, _pi, _pi, _pi, _pi, _pi]),
     "symla_symbolic_get_fundamental": (_i, [_p, _pi, _pi, _pi, _pi]),

@@ -103,7 +103,7 @@ extern "C" int symla_analyze(int n, const int* colptr, const int* rowind, int or
   if (!out) return set_error(SYMLA_ERR_INVALID, "symla_analyze: out is NULL");
   *out = nullptr;
   if (n < 0 || (n > 0 && (!colptr || !rowind))) return set_error(SYMLA_ERR_BAD_SIZE, "symla_analyze: bad matrix");
-  if (ordering < 0 || ordering > 2) return set_error(SYMLA_ERR_INVALID, "symla::computeOrdering: unknown OrderingType");
+  if (ordering < 0 || ordering > 3) return set_error(SYMLA_ERR_INVALID, "symla::computeOrdering: unknown OrderingType");
   return guarded([&] {
     symla_host::SymbolicFactorOptions opt;
     opt.max_relax_size = max_relax_size;
@@ -119,6 +119,22 @@ extern "C" int symla_analyze(int n, const int* colptr, const int* rowind, int or
       throw;
     }
     *out = s;
+  });
+}
+
+extern "C" int symla_compute_ordering(int n, const int* colptr, const int* rowind, int ordering, int* perm) {
+  if (n < 0 || (n > 0 && (!colptr || !rowind || !perm)))
+    return set_error(SYMLA_ERR_BAD_SIZE, "symla_compute_ordering: bad matrix");
+  if (ordering < 0 || ordering > 3) return set_error(SYMLA_ERR_INVALID, "symla::computeOrdering: unknown OrderingType");
+  return guarded([&] {
+    std::vector<int> p;
+    try {
+      const auto sym = symla_host::symmetricPatternNoDiag(n, colptr, rowind);
+      p = symla_host::computeOrdering(sym, static_cast<symla_host::OrderingType>(ordering));
+    } catch (const std::runtime_error& e) {
+      throw SymlaError(SYMLA_ERR_INTERNAL, e.what());
+    }
+    std::copy(p.begin(), p.end(), perm);
   });
 }
 

@@ -10,7 +10,9 @@
 // matrix, the original vertex placed there, which is exactly this convention
 // (the separator vertices of the top-level bisection come out last). The
 // reference passes METIS's second array (`iperm`) instead; that is the
-// inverse permutation, not the nested-dissection order itself.
+// inverse permutation, not the nested-dissection order itself. `takeIperm`
+// reproduces the reference's choice for callers that need its exact
+// permutation.
 #include "symbolic.hpp"
 
 #include <cstdint>
@@ -24,7 +26,7 @@ int METIS_NodeND(int64_t* nvtxs, int64_t* xadj, int64_t* adjncy, int64_t* vwgt, 
 
 namespace symla_host {
 
-std::vector<int> metisOrder(const CscPattern& sym) {
+std::vector<int> metisOrder(const CscPattern& sym, bool takeIperm) {
   const int n = sym.n;
   std::vector<int64_t> xadj(sym.colPtr.begin(), sym.colPtr.end());
   std::vector<int64_t> adjncy(sym.rowIdx.begin(), sym.rowIdx.end());
@@ -37,7 +39,7 @@ std::vector<int> metisOrder(const CscPattern& sym) {
   std::vector<int> perm(n);
   std::vector<char> seen(n, 0);
   for (int k = 0; k < n; ++k) {
-    const int64_t v = mperm[k];
+    const int64_t v = takeIperm ? miperm[k] : mperm[k];
     if (v < 0 || v >= n || seen[v]) throw std::runtime_error("symla::computeOrdering: METIS returned an invalid permutation");
     seen[v] = 1;
     perm[k] = static_cast<int>(v);

@@ -74,9 +74,9 @@ std::vector<int> computeOrdering(const CscPattern& sym, OrderingType type) {
     return perm;
   }
   if (type == OrderingType::AMD) return amdOrder(sym);
-  if (type == OrderingType::Metis) {
+  if (type == OrderingType::Metis || type == OrderingType::MetisIperm) {
     if (n == 0) return {};
-    return metisOrder(sym);
+    return metisOrder(sym, type == OrderingType::MetisIperm);
   }
   throw std::invalid_argument("symla::computeOrdering: unknown OrderingType");
 }

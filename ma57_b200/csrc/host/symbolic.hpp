@@ -18,7 +18,10 @@
 
 namespace symla_host {
 
-enum class OrderingType { AMD = 0, Metis = 1, Natural = 2 };
+// MetisIperm is the reference's own METIS convention (ordering.hpp:130-141):
+// METIS_NodeND's second output array is taken as the pivot order. Metis takes
+// the first array, which lists the original vertex at each new position.
+enum class OrderingType { AMD = 0, Metis = 1, Natural = 2, MetisIperm = 3 };
 
 // Compressed-column pattern (0-based, square).
 struct CscPattern {
@@ -45,8 +48,10 @@ std::vector<int> computeOrdering(const CscPattern& sym, OrderingType type);
 std::vector<int> amdOrder(const CscPattern& sym);
 
 // Nested dissection through METIS_NodeND (METIS 5 API, 64-bit idx_t as built
-// into the CUDA toolkit's libmetis_static.a). Output convention as above.
-std::vector<int> metisOrder(const CscPattern& sym);
+// into the CUDA toolkit's libmetis_static.a). Output convention as above;
+// with takeIperm the second output array is returned instead (the reference's
+// convention, ordering.hpp:130-141).
+std::vector<int> metisOrder(const CscPattern& sym, bool takeIperm = false);
 
 struct EliminationTree {
   std::vector<int> parent;    // parent[j] or -1

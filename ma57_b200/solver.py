@@ -38,9 +38,13 @@ class Mode(enum.IntEnum):
 
 
 class OrderingType(enum.IntEnum):
+    """OrderingType (ordering.hpp:31-35). ``Metis`` is nested dissection in
+    METIS's pivot order; ``MetisIperm`` takes METIS's inverse array, as the
+    reference does (ordering.hpp:130-141), for bit-identical permutations."""
     AMD = 0
     Metis = 1
     Natural = 2
+    MetisIperm = 3
 
 
 class Precision(enum.IntEnum):
@@ -159,6 +163,15 @@ def _check(rc: int):
     if rc in (L.SYMLA_ERR_BAD_SIZE, L.SYMLA_ERR_INVALID):
         raise InvalidArgument(msg)
     raise RuntimeError(f"{msg} (status {rc})")
+
+
+def computeOrdering(A, ordering) -> np.ndarray:
+    """symla::computeOrdering (ordering.hpp:84-149): perm[k] = original index
+    of the k-th pivot, without the postorder that analyzePattern applies."""
+    n, cp, ri, _ = as_csc(A)
+    perm = np.zeros(max(1, n), np.int32)
+    _check(L.load().symla_compute_ordering(n, L.ptr_i(cp), L.ptr_i(ri), int(OrderingType(ordering)), L.ptr_i(perm)))
+    return perm[:n]
 
 
 class Analysis:
