@@ -254,6 +254,27 @@ enum { SYMLA_KERNEL_TRAILING = 0, SYMLA_KERNEL_PANEL = 1, SYMLA_KERNEL_SMALL = 2
        SYMLA_KERNEL_KINDS = 8 };
 int symla_gpu_set_profiling(symla_gpu_ctx* ctx, int enable);
 
+/* Failure handling (no reference counterpart; the reference has no device
+ * waits or device memory).
+ *
+ * symla_gpu_set_wait_limit_ns: every device-side wait on another CTA's
+ * progress -- the pipelined solves' block flags and the tensor-core Schur
+ * update's copy/MMA barriers -- gives up after `ns` nanoseconds of the GPU's
+ * global timer (0 restores the default of 2 s). A wait that runs out makes
+ * the call return SYMLA_ERR_TIMEOUT; the context stays usable (a solve can be
+ * repeated, a factorization must be repeated). If a tensor-core tile that
+ * gave up cannot then confirm, within the default limit, that its copies and
+ * MMAs have finished, the call also reports SYMLA_ERR_TIMEOUT and every later
+ * call on the context fails with SYMLA_ERR_CUDA: destroy it.
+ *
+ * symla_gpu_set_memory_limit: process-wide cap, in bytes, on the device
+ * memory that each later symla_gpu_create may allocate for a context's plan
+ * (front arena, maps, solve workspaces); 0 removes it. A plan that does not
+ * fit fails with SYMLA_ERR_OOM before touching the GPU further, like a
+ * failing cudaMalloc does without a cap. */
+int symla_gpu_set_wait_limit_ns(symla_gpu_ctx* ctx, unsigned long long ns);
+int symla_gpu_set_memory_limit(long long bytes);
+
 /* Graph launch of the factorization (no reference counterpart): when
  * enabled (and profiling is off), the static pass over all tree levels, with
  * a few spare panel iterations per level, is captured once per set of
@@ -274,6 +295,17 @@ int symla_gpu_level_info(symla_gpu_ctx* ctx, int level, int* out6);
 int symla_gpu_set_level_schedule(symla_gpu_ctx* ctx, int level, int small_threads, int cluster_ctas);
 int symla_gpu_graph_stats(symla_gpu_ctx* ctx, int* captures, int* resumes);
 int symla_gpu_kernel_stats(symla_gpu_ctx* ctx, int kind, double* out4);
+/* The same per tree level (the per-phase timers the reference keeps under
+ * SYMLA_PROFILE, multifrontal.hpp:56-78, by level instead of by phase):
+ * launches of `kind` issued for that level's fronts (factorization) or
+ * blocks (solves). Algorithmic flops of the Schur updates are counted on the
+ * device per factorization, not per level, and read 0 here. */
+int symla_gpu_level_kernel_stats(symla_gpu_ctx* ctx, int level, int kind, double* out4);
+/* Large-front panel outcomes of a level, counted while profiling is enabled
+ * (ordinary launches, not the graph): [0] speculated and accepted whole,
+ * [1] accepted up to a failing pivot, [2] failed at the first pivot, [3] run
+ * sequentially throughout (the totals of symla_gpu_plan_stats [7..10]). */
+int symla_gpu_level_panel_stats(symla_gpu_ctx* ctx, int level, long long* out4);
 void symla_gpu_reset_kernel_stats(symla_gpu_ctx* ctx);
 /* Number of kernels the library launched since the last reset (the kernel
  * nodes of a replayed factorization graph count at every replay). */
@@ -284,8 +316,10 @@ long long symla_gpu_launch_count(symla_gpu_ctx* ctx);
  * (lower-triangle convention), [5] nnz(L) entries, [6] arena doubles;
  * large-front panels of the last factorize: [7] speculated and accepted
  * whole, [8] accepted up to a failing pivot, [9] failed at the first pivot
- * (one sequential decision), [10] run sequentially throughout. Returns the
- * number of entries (11). */
+ * (one sequential decision), [10] run sequentially throughout; decisions of
+ * the panels' sequential (per-pivot) path: [11] 1x1 at k by the first
+ * Bunch-Kaufman test or an isolated column, [12] 1x1 at k by the sigma test,
+ * [13] interchange then 1x1, [14] 2x2. Returns the number of entries (15). */
 int symla_gpu_plan_stats(symla_gpu_ctx* ctx, double* out, int cap);
 
 /* Learned first-attempt delta for Mode::StaticRegularized (no reference

@@ -101,8 +101,12 @@ _SIGS = {
     "symla_gpu_set_level_schedule": (_i, [_p, _i, _i, _i]),
     "symla_gpu_graph_stats": (_i, [_p, _pi, _pi]),
     "symla_gpu_kernel_stats": (_i, [_p, _i, _pd]),
+    "symla_gpu_level_kernel_stats": (_i, [_p, _i, _i, _pd]),
+    "symla_gpu_level_panel_stats": (_i, [_p, _i, C.POINTER(C.c_longlong)]),
     "symla_gpu_reset_kernel_stats": (None, [_p]),
     "symla_gpu_launch_count": (C.c_longlong, [_p]),
+    "symla_gpu_set_wait_limit_ns": (_i, [_p, C.c_ulonglong]),
+    "symla_gpu_set_memory_limit": (_i, [C.c_longlong]),
     "symla_gpu_relative_residual_noalloc": (_i, [_p, _p, _i, _p, _i, _i, _pd]),
     "symla_mlp_create": (_i, [_i, _pd, C.POINTER(_p)]),
     "symla_mlp_destroy": (None, [_p]),

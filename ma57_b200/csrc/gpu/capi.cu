@@ -1,6 +1,7 @@
 // C ABI implementation (include/symla_gpu.h): symbolic entry points, the
 // device plan, and the factorize / solve / refine drivers.
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -73,9 +74,20 @@ int guarded(F&& body) {
   }
 }
 
+// Device bytes a context's creation may still allocate (symla_gpu_set_memory_limit),
+// or < 0 for no limit; set for the duration of one symla_gpu_create.
+std::atomic<long long> g_create_limit{0};
+thread_local long long tl_alloc_budget = -1;
+
 template <typename T>
 T* dalloc(size_t count) {
   if (count == 0) count = 1;
+  const long long bytes = static_cast<long long>(count * sizeof(T));
+  if (tl_alloc_budget >= 0) {
+    if (bytes > tl_alloc_budget)
+      throw SymlaError(SYMLA_ERR_OOM, "symla_gpu_create: the context's device memory limit is too small for its plan");
+    tl_alloc_budget -= bytes;
+  }
   void* p = nullptr;
   CK(cudaMalloc(&p, count * sizeof(T)));
   return static_cast<T*>(p);
@@ -316,12 +328,20 @@ void build_level_lists(symla_gpu_ctx* c, const std::vector<int>& frontsOfLevel, 
     // tiles up to one per SM (the update launchers double it: 128 x 64 tiles,
     // two CTAs per SM)
     L.trailing_grid = std::max(1, std::min(tiles * static_cast<int>(L.large.size()), 148));
+    // fronts too tall for a full-width cluster panel take narrower panels
+    L.panel_width = panel_width_for(L.large_max_m, static_cast<int>(L.large.size()));
+    if (L.panel_width != kPanelWidth) {
+      L.panels = 0;
+      for (int s : L.large) L.panels = std::max(L.panels, (c->fronts[s].nelig + L.panel_width - 1) / L.panel_width);
+    }
   } else {
     L.trailing_grid = 0;
   }
 }
 
 void free_level_device(LevelLists& L) {
+  dfree(L.d_panel_cols);
+  L.d_panel_cols = nullptr;
   dfree(L.d_small);
   dfree(L.d_large);
   dfree(L.d_tasks);
@@ -422,6 +442,8 @@ void upload_level_lists(LevelLists& L, cudaStream_t s) {
   free_level_device(L);
   L.d_small = dupload(L.small, s);
   L.d_large = dupload(L.large, s);
+  if (!L.large.empty() && !panel_fits_shared(L.large_max_m))
+    L.d_panel_cols = dalloc<double>(2 * static_cast<size_t>(L.large_max_m) * L.large.size());
   L.d_tasks = dupload(L.tasks, s);
   L.d_all = dupload(L.all, s);
 }
@@ -720,14 +742,17 @@ KernelOpts make_kernel_opts(symla_gpu_ctx* c, const symla_factor_opts* o) {
 void launch_panel_iteration(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
                             const int* d_large) {
   cudaStream_t st = c->stream;
+  c->cur_level = level;
   const int nl = static_cast<int>(L.large.size());
   timed(c, SYMLA_KERNEL_PANEL, 0.0, 0.0, [&] {
-    if (c->use_cluster_panel && cluster_size_for(L.large_max_m, nl) > 0) {
-      CK(launch_cluster_panel(c->d_desc, c->d_state, d_large, nl, L.large_max_m, kPanelWidth, ko, c->d_glob, level,
+    if (c->use_cluster_panel && cluster_size_for(L.large_max_m, nl, L.panel_width) > 0) {
+      CK(launch_cluster_panel(c->d_desc, c->d_state, d_large, nl, L.large_max_m, L.panel_width, ko, c->d_glob, level,
                               dynamic, st, L.cluster_ctas));
     } else {
-      launch_panel(c->d_desc, c->d_state, d_large, nl, L.large_max_m, kPanelWidth, ko, c->d_glob, level, dynamic,
-                   st);
+      // fronts too tall for shared memory keep their two working columns in
+      // a global buffer (allocated with the level's lists)
+      CK(launch_panel(c->d_desc, c->d_state, d_large, nl, L.large_max_m, L.panel_width, ko, c->d_glob, level,
+                      dynamic, st, panel_fits_shared(L.large_max_m) ? nullptr : L.d_panel_cols));
     }
   });
   if (ko.precision != SYMLA_PREC_MIXED) {
@@ -769,6 +794,7 @@ void launch_panel_iteration(symla_gpu_ctx* c, const LevelLists& L, int level, co
 void launch_level_planned(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
                           const int* d_small, const int* d_large, const int* d_tasks, int iters) {
   cudaStream_t st = c->stream;
+  c->cur_level = level;
   if (!L.small.empty())
     timed(c, SYMLA_KERNEL_SMALL, L.small_flops, 0.0, [&] {
       launch_factor_small(c->d_desc, c->d_links, c->d_state, d_small, static_cast<int>(L.small.size()),
@@ -797,8 +823,24 @@ int level_plan_iters(const symla_gpu_ctx* c, const LevelLists& L, int level) {
 void launch_level(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
                   const int* d_small, const int* d_large, const int* d_tasks) {
   const int iters = level_plan_iters(c, L, level);
+  FactorGlobals before{};
+  if (c->profiling && !L.large.empty()) {
+    CK(cudaMemcpyAsync(&before, c->d_glob, sizeof before, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
   launch_level_planned(c, L, level, ko, dynamic, d_small, d_large, d_tasks, iters);
   if (!L.large.empty()) complete_level(c, L, level, ko, dynamic, d_large, iters);
+  if (c->profiling && !L.large.empty()) {
+    FactorGlobals after{};
+    CK(cudaMemcpyAsync(&after, c->d_glob, sizeof after, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->level_panels.size() != static_cast<size_t>(c->numLevels) * 4) c->level_panels.assign(c->numLevels * 4, 0);
+    long long* lp = &c->level_panels[static_cast<size_t>(level) * 4];
+    lp[0] += after.spec_full - before.spec_full;
+    lp[1] += after.spec_partial - before.spec_partial;
+    lp[2] += after.spec_failed - before.spec_failed;
+    lp[3] += after.seq_panels - before.seq_panels;
+  }
   CK(cudaGetLastError());
 }
 
@@ -1002,7 +1044,7 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
   reset_to_static(c);
   const KernelOpts ko = make_kernel_opts(c, o);
   CK(cudaMemsetAsync(c->d_state, 0, c->numSN * sizeof(FrontState), st));
-  FactorGlobals g0{INT_MAX, 0, -1, INT_MAX, 0.0, 0.0, 0.0, 0, 0, 0, 0};
+  FactorGlobals g0{INT_MAX, 0, -1, INT_MAX, 0.0, 0.0, 0.0, 0, 0, 0, 0, c->wait_ns, {0, 0, 0, 0}};
   CK(cudaMemcpyAsync(c->d_glob, &g0, sizeof g0, cudaMemcpyHostToDevice, st));
   const bool mixed = o->precision == SYMLA_PREC_MIXED;
   if (mixed) {
@@ -1090,10 +1132,17 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
     c->panel_counts[1] = gp.spec_partial;
     c->panel_counts[2] = gp.spec_failed;
     c->panel_counts[3] = gp.seq_panels;
+    for (int i = 0; i < 4; ++i) c->seq_dec_counts[i] = gp.seq_dec[i];
   }
   if (mixed) {
     int tcerr = 0;
     CK(cudaMemcpy(&tcerr, c->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (tcerr & kTcErrDrain) {
+      c->unusable = true;
+      throw SymlaError(SYMLA_ERR_TIMEOUT,
+                       "tensor-core Schur update: a pipeline wait timed out and its drain did not finish; "
+                       "the context is no longer usable");
+    }
     if (tcerr != 0) throw SymlaError(SYMLA_ERR_TIMEOUT, "tensor-core Schur update: a pipeline wait timed out");
   }
   if (!dynamic) read_states(c);
@@ -1266,9 +1315,10 @@ void device_solve(symla_gpu_ctx* c, const double* dB, int ldb, int nrhs, double*
       const auto& L = c->levels[l];
       const int nt = static_cast<int>(L.fwd_tasks.size());
       const int grid = std::min(nt, c->fwd_resident);
+      c->cur_level = l;
       timed(c, SYMLA_KERNEL_FORWARD, 0.0, L.solve_bytes_fixed + nc * L.solve_bytes_per_rhs, [&] {
         CK(launch_forward_pipelined(c->d_desc, c->d_links, c->d_state, L.d_fwd_tasks, nt, grid, c->d_flag_base,
-                                    c->d_flags, ef, c->d_solve_err, nrhs, c0, c->d_Bp, n, st));
+                                    c->d_flags, ef, c->d_solve_err, c->wait_ns, nrhs, c0, c->d_Bp, n, st));
       });
     }
     if (c0 == 0) CK(cudaEventRecord(c->ev[3], st));
@@ -1277,12 +1327,14 @@ void device_solve(symla_gpu_ctx* c, const double* dB, int ldb, int nrhs, double*
       const auto& L = c->levels[l];
       const int nt = static_cast<int>(L.bwd_tasks.size());
       const int grid = std::min(nt, c->bwd_resident);
+      c->cur_level = l;
       timed(c, SYMLA_KERNEL_BACKWARD, 0.0, L.solve_bytes_fixed + nc * L.solve_bytes_per_rhs, [&] {
         CK(launch_backward_pipelined(c->d_desc, c->d_state, L.d_bwd_tasks, nt, grid, c->d_flag_base, c->d_flags,
-                                     c->d_hflags, c->d_hscratch, eb, c->d_solve_err, nrhs, c0, c->d_Xf, n, st));
+                                     c->d_hflags, c->d_hscratch, eb, c->d_solve_err, c->wait_ns, nrhs, c0, c->d_Xf, n, st));
       });
     }
   }
+  c->cur_level = -1;
   CK(cudaEventRecord(c->ev[4], st));
   launch_permute_out(n, nrhs, c->d_perm, c->d_Xf, dX, ldx, st);
   CK(cudaGetLastError());
@@ -1298,7 +1350,14 @@ void check_solve_error(symla_gpu_ctx* c) {
   }
 }
 
+void check_usable(symla_gpu_ctx* c) {
+  if (c->unusable)
+    throw SymlaError(SYMLA_ERR_CUDA,
+                     "symla_gpu: the context is no longer usable (a tensor-core tile's drain timed out); destroy it");
+}
+
 void check_solvable(symla_gpu_ctx* c) {
+  check_usable(c);
   if (!c->factorized)
     throw SymlaError(SYMLA_ERR_NOT_FACTORIZED, "symla::SymLDLT::solve: factorize() must be called before solve()");
   if (c->singular)
@@ -1339,7 +1398,7 @@ void timed(symla_gpu_ctx* c, int kind, double flops, double bytes, F&& launch) {
   CK(cudaEventRecord(a, c->stream));
   launch();
   CK(cudaEventRecord(b, c->stream));
-  c->pending.push_back({a, b, kind, flops, bytes});
+  c->pending.push_back({a, b, kind, c->cur_level, flops, bytes});
 }
 
 void collect_pending(symla_gpu_ctx* c) {
@@ -1353,6 +1412,15 @@ void collect_pending(symla_gpu_ctx* c) {
     k.ms += ms;
     k.flops += p.flops;
     k.bytes += p.bytes;
+    if (p.level >= 0 && p.level < c->numLevels) {
+      if (c->level_kstat.size() != static_cast<size_t>(c->numLevels) * SYMLA_KERNEL_KINDS)
+        c->level_kstat.assign(static_cast<size_t>(c->numLevels) * SYMLA_KERNEL_KINDS, {});
+      auto& kl = c->level_kstat[static_cast<size_t>(p.level) * SYMLA_KERNEL_KINDS + p.kind];
+      kl.launches++;
+      kl.ms += ms;
+      kl.flops += p.flops;
+      kl.bytes += p.bytes;
+    }
     c->evpool.push_back(p.a);
     c->evpool.push_back(p.b);
   }
@@ -1368,6 +1436,8 @@ extern "C" int symla_gpu_create(const symla_symbolic* sym, int n, const int* col
   if (!sym) return set_error(SYMLA_ERR_NOT_ANALYZED, "symla::SymLDLT::factorize: analyzePattern must be called first");
   if (n != sym->sf.etree.n) return set_error(SYMLA_ERR_BAD_SIZE, "symla_gpu_create: matrix size differs from the analysis");
   symla_gpu_ctx* c = new symla_gpu_ctx();
+  const long long limit = g_create_limit.load();
+  tl_alloc_budget = limit > 0 ? limit : -1;
   const int rc = guarded([&] {
     int count = 0;
     CK(cudaGetDeviceCount(&count));
@@ -1392,6 +1462,7 @@ extern "C" int symla_gpu_create(const symla_symbolic* sym, int n, const int* col
     CK(cudaMemsetAsync(c->d_solve_err, 0, sizeof(int), c->stream));
     build_plan(c, sym->sf, colptr, rowind);
   });
+  tl_alloc_budget = -1;
   if (rc != SYMLA_OK) {
     symla_gpu_destroy(c);
     return rc;
@@ -1445,6 +1516,7 @@ extern "C" int symla_gpu_factorize(symla_gpu_ctx* c, const double* values, int v
   if (!opts) opts = &def;
   if (c->nnz > 0 && !values) return set_error(SYMLA_ERR_INVALID, "symla_gpu_factorize: values is NULL");
   return guarded([&] {
+    check_usable(c);
     CK(cudaSetDevice(c->device));
     c->factorized = false;
     upload_values(c, values, values_on_device);
@@ -1745,7 +1817,7 @@ extern "C" int symla_gpu_phase_ms(symla_gpu_ctx* c, float* ms, int cap) {
 
 extern "C" int symla_gpu_plan_stats(symla_gpu_ctx* c, double* out, int cap) {
   if (!c) return 0;
-  double v[11] = {0};
+  double v[15] = {0};
   v[0] = c->numSN;
   v[1] = c->numLevels;
   v[2] = c->plan_max_m;
@@ -1775,8 +1847,9 @@ extern "C" int symla_gpu_plan_stats(symla_gpu_ctx* c, double* out, int cap) {
   }
   v[6] = static_cast<double>(c->arena_doubles);
   for (int i = 0; i < 4; ++i) v[7 + i] = c->panel_counts[i];
-  for (int i = 0; i < cap && i < 11; ++i) out[i] = v[i];
-  return 11;
+  for (int i = 0; i < 4; ++i) v[11 + i] = c->seq_dec_counts[i];
+  for (int i = 0; i < cap && i < 15; ++i) out[i] = v[i];
+  return 15;
 }
 
 extern "C" int symla_gpu_level_info(symla_gpu_ctx* c, int level, int* out6) {
@@ -1809,6 +1882,18 @@ extern "C" int symla_gpu_set_level_schedule(symla_gpu_ctx* c, int level, int sma
   return SYMLA_OK;
 }
 
+extern "C" int symla_gpu_set_memory_limit(long long bytes) {
+  if (bytes < 0) return set_error(SYMLA_ERR_INVALID, "symla_gpu_set_memory_limit: negative limit");
+  g_create_limit.store(bytes);
+  return SYMLA_OK;
+}
+
+extern "C" int symla_gpu_set_wait_limit_ns(symla_gpu_ctx* c, unsigned long long ns) {
+  if (!c) return set_error(SYMLA_ERR_INVALID, "null context");
+  c->wait_ns = ns == 0 ? symla_gpu::kDefaultWaitNs : ns;
+  return SYMLA_OK;
+}
+
 extern "C" int symla_gpu_set_graph(symla_gpu_ctx* c, int enable) {
   if (!c) return set_error(SYMLA_ERR_INVALID, "null context");
   c->use_graph = enable != 0;
@@ -1838,9 +1923,33 @@ extern "C" int symla_gpu_kernel_stats(symla_gpu_ctx* c, int kind, double* out4) 
   return SYMLA_OK;
 }
 
+extern "C" int symla_gpu_level_kernel_stats(symla_gpu_ctx* c, int level, int kind, double* out4) {
+  if (!c || kind < 0 || kind >= SYMLA_KERNEL_KINDS || !out4 || level < 0 || level >= c->numLevels)
+    return set_error(SYMLA_ERR_INVALID, "bad arguments");
+  symla_gpu_ctx::KStat k;
+  if (c->level_kstat.size() == static_cast<size_t>(c->numLevels) * SYMLA_KERNEL_KINDS)
+    k = c->level_kstat[static_cast<size_t>(level) * SYMLA_KERNEL_KINDS + kind];
+  out4[0] = static_cast<double>(k.launches);
+  out4[1] = k.ms;
+  out4[2] = k.flops;
+  out4[3] = k.bytes;
+  return SYMLA_OK;
+}
+
+extern "C" int symla_gpu_level_panel_stats(symla_gpu_ctx* c, int level, long long* out4) {
+  if (!c || !out4 || level < 0 || level >= c->numLevels) return set_error(SYMLA_ERR_INVALID, "bad arguments");
+  for (int t = 0; t < 4; ++t)
+    out4[t] = c->level_panels.size() == static_cast<size_t>(c->numLevels) * 4
+                  ? c->level_panels[static_cast<size_t>(level) * 4 + t]
+                  : 0;
+  return SYMLA_OK;
+}
+
 extern "C" void symla_gpu_reset_kernel_stats(symla_gpu_ctx* c) {
   if (!c) return;
   for (auto& k : c->kstat) k = symla_gpu_ctx::KStat();
+  c->level_kstat.clear();
+  c->level_panels.clear();
   c->launches = 0;
 }
 

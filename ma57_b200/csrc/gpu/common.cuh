@@ -77,6 +77,17 @@ __host__ __device__ inline bool tc_block_ok(int K, double lmax, double wmax, dou
 
 // Error word of the pipelined solve kernels.
 constexpr int kSolveErrTimeout = 1;
+// Error bits of the tensor-core Schur update: a pipeline wait ran out (the
+// CTA abandoned its tile), and the drain after such an abandonment could not
+// confirm that the CTA's copies and tensor-core operations had finished before
+// it released its tensor memory (the context is then not trusted again).
+constexpr int kTcErrTimeout = 2;
+constexpr int kTcErrDrain = 4;
+// Default bound of every device-side wait on another CTA's progress (flags of
+// the pipelined solves, mbarriers of the tensor-core update), in ns of the
+// global timer; a context may lower it (symla_gpu_set_wait_limit_ns). The
+// drain after an abandoned tile always waits up to this default.
+constexpr unsigned long long kDefaultWaitNs = 2000000000ull;
 
 // Global counters for one factorization (device, zeroed per call).
 struct FactorGlobals {
@@ -90,6 +101,11 @@ struct FactorGlobals {
   // large-front panels of the last factorization: speculation accepted the
   // whole panel / a prefix / failed at its first pivot; whole sequential panels
   int spec_full, spec_partial, spec_failed, seq_panels;
+  unsigned long long wait_ns;  // bound of the tensor-core update's waits (set per call)
+  // decisions of the panels' sequential (per-pivot) path: 1x1 at k by the
+  // first Bunch-Kaufman test (or an isolated column), 1x1 at k by the sigma
+  // test, interchange then 1x1, 2x2
+  int seq_dec[4];
 };
 
 // Kernels of a level return at once when an earlier level stopped the

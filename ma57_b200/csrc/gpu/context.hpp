@@ -34,6 +34,8 @@ struct LevelLists {
   int small_threads = 0;       // tile schedule (autotuner): small-front kernel width, 0 = by size
   int cluster_ctas = 0;        // panel cluster size, 0 = by size
   int panels = 0;              // panel iterations needed
+  int panel_width = 32;        // pivots per panel (narrower for fronts too tall for a full-width cluster panel)
+  double* d_panel_cols = nullptr;  // single-CTA panel kernel, fronts too tall for shared memory: 2 m per front
   int trailing_grid = 0;
   std::vector<int> tasks;      // assembly tasks (front, column block) for large fronts
   std::vector<int> all;        // every front of the level (solve)
@@ -163,6 +165,13 @@ struct symla_gpu_ctx {
   // dynamic (delayed-pivot) allocations for the current factorization
   std::vector<void*> dyn_allocs;
 
+  // bound of every device-side wait on another CTA (solve flags, tensor-core
+  // mbarriers), global-timer ns; set by symla_gpu_set_wait_limit_ns
+  unsigned long long wait_ns = symla_gpu::kDefaultWaitNs;
+  // set when a tensor-core tile's drain ran out: its tensor memory was freed
+  // with work possibly outstanding, so no further work is run on the context
+  bool unusable = false;
+
   // state
   bool factorized = false;
   bool singular = false;
@@ -176,6 +185,7 @@ struct symla_gpu_ctx {
   long long nnzL = 0;
   int last_precision = 0;
   int panel_counts[4] = {0, 0, 0, 0};  // large-front panels: speculative full / prefix / failed, sequential
+  int seq_dec_counts[4] = {0, 0, 0, 0};  // sequential-path decisions (FactorGlobals::seq_dec)
 
   // panel kernel choice (the cluster kernel unless SYMLA_PANEL=single)
   bool use_cluster_panel = true;
@@ -197,9 +207,16 @@ struct symla_gpu_ctx {
     long long launches = 0;
     double ms = 0.0, flops = 0.0, bytes = 0.0;
   } kstat[8];
+  // the same per tree level (numLevels x 8, level-major); launches outside a
+  // level (permutations, residual) count in kstat only
+  std::vector<KStat> level_kstat;
+  int cur_level = -1;  // tree level of the launches being issued, or -1
+  // large-front panel outcomes per level (profiling, non-graph launches):
+  // speculative full / prefix / failed, sequential; numLevels x 4
+  std::vector<long long> level_panels;
   struct PendingEv {
     cudaEvent_t a, b;
-    int kind;
+    int kind, level;
     double flops, bytes;
   };
   std::vector<PendingEv> pending;

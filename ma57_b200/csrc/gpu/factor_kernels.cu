@@ -576,7 +576,8 @@ __device__ void global_swap(const FrontDesc& f, int i, int j) {
 
 __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
                                                               const int* __restrict__ front_list, int nb, KernelOpts o,
-                                                              FactorGlobals* g, int level, int dynamic) {
+                                                              FactorGlobals* g, int level, int dynamic,
+                                                              double* cols, int cols_stride) {
   if (level_aborted(g, level, dynamic)) return;
   constexpr int NT = kPanelThreads;
   extern __shared__ double smem[];
@@ -603,8 +604,10 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* _
   }
   const int m = f.m;
   const int effEnd = f.nelig;
-  double* colk = smem;
-  double* colr = smem + m;
+  // the two working columns: shared memory, or this front's slice of the
+  // global buffer for fronts too tall for shared memory
+  double* colk = cols ? cols + static_cast<size_t>(blockIdx.x) * 2 * cols_stride : smem;
+  double* colr = colk + m;
 
   // First panel: orig_max of the assembled front (from the assembly kernel).
   if (S.k == 0) {
@@ -1142,11 +1145,19 @@ void launch_factor_small(const FrontDesc* fronts, const ChildLink* links, FrontS
   }
 }
 
-void launch_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m, int nb,
-                  const KernelOpts& o, FactorGlobals* g, int level, int dynamic, cudaStream_t stream) {
-  if (count <= 0) return;
-  const size_t sm = 2 * static_cast<size_t>(max_m) * sizeof(double);
-  panel_kernel<<<count, kPanelThreads, sm, stream>>>(fronts, st, list, nb, o, g, level, dynamic);
+// Dynamic shared memory the single-CTA panel kernel is configured for.
+constexpr size_t kPanelSmemMax = 200 * 1024;
+
+bool panel_fits_shared(int max_m) { return 2 * static_cast<size_t>(max_m) * sizeof(double) <= kPanelSmemMax; }
+
+cudaError_t launch_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m, int nb,
+                         const KernelOpts& o, FactorGlobals* g, int level, int dynamic, cudaStream_t stream,
+                         double* cols) {
+  if (count <= 0) return cudaSuccess;
+  if (!panel_fits_shared(max_m) && !cols) return cudaErrorInvalidValue;
+  const size_t sm = cols ? 0 : 2 * static_cast<size_t>(max_m) * sizeof(double);
+  panel_kernel<<<count, kPanelThreads, sm, stream>>>(fronts, st, list, nb, o, g, level, dynamic, cols, max_m);
+  return cudaGetLastError();
 }
 
 
@@ -1215,7 +1226,7 @@ cudaError_t configure_factor_kernels() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(factor_small_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  e = cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kPanelSmemMax));
   if (e != cudaSuccess) return e;
   for (auto fn : {update_mma_kernel<0>, update_mma_kernel<1>, update_mma_kernel<2>}) {
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMmaSmem);

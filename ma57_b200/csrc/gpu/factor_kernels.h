@@ -26,13 +26,25 @@ void launch_assemble(const FrontDesc* fronts, const ChildLink* links, FrontState
 void launch_factor_small(const FrontDesc* fronts, const ChildLink* links, FrontState* st, const int* list, int count,
                          int max_m, const int* a_colptr, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
                          cudaStream_t stream, int threads = 0);  // threads: 128, 256, or 0 (by front size)
-void launch_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m, int nb,
-                  const KernelOpts& o, FactorGlobals* g, int level, int dynamic, cudaStream_t stream);
+// Single-CTA panel kernel. Its two working columns (2 m doubles per front)
+// live in shared memory when panel_fits_shared(max_m), else in `cols`
+// (device, 2 max_m doubles per front of the list), which is then required.
+bool panel_fits_shared(int max_m);
+cudaError_t launch_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m, int nb,
+                         const KernelOpts& o, FactorGlobals* g, int level, int dynamic, cudaStream_t stream,
+                         double* cols);
 // Cluster panel (panel_cluster.cu): returns 0 from cluster_size_for when a
-// front is too large for it (the single-CTA panel kernel then runs).
-int cluster_size_for(int max_m, int count);
+// front is too large for it with nb-pivot panels (the single-CTA panel
+// kernel then runs).
+int cluster_size_for(int max_m, int count, int nb = kPanelWidth);
 // whether a cluster of cs CTAs (2, 4, 8 or 16) can hold fronts of max_m rows
-bool cluster_size_fits(int max_m, int cs);
+// with nb-pivot panels
+bool cluster_size_fits(int max_m, int cs, int nb = kPanelWidth);
+// Pivots per panel for a level whose tallest large front has max_m rows:
+// kPanelWidth when a cluster holds such fronts at that width, else the widest
+// panel (at least 8 pivots) a 16-CTA cluster holds, else kPanelWidth for the
+// single-CTA kernel.
+int panel_width_for(int max_m, int count);
 cudaError_t configure_cluster_panel();
 // cs: 2, 4, 8 or 16, or 0 for cluster_size_for's choice
 cudaError_t launch_cluster_panel(const FrontDesc* fronts, FrontState* st, const int* list, int count, int max_m,
@@ -69,17 +81,19 @@ void launch_permute_in(int n, int nrhs, const int* perm, const double* B, int ld
 void launch_permute_out(int n, int nrhs, const int* perm, const double* X, double* Xout, int ldx, cudaStream_t stream);
 // Pipelined level solves (one cooperative launch per level; see
 // solve_kernels.cu). tasks: int4 (see the kernels); flags indexed by
-// flag_base[front] + block, compared against epoch.
+// flag_base[front] + block, compared against epoch; every wait on another
+// CTA's flag gives up after wait_ns of the global timer (error word set).
 int solve_block_rows();
 int solve_rhs_chunk();
 cudaError_t solve_max_resident(int device, int* fwd_ctas, int* bwd_ctas);
 cudaError_t launch_forward_pipelined(const FrontDesc* fronts, const ChildLink* links, const FrontState* st,
                                      const int4* tasks, int ntasks, int grid, const int* flag_base, int* flags,
-                                     int epoch, int* err, int nrhs, int c0, const double* Bp, int n,
-                                     cudaStream_t stream);
+                                     int epoch, int* err, unsigned long long wait_ns, int nrhs, int c0,
+                                     const double* Bp, int n, cudaStream_t stream);
 cudaError_t launch_backward_pipelined(const FrontDesc* fronts, const FrontState* st, const int4* tasks, int ntasks,
                                       int grid, const int* flag_base, int* flags, int* hflags, double* hscratch,
-                                      int epoch, int* err, int nrhs, int c0, double* X, int n, cudaStream_t stream);
+                                      int epoch, int* err, unsigned long long wait_ns, int nrhs, int c0, double* X,
+                                      int n, cudaStream_t stream);
 
 // Residual R = B - sym(A) X in the original index space (full symmetric CSR
 // gathered from the stored lower triangle); rowptr/colind/vidx describe it.

@@ -632,6 +632,7 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     const double lambda = gm.v;
     const int r = gm.i;
     int dec;
+    int dec_kind = 0;  // the seq_dec slot of this decision
     double arr = 0.0, vkr = 0.0;
     if (lambda <= o.zero_tol) {
       const double isolatedFloor = fmax(o.zero_tol, o.rel_floor * orig_max);
@@ -678,10 +679,12 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
         dec = 1;
       else
         dec = 2;
+      dec_kind = dec + 1;
       // the slow path consumed extra barriers; make every CTA finish reading
       // the exchange slots before anyone writes them again
       cluster.sync();
     }
+    if (q == 0 && threadIdx.x == 0 && dec <= 2) atomicAdd(&g->seq_dec[dec_kind], 1);
     if (dec != 0) ++nontrivial;
     if (dec == 3) {
       stopped = true;
@@ -826,13 +829,20 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
   cluster.sync();
 }
 
-bool cluster_size_fits(int max_m, int cs) {
+bool cluster_size_fits(int max_m, int cs, int nb) {
   const size_t limit = 184 * 1024;  // + the static ClusterShared (~38 KB) <= 227 KB
-  return (cs == 2 || cs == 4 || cs == 8 || cs == 16) &&
-         static_cast<size_t>((max_m + cs - 1) / cs) * (kPanelWidth + 4) * sizeof(double) <= limit;
+  return (cs == 2 || cs == 4 || cs == 8 || cs == 16) && nb >= 1 && nb <= kNBMax - 2 &&
+         static_cast<size_t>((max_m + cs - 1) / cs) * (nb + 4) * sizeof(double) <= limit;
 }
 
-int cluster_size_for(int max_m, int count) {
+int panel_width_for(int max_m, int count) {
+  if (cluster_size_for(max_m, count, kPanelWidth) > 0) return kPanelWidth;
+  for (int nb = kPanelWidth - 4; nb >= 8; nb -= 4)
+    if (cluster_size_fits(max_m, 16, nb)) return nb;
+  return kPanelWidth;
+}
+
+int cluster_size_for(int max_m, int count, int nb) {
   // The panel is latency-bound: a CTA costs a fixed ~8 us (the diagonal
   // block's pivot chain, the exchanges) plus ~10 ns per row it holds, and
   // one CTA runs per SM (200 registers x 256 threads). More CTAs per front
@@ -841,7 +851,7 @@ int cluster_size_for(int max_m, int count) {
   int best = 0;
   double best_t = 0.0;
   for (int cs : {2, 4, 8, 16}) {
-    if (!cluster_size_fits(max_m, cs)) continue;
+    if (!cluster_size_fits(max_m, cs, nb)) continue;
     const double waves = std::ceil(static_cast<double>(count) * cs / 148.0);
     const double t = waves * (8.0 + 0.01 * ((max_m + cs - 1) / cs));
     if (best == 0 || t < best_t) {
@@ -873,7 +883,8 @@ cudaError_t launch_cluster_panel(const FrontDesc* fronts, FrontState* st, const 
                                  int nb, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
                                  cudaStream_t stream, int cs_choice) {
   if (count <= 0) return cudaSuccess;
-  const int cs = cluster_size_fits(max_m, cs_choice) ? cs_choice : cluster_size_for(max_m, count);
+  const int cs = cluster_size_fits(max_m, cs_choice, nb) ? cs_choice : cluster_size_for(max_m, count, nb);
+  if (cs == 0) return cudaErrorInvalidValue;
   const int R = (max_m + cs - 1) / cs;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cs * count);

@@ -76,10 +76,18 @@ __device__ __forceinline__ double warp_max_nonneg(double v) {
   return __longlong_as_double(static_cast<long long>((static_cast<unsigned long long>(mh) << 32) | ml));
 }
 
-// atomicMax for non-negative doubles (IEEE order == integer order there).
+// atomicMax for non-negative doubles (IEEE order == integer order there). A
+// NaN is kept (its pattern orders above +Inf), so a maximum over values that
+// include a NaN reads NaN instead of a finite number.
 __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
-  if (!(v >= 0.0)) return;
+  if (v < 0.0) return;
   atomicMax(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+// max(m, |x|) that keeps a NaN once one was seen (fmax would drop it).
+__device__ __forceinline__ double nan_sticky_absmax(double m, double x) {
+  const double a = fabs(x);
+  return (a > m || a != a) ? (m != m ? m : a) : m;
 }
 
 }  // namespace symla_gpu

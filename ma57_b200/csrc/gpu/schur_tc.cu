@@ -43,7 +43,6 @@ constexpr int kBoxK = 32;      // floats per TMA box row (128 B)
 constexpr int kThreads = 128;  // 4 warps: one per 32-lane TMEM quarter
 constexpr int kStageBytes = 4 * kTM * kBoxK * 4;  // A_hi, A_lo, B_hi, B_lo
 constexpr int kStages = 2;
-constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s per wait
 constexpr int kMaxFronts = 512;
 constexpr int kSplitRows = 16;  // rows per pass of the split pre-pass
 
@@ -79,20 +78,22 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Bounded wait (kWaitNs of wall time); false on timeout, with the error word
-// set when err is given. Gives up early once another CTA recorded an error.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+// Bounded wait; false on timeout, with the timeout bit set in the error word
+// when err is given. The wait ends once limit_ns of the global timer have
+// passed or after limit_ns / 8 unsuccessful probes (a probe takes longer than
+// 8 ns), whichever comes first: a limit below the timer's resolution still
+// ends the wait. Gives up early once another CTA recorded an error.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, uint64_t limit_ns) {
   if (mbar_test(bar, parity)) return true;
   const uint64_t t0 = global_ns();
-  for (unsigned it = 1;; ++it) {
-    if (mbar_test(bar, parity)) return true;
-    if ((it & 1023) == 0) {
-      if (global_ns() - t0 > kWaitNs) {
-        if (err) atomicCAS(err, 0, 2);
-        return false;
-      }
-      if (err && *reinterpret_cast<volatile int*>(err) != 0) return false;
+  const uint64_t max_probes = limit_ns / 8;
+  for (uint64_t it = 1;; ++it) {
+    if (it > max_probes || ((it & 15) == 0 && global_ns() - t0 > limit_ns)) {
+      if (err) atomicOr(err, kTcErrTimeout);
+      return false;
     }
+    if (mbar_test(bar, parity)) return true;
+    if ((it & 63) == 0 && err && *reinterpret_cast<volatile int*>(err) != 0) return false;
   }
 }
 
@@ -246,6 +247,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_far_update_kernel(const FrontD
                                                                      FactorGlobals* g, int level, int dynamic,
                                                                      int* err) {
   if (level_skipped(g, level, dynamic)) return;
+  const uint64_t wait_ns = g->wait_ns;
   extern __shared__ __align__(1024) unsigned char tsm_raw[];
   // 1024-byte aligned stage ring (128B swizzle atoms)
   unsigned char* ring =
@@ -343,7 +345,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_far_update_kernel(const FrontD
       auto issue = [&](int c) -> bool {
         const int st_i = c % kStages;
         if (issued[st_i]) {
-          if (!mbar_wait(&empty_bar[st_i], empty_phase[st_i], err)) return false;
+          if (!mbar_wait(&empty_bar[st_i], empty_phase[st_i], err, wait_ns)) return false;
           empty_phase[st_i] ^= 1;
           issued[st_i] = 0;
         }
@@ -365,7 +367,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_far_update_kernel(const FrontD
           break;
         }
         unsigned char* base = ring + st_i * kStageBytes;
-        if (!mbar_wait(&full_bar[st_i], full_phase[st_i], err)) {
+        if (!mbar_wait(&full_bar[st_i], full_phase[st_i], err, wait_ns)) {
           ok = false;
           break;
         }
@@ -393,7 +395,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_far_update_kernel(const FrontD
       break;
     }
     // accumulator ready
-    if (!mbar_wait(&done_bar, done_phase, err)) {
+    if (!mbar_wait(&done_bar, done_phase, err, wait_ns)) {
       ok = false;
       s_abort = 1;
     }
@@ -437,11 +439,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_far_update_kernel(const FrontD
     tc_fence_after();
   }
 
-  // drain: wait (bounded) for copies and MMA groups still in flight
+  // drain: wait (bounded by the default limit, whatever the caller's) for
+  // copies and MMA groups still in flight; a drain that runs out is recorded
+  // separately, since the tensor memory is then released with work possibly
+  // outstanding
   if (threadIdx.x == 0)
     for (int i = 0; i < kStages; ++i) {
-      if (loading[i]) mbar_wait(&full_bar[i], full_phase[i], nullptr);
-      if (issued[i]) mbar_wait(&empty_bar[i], empty_phase[i], nullptr);
+      bool drained = true;
+      if (loading[i]) drained = mbar_wait(&full_bar[i], full_phase[i], nullptr, kDefaultWaitNs) && drained;
+      if (issued[i]) drained = mbar_wait(&empty_bar[i], empty_phase[i], nullptr, kDefaultWaitNs) && drained;
+      if (!drained) atomicOr(err, kTcErrDrain);
     }
   tc_fence_before();
   __syncthreads();

@@ -38,7 +38,6 @@ namespace {
 constexpr int kRB = 64;        // rows (forward) / columns (backward) per block
 constexpr int kST = 256;       // threads per CTA
 constexpr int kRhsChunk = 16;  // right-hand sides per pass
-constexpr long long kSpinLimit = 40000000;  // a few seconds with the sleep below
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -49,23 +48,34 @@ __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Wait until flags[idx] >= epoch; false on timeout or a raised error.
-__device__ bool wait_flag(const int* flags, int idx, int epoch, int* err) {
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Wait until flags[idx] >= epoch; false once wait_ns of the global timer or
+// wait_ns / 64 unsuccessful probes (each sleeps 64 ns) have passed (the
+// timeout is recorded in the error word), or another CTA raised an error.
+__device__ bool wait_flag(const int* flags, int idx, int epoch, int* err, unsigned long long wait_ns) {
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
-    long long it = 0;
     int ok = 1;
-    while (ld_acquire(flags + idx) < epoch) {
-      if (ld_acquire(err) != 0) {
-        ok = 0;
-        break;
+    if (ld_acquire(flags + idx) < epoch) {
+      const unsigned long long t0 = global_ns();
+      const unsigned long long max_probes = wait_ns / 64;
+      for (unsigned long long it = 1; ld_acquire(flags + idx) < epoch; ++it) {
+        if (ld_acquire(err) != 0) {
+          ok = 0;
+          break;
+        }
+        if (it > max_probes || global_ns() - t0 > wait_ns) {
+          atomicCAS(err, 0, kSolveErrTimeout);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
       }
-      if (++it > kSpinLimit) {
-        atomicCAS(err, 0, kSolveErrTimeout);
-        ok = 0;
-        break;
-      }
-      __nanosleep(64);
     }
     s_ok = ok;
   }
@@ -141,8 +151,8 @@ __device__ __forceinline__ void stage_tile(double* T, const double* F, int64_t l
 // ended in an error (the CTA then leaves the launch).
 __device__ bool forward_block(const FrontDesc* __restrict__ fronts, const ChildLink* __restrict__ links,
                               const FrontState* __restrict__ st, int s, int rb, const int* __restrict__ flag_base,
-                              int* flags, int epoch, int* err, int nc, int c0, const double* __restrict__ Bp, int n,
-                              double* acc, double* xb, double* Lb0) {
+                              int* flags, int epoch, int* err, unsigned long long wait_ns, int nc, int c0,
+                              const double* __restrict__ Bp, int n, double* acc, double* xb, double* Lb0) {
   const int row = threadIdx.x % kRB, cg = threadIdx.x / kRB;  // product layout: a row, 4 right-hand sides
   const FrontDesc f = fronts[s];
   const int m = f.m, np = st[s].npiv;
@@ -189,7 +199,7 @@ __device__ bool forward_block(const FrontDesc* __restrict__ fronts, const ChildL
     if (tt < jend) {
       // 2. contribution of finished pivot block j = tt
       const int j = tt;
-      if (!wait_flag(flags, flag_base[s] + j, epoch, err)) {
+      if (!wait_flag(flags, flag_base[s] + j, epoch, err, wait_ns)) {
         scp_wait<0>();
         return false;
       }
@@ -265,7 +275,7 @@ __device__ bool forward_block(const FrontDesc* __restrict__ fronts, const ChildL
 __global__ void __launch_bounds__(kST, 2) forward_pipelined_kernel(
     const FrontDesc* __restrict__ fronts, const ChildLink* __restrict__ links, const FrontState* __restrict__ st,
     const int4* __restrict__ tasks, int ntasks, const int* __restrict__ flag_base, int* flags, int epoch, int* err,
-    int nrhs, int c0, const double* __restrict__ Bp, int n) {
+    unsigned long long wait_ns, int nrhs, int c0, const double* __restrict__ Bp, int n) {
   extern __shared__ double ssm[];
   double* acc = ssm;
   double* xb = acc + kRB * kAccStride;
@@ -276,11 +286,11 @@ __global__ void __launch_bounds__(kST, 2) forward_pipelined_kernel(
     const int4 tk = tasks[task];
     const int s = tk.x;
     if (tk.y >= 0) {
-      if (!forward_block(fronts, links, st, s, tk.y, flag_base, flags, epoch, err, nc, c0, Bp, n, acc, xb, Lb0)) return;
+      if (!forward_block(fronts, links, st, s, tk.y, flag_base, flags, epoch, err, wait_ns, nc, c0, Bp, n, acc, xb, Lb0)) return;
     } else {
       const int nb = (fronts[s].m + kRB - 1) / kRB;
       for (int rb = 0; rb < nb; ++rb)
-        if (!forward_block(fronts, links, st, s, rb, flag_base, flags, epoch, err, nc, c0, Bp, n, acc, xb, Lb0))
+        if (!forward_block(fronts, links, st, s, rb, flag_base, flags, epoch, err, wait_ns, nc, c0, Bp, n, acc, xb, Lb0))
           return;
     }
   }
@@ -295,8 +305,9 @@ __global__ void __launch_bounds__(kST, 2) forward_pipelined_kernel(
 // only sums its ancestor chunks into its scratch slot and raises its flag.
 __device__ bool backward_block(const FrontDesc* __restrict__ fronts, const FrontState* __restrict__ st, int s, int cb,
                                bool helper, int a0, int a1, int hslot0, int nh, const int* __restrict__ flag_base,
-                               int* flags, int* hflags, double* hscratch, int epoch, int* err, int nc, int c0,
-                               double* __restrict__ X, int n, double* acc, double* xb, double* Lb0) {
+                               int* flags, int* hflags, double* hscratch, int epoch, int* err,
+                               unsigned long long wait_ns, int nc, int c0, double* __restrict__ X, int n, double* acc,
+                               double* xb, double* Lb0) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int NW = kST / 32;
   const int col = threadIdx.x % kRB, cg = threadIdx.x / kRB;
@@ -366,7 +377,7 @@ __device__ bool backward_block(const FrontDesc* __restrict__ fronts, const Front
       //    this front are waited for
       if (tt >= nanc) {
         const int j = nbp - 1 - (tt - nanc);
-        if (!wait_flag(flags, flag_base[s] + j, epoch, err)) {
+        if (!wait_flag(flags, flag_base[s] + j, epoch, err, wait_ns)) {
           scp_wait<0>();
           return false;
         }
@@ -405,7 +416,7 @@ __device__ bool backward_block(const FrontDesc* __restrict__ fronts, const Front
     } else {
       // helper parts' partial sums, in slot order (deterministic)
       for (int h = 0; h < nh; ++h) {
-        if (!wait_flag(hflags, hslot0 + h, epoch, err)) {
+        if (!wait_flag(hflags, hslot0 + h, epoch, err, wait_ns)) {
           scp_wait<0>();
           return false;
         }
@@ -468,7 +479,7 @@ __device__ bool backward_block(const FrontDesc* __restrict__ fronts, const Front
 __global__ void __launch_bounds__(kST, 2) backward_pipelined_kernel(
     const FrontDesc* __restrict__ fronts, const FrontState* __restrict__ st, const int4* __restrict__ tasks,
     int ntasks, const int* __restrict__ flag_base, int* flags, int* hflags, double* hscratch, int epoch, int* err,
-    int nrhs, int c0, double* __restrict__ X, int n) {
+    unsigned long long wait_ns, int nrhs, int c0, double* __restrict__ X, int n) {
   extern __shared__ double ssm[];
   double* acc = ssm;
   double* xb = acc + kRB * kAccStride;
@@ -484,14 +495,14 @@ __global__ void __launch_bounds__(kST, 2) backward_pipelined_kernel(
       const int nbp = (np + kRB - 1) / kRB;
       for (int cb = nbp - 1; cb >= 0; --cb)
         if (!backward_block(fronts, st, s, cb, false, 0, nanc, 0, 0, flag_base, flags, hflags, hscratch, epoch, err,
-                            nc, c0, X, n, acc, xb, Lb0))
+                            wait_ns, nc, c0, X, n, acc, xb, Lb0))
           return;
     } else {
       const int P = tk.w >> 20, slot = tk.w & ((1 << 20) - 1), p = tk.z;
       const int a0 = static_cast<int>(static_cast<long long>(nanc) * p / P);
       const int a1 = static_cast<int>(static_cast<long long>(nanc) * (p + 1) / P);
       if (!backward_block(fronts, st, s, tk.y, p > 0, a0, a1, slot, p > 0 ? 1 : P - 1, flag_base, flags, hflags,
-                          hscratch, epoch, err, nc, c0, X, n, acc, xb, Lb0))
+                          hscratch, epoch, err, wait_ns, nc, c0, X, n, acc, xb, Lb0))
         return;
     }
   }
@@ -510,12 +521,15 @@ __global__ void residual_kernel(int n, int nrhs, const int* __restrict__ rowptr,
   R[i + static_cast<long long>(c) * n] = B[i + static_cast<long long>(c) * ldb] - acc;
 }
 
+// The norms of the refinement propagate a NaN (the bit-pattern maximum of
+// non-negative values orders NaN above +Inf), so a non-finite residual or
+// solution can never read as converged.
 __global__ void absmax_kernel(const double* __restrict__ v, long long len, double* out) {
   double m = 0.0;
   for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < len;
        t += static_cast<long long>(gridDim.x) * blockDim.x)
-    m = fmax(m, fabs(v[t]));
-  m = warp_max(m);
+    m = nan_sticky_absmax(m, v[t]);
+  m = warp_max_nonneg(m);
   if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, m);
 }
 
@@ -525,7 +539,7 @@ __global__ void rowsum_max_kernel(int n, const int* __restrict__ srowptr, const 
   double s = 0.0;
   if (i < n)
     for (int e = srowptr[i]; e < srowptr[i + 1]; ++e) s += fabs(vals[svidx[e]]);
-  s = warp_max(s);
+  s = warp_max_nonneg(fabs(s));
   if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, s);
 }
 
@@ -573,23 +587,24 @@ cudaError_t solve_max_resident(int device, int* fwd_ctas, int* bwd_ctas) {
 
 cudaError_t launch_forward_pipelined(const FrontDesc* fronts, const ChildLink* links, const FrontState* st,
                                      const int4* tasks, int ntasks, int grid, const int* flag_base, int* flags,
-                                     int epoch, int* err, int nrhs, int c0, const double* Bp, int n,
-                                     cudaStream_t stream) {
+                                     int epoch, int* err, unsigned long long wait_ns, int nrhs, int c0,
+                                     const double* Bp, int n, cudaStream_t stream) {
   if (ntasks <= 0) return cudaSuccess;
   void* args[] = {(void*)&fronts, (void*)&links, (void*)&st,  (void*)&tasks, (void*)&ntasks,
-                  (void*)&flag_base, (void*)&flags, (void*)&epoch, (void*)&err, (void*)&nrhs,
-                  (void*)&c0,     (void*)&Bp,    (void*)&n};
+                  (void*)&flag_base, (void*)&flags, (void*)&epoch, (void*)&err, (void*)&wait_ns,
+                  (void*)&nrhs, (void*)&c0,     (void*)&Bp,    (void*)&n};
   return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(forward_pipelined_kernel), dim3(grid), dim3(kST),
                                      args, kSolveSmem, stream);
 }
 
 cudaError_t launch_backward_pipelined(const FrontDesc* fronts, const FrontState* st, const int4* tasks, int ntasks,
                                       int grid, const int* flag_base, int* flags, int* hflags, double* hscratch,
-                                      int epoch, int* err, int nrhs, int c0, double* X, int n, cudaStream_t stream) {
+                                      int epoch, int* err, unsigned long long wait_ns, int nrhs, int c0, double* X,
+                                      int n, cudaStream_t stream) {
   if (ntasks <= 0) return cudaSuccess;
   void* args[] = {(void*)&fronts, (void*)&st,    (void*)&tasks, (void*)&ntasks, (void*)&flag_base,
                   (void*)&flags,  (void*)&hflags, (void*)&hscratch, (void*)&epoch, (void*)&err,
-                  (void*)&nrhs,   (void*)&c0,    (void*)&X,     (void*)&n};
+                  (void*)&wait_ns, (void*)&nrhs,   (void*)&c0,    (void*)&X,     (void*)&n};
   return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(backward_pipelined_kernel), dim3(grid), dim3(kST),
                                      args, kSolveSmem, stream);
 }

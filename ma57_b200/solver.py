@@ -563,8 +563,9 @@ class SymLDLT:
         return list(buf)
 
     def plan_stats(self):
-        buf = (C.c_double * 11)()
-        L.load().symla_gpu_plan_stats(self._ctx.h, buf, 11)
+        buf = (C.c_double * 15)()
+        L.load().symla_gpu_plan_stats(self._ctx.h, buf, 15)
         keys = ["fronts", "levels", "max_m", "sum_m2", "factor_flops", "nnz_L", "arena_doubles",
-                "panels_spec_full", "panels_spec_prefix", "panels_spec_failed", "panels_sequential"]
+                "panels_spec_full", "panels_spec_prefix", "panels_spec_failed", "panels_sequential",
+                "seq_1x1_first_test", "seq_1x1_sigma_test", "seq_interchange", "seq_2x2"]
         return dict(zip(keys, list(buf)))
