@@ -225,7 +225,9 @@ extern "C" int symla_symbolic_import(int n, const int* perm, const int* etree_pa
 // Plan construction
 namespace {
 
-int pad_ld(int m) { return m; }
+// Leading dimension of a front: m rounded up to even, so that every column
+// of a front starts on a 16-byte boundary (bulk copies of whole columns).
+int pad_ld(int m) { return m + (m & 1); }
 
 // Builds invmap (length m_parent) and relmap (length cb) for child c of a
 // parent whose local row order is given by parentLocal (global -> local).
@@ -1044,7 +1046,7 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
   reset_to_static(c);
   const KernelOpts ko = make_kernel_opts(c, o);
   CK(cudaMemsetAsync(c->d_state, 0, c->numSN * sizeof(FrontState), st));
-  FactorGlobals g0{INT_MAX, 0, -1, INT_MAX, 0.0, 0.0, 0.0, 0, 0, 0, 0, c->wait_ns, {0, 0, 0, 0}};
+  FactorGlobals g0{INT_MAX, 0, -1, INT_MAX, 0.0, 0.0, 0.0, 0, 0, 0, 0, c->wait_ns, {0, 0, 0, 0}, 0};
   CK(cudaMemcpyAsync(c->d_glob, &g0, sizeof g0, cudaMemcpyHostToDevice, st));
   const bool mixed = o->precision == SYMLA_PREC_MIXED;
   if (mixed) {
@@ -1133,6 +1135,8 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
     c->panel_counts[2] = gp.spec_failed;
     c->panel_counts[3] = gp.seq_panels;
     for (int i = 0; i < 4; ++i) c->seq_dec_counts[i] = gp.seq_dec[i];
+    if (gp.error == kPanelErrTimeout)
+      throw SymlaError(SYMLA_ERR_TIMEOUT, "panel factorization: a bulk copy of the panel rows did not complete");
   }
   if (mixed) {
     int tcerr = 0;

@@ -77,6 +77,9 @@ __host__ __device__ inline bool tc_block_ok(int K, double lmax, double wmax, dou
 
 // Error word of the pipelined solve kernels.
 constexpr int kSolveErrTimeout = 1;
+// FactorGlobals::error: a panel's bulk staging of its rows did not complete
+// within the default wait limit.
+constexpr int kPanelErrTimeout = 3;
 // Error bits of the tensor-core Schur update: a pipeline wait ran out (the
 // CTA abandoned its tile), and the drain after such an abandonment could not
 // confirm that the CTA's copies and tensor-core operations had finished before
@@ -106,6 +109,7 @@ struct FactorGlobals {
   // first Bunch-Kaufman test (or an isolated column), 1x1 at k by the sigma
   // test, interchange then 1x1, 2x2
   int seq_dec[4];
+  int spec_restarts;  // speculative runs started after a sequential decision inside a panel
 };
 
 // Kernels of a level return at once when an earlier level stopped the

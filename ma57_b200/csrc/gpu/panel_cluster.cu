@@ -47,7 +47,8 @@ constexpr double kAlphaBK = 0.64038820320220756;  // (1 + sqrt(17)) / 8
 constexpr int kCT = 256;                           // threads per CTA
 constexpr int kNBMax = 34;                         // panel width + 2
 constexpr int kSpecMax = 32;                       // pivots per speculative panel (= panel width)
-constexpr int kSpecRetry = 2;                      // consecutive failures before a whole sequential panel
+constexpr int kSpecRetry = 2;                      // consecutive failed panel starts before one sequential decision first
+constexpr int kStageHalf = (kNBMax / 2) * (kNBMax / 2 + 1);  // >= np * p0 of any restart (np + p0 <= kNBMax)
 
 struct ClusterShared {
   double w[kNBMax];     // D * L(k, :)^T for the current pivot row
@@ -81,6 +82,41 @@ struct ClusterShared {
   double lamx[16][kSpecMax];          // per CTA partial lambda (exchange)
   int kstar;                          // accepted speculative pivots
 };
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long pc_global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// Bulk (TMA, non-tensor, no multicast) global -> own shared memory copy of
+// `bytes` (a multiple of 16; both addresses 16-byte aligned), completing on
+// the mbarrier's transaction count.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// Bounded wait for the mbarrier phase `parity` (at most kDefaultWaitNs of the
+// global timer, and as many probes); false on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  const unsigned long long t0 = pc_global_ns();
+  for (unsigned long long it = 0;; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (it > kDefaultWaitNs / 8 || ((it & 255) == 255 && pc_global_ns() - t0 > kDefaultWaitNs)) return false;
+  }
+}
 
 // 8-byte asynchronous global -> shared copy (no register round trip, so
 // the copies of a staging loop are all in flight at once)
@@ -120,7 +156,8 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     S.far = 0;
     S.flags &= ~kFlagFlush;
   }
-  extern __shared__ double dsm[];
+  extern __shared__ __align__(16) double dsm[];
+  __shared__ __align__(8) uint64_t rows_bar;  // bulk staging of the rows below the block
   __shared__ ClusterShared sh;
   const int m = f.m, effEnd = f.nelig;
   const int64_t ld = f.ld;
@@ -131,9 +168,22 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
   const int Rr = (span + CS - 1) / CS;  // rows per CTA (<= R)
   const int base = ps + q * Rr;
   const int rend = min(base + Rr, m);
-  double* Lr = dsm;                 // column-major: Lr[col * R + li]
-  double* vk = dsm + static_cast<size_t>(nb + 2) * R;
+  // Lr (column-major, Lr[col * R + li]), vk and vr start at the parity of
+  // this CTA's first row, so that a row's slot and its column entry in the
+  // front (16-byte aligned columns: even leading dimension) share their
+  // 16-byte alignment and whole columns can be staged by bulk copies; R is
+  // even with a spare slot past the last row.
+  auto lr_of = [&](int rank) { return dsm + ((ps + rank * Rr) & 1); };
+  double* Lr = lr_of(q);
+  double* vk = Lr + static_cast<size_t>(nb + 2) * R;
   double* vr = vk + R;
+  double* stage = dsm + 2 + static_cast<size_t>(nb + 4) * R;  // speculation restarts (2 kStageHalf)
+  uint32_t rows_phase = 0;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&rows_bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
 
   auto owner = [&](int i) { return (i - ps) / Rr; };
   auto remote = [&](auto* p, int rank) { return cluster.map_shared_rank(p, rank); };
@@ -230,7 +280,7 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     auto stage_row = [&](int row, double* dst, double* vdst) {
       const int oo = owner(row);
       const int lo = row - (ps + oo * Rr);
-      double* Lo = remote(dsm, oo);
+      double* Lo = remote(lr_of(oo), oo);
       const double* vko = Lo + static_cast<size_t>(nb + 2) * R;
       const double* vro = vko + R;
       for (int t = threadIdx.x; t < nb + 2; t += kCT) dst[t] = Lo[static_cast<size_t>(t) * R + lo];
@@ -262,232 +312,6 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
   bool flush = false;
   int step = 0;
 
-  // ---- speculative panel: 1x1 pivots at k, verified against lambda after
-  // the fact (see the file comment)
-  int spec = S.spec;
-  bool run_seq = true;
-  int spec_kind = 0;  // 0 no speculation, 1 all accepted, 2 a prefix, 3 none
-  const int np = pe - ps;
-  if (np > 0 && spec < kSpecRetry) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r0 = max(base, pe);
-    // raw diagonal block (lower triangle)
-    for (int j = 0; j < np; ++j)
-      for (int i = j + threadIdx.x; i < np; i += kCT) cp_async8(&sh.db[i][j], F + static_cast<int64_t>(ps + j) * ld + ps + i);
-    cp_async_commit();
-    // the raw panel columns of this CTA's rows below the block go to Lr
-    // while warp 0 factors the diagonal block
-    for (int c = 0; c < np; ++c)
-      for (int i = r0 + threadIdx.x; i < rend; i += kCT)
-        cp_async8(Lr + c * R + (i - base), F + static_cast<int64_t>(ps + c) * ld + i);
-    cp_async_commit();
-    cp_async_wait_but_newest();
-    __syncthreads();
-    // diagonal block, left-looking: warp 0 of every CTA, lane = row (the
-    // row lives in sh.db, conflict-free with the odd row stride). The sums
-    // use four partial accumulators to shorten the dependency chain; |a| of
-    // the column values go to shared memory and are reduced afterwards.
-    if (warp == 0) {
-      const double floorv = fmax(o.static_abs_floor, o.static_rel_floor * orig_max);
-      const int lr = lane < np ? lane : 0;
-      for (int c = 0; c < np; ++c) {
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        int t = 0;
-        for (; t + 4 <= c; t += 4) {
-          s0 = fma(sh.db[lr][t], sh.wv[c][t], s0);
-          s1 = fma(sh.db[lr][t + 1], sh.wv[c][t + 1], s1);
-          s2 = fma(sh.db[lr][t + 2], sh.wv[c][t + 2], s2);
-          s3 = fma(sh.db[lr][t + 3], sh.wv[c][t + 3], s3);
-        }
-        for (; t < c; ++t) s0 = fma(sh.db[lr][t], sh.wv[c][t], s0);
-        const double a = sh.db[lr][c] - ((s0 + s1) + (s2 + s3));
-        const double akk = __shfl_sync(0xffffffffu, a, c);
-        double d = akk, applied = 0.0;
-        if (o.mode == 1) {
-          // static pivoting (dense_kernel.hpp:982-1034), as in the sequential path
-          const int sign = o.sign_final ? o.sign_final[f.fidx[ps + c]] : 0;
-          bool need;
-          if (sign > 0)
-            need = akk < floorv;
-          else if (sign < 0)
-            need = akk > -floorv;
-          else
-            need = fabs(akk) < floorv;
-          if (need) {
-            const double sg = (sign != 0) ? static_cast<double>(sign) : (akk >= 0.0 ? 1.0 : -1.0);
-            d = akk + sg * S.delta;
-            applied = d - akk;
-          }
-        }
-        const double inv = __drcp_rn(d);
-        __syncwarp();
-        if (lane > c && lane < np) {
-          const double l = a * inv;
-          sh.db[lane][c] = l;
-          sh.aabs[c][lane] = fabs(a);
-          sh.wv[lane][c] = d * l;
-        } else if (lane == c) {
-          sh.db[c][c] = d;
-        }
-        if (lane == 0) {
-          sh.dv[c] = d;
-          sh.iv[c] = inv;
-          sh.pv[c] = applied;
-        }
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    // lambda and running-max parts of the diagonal-block rows
-    if (threadIdx.x < np) {
-      const int c = threadIdx.x;
-      double lm = 0.0, rv = fabs(sh.dv[c]);
-      for (int i = c + 1; i < np; ++i) {
-        const double v = sh.aabs[c][i];
-        if (ps + i < effEnd) lm = fmax(lm, v);
-        rv = fmax(rv, v);
-      }
-      sh.lamd[c] = lm;
-      sh.rmd[c] = rv;
-    }
-    // rows below the block, left-looking: the raw panel columns of this
-    // CTA's rows are in Lr (staged above), then each thread takes one row at a time
-    // into registers and walks it pivot by pivot, touching only its own
-    // rows, so no synchronisation is needed between pivots; the L(c, t) are
-    // warp-uniform (broadcast) shared loads. Lr receives the current values
-    // a_ic = raw_ic - sum_t a_it L_ct (L = a_ic / d_c on write-back). Columns
-    // past np compute unused values (column c depends on columns t < c only).
-    cp_async_wait_all();
-    __syncthreads();
-    for (int i = r0 + threadIdx.x; i < rend; i += kCT) {
-      const int li = i - base;
-      double a[kSpecMax];
-#pragma unroll
-      for (int c = 0; c < kSpecMax; ++c) a[c] = (c < np) ? Lr[c * R + li] : 0.0;
-#pragma unroll
-      for (int c = 1; c < kSpecMax; ++c) {
-        // sum_t L_it d_t L_ct = sum_t a_it L_ct (a_it = L_it d_t): even and
-        // odd t in two partial sums
-        double s0 = 0.0, s1 = 0.0;
-#pragma unroll
-        for (int t = 0; t < c; ++t) {
-          if (t & 1)
-            s1 = fma(a[t], sh.db[c][t], s1);
-          else
-            s0 = fma(a[t], sh.db[c][t], s0);
-        }
-        a[c] -= s0 + s1;
-        asm volatile("" ::: "memory");  // keep the next pivot's loads from being hoisted (registers)
-      }
-#pragma unroll
-      for (int c = 0; c < kSpecMax; ++c)
-        if (c < np) Lr[c * R + li] = a[c];
-    }
-    __syncthreads();
-    // per pivot and warp: lambda part (eligible rows) and running-max part
-    // (all rows) of this CTA's rows below the block
-    for (int c = warp; c < np; c += kCT / 32) {
-      double lm = 0.0, rv = 0.0;
-      for (int i = r0 + lane; i < rend; i += 32) {
-        const double v = fabs(Lr[c * R + (i - base)]);
-        if (i < effEnd) lm = fmax(lm, v);
-        rv = fmax(rv, v);
-      }
-      lm = warp_max_nonneg(lm);
-      rv = warp_max_nonneg(rv);
-      if (lane == 0) {
-        sh.lamw[0][c] = lm;
-        sh.rvw[0][c] = rv;
-      }
-    }
-    __syncthreads();
-    int kstar = np;
-    if (o.mode != 1) {
-      // lambda per pivot: this CTA's part to every CTA of the cluster
-      if (threadIdx.x < np) {
-        const double lc = sh.lamw[0][threadIdx.x];
-        for (int dd = 0; dd < CS; ++dd) *cluster.map_shared_rank(&sh.lamx[q][threadIdx.x], dd) = lc;
-      }
-      cluster.sync();
-      if (warp == 0) {
-        // the sequential path's 1x1-at-k decision (dense_kernel.hpp:576-600),
-        // one lane per pivot; the first failing pivot ends the accepted prefix
-        bool fail = false;
-        if (lane < np) {
-          const double isolatedFloor = fmax(o.zero_tol, o.rel_floor * orig_max);
-          double lam = sh.lamd[lane];
-          for (int dd = 0; dd < CS; ++dd) lam = fmax(lam, sh.lamx[dd][lane]);
-          const double akk = sh.dv[lane];
-          const bool pass = (lam <= o.zero_tol) ? (fabs(akk) > isolatedFloor) : (fabs(akk) >= kAlphaBK * lam);
-          fail = !pass;
-        }
-        const unsigned bad = __ballot_sync(0xffffffffu, fail);
-        if (lane == 0) sh.kstar = bad ? __ffs(bad) - 1 : np;
-      }
-      __syncthreads();
-      kstar = sh.kstar;
-    }
-    if (kstar > 0) {
-      for (int c = 0; c < kstar; ++c) {
-        const double iv = sh.iv[c];
-        for (int i = r0 + threadIdx.x; i < rend; i += kCT) F[static_cast<int64_t>(ps + c) * ld + i] = Lr[c * R + (i - base)] * iv;
-      }
-      if (q == 0) {
-        for (int c = 0; c < kstar; ++c)
-          for (int i = c + threadIdx.x; i < np; i += kCT) F[static_cast<int64_t>(ps + c) * ld + ps + i] = sh.db[i][c];
-        for (int c = threadIdx.x; c < kstar; c += kCT) {
-          f.Dd[ps + c] = sh.dv[c];
-          f.Do[ps + c] = 0.0;
-          f.pk[ps + c] = 0;
-        }
-      }
-      for (int c = 0; c < kstar; ++c) {
-        const double d = sh.dv[c];
-        if (d > 0)
-          ++n_pos;
-        else if (d < 0)
-          ++n_neg;
-        else
-          ++n_zero;
-        if (sh.pv[c] != 0.0) {
-          pert += fabs(sh.pv[c]);
-          ++nPert;
-        }
-      }
-      if (threadIdx.x < kstar) {
-        // running max of the accepted columns (one thread per column)
-        thread_rmax = fmax(thread_rmax, fmax(sh.rmd[threadIdx.x], sh.rvw[0][threadIdx.x]));
-      }
-      k = ps + kstar;
-      run_seq = false;
-      spec = 0;
-      spec_kind = kstar == np ? 1 : 2;
-      if (kstar < np) {
-        // Continue in this launch from the failing pivot with the sequential
-        // path, which needs for the accepted pivots: L of this CTA's rows in
-        // Lr (below the block: a / d as written to F; block rows: sh.db), D
-        // in sh.Dd/Do/pk, and w = D L(k, :)^T of the next row (sh.wv[kstar]).
-        for (int c = 0; c < kstar; ++c) {
-          const double iv = sh.iv[c];
-          for (int i = r0 + threadIdx.x; i < rend; i += kCT) Lr[c * R + (i - base)] *= iv;
-          for (int i = max(base, ps + c + 1) + threadIdx.x; i < min(rend, pe); i += kCT)
-            Lr[c * R + (i - base)] = sh.db[i - ps][c];
-        }
-        if (threadIdx.x < kstar) {
-          sh.Dd[threadIdx.x] = sh.dv[threadIdx.x];
-          sh.Do[threadIdx.x] = 0.0;
-          sh.pk[threadIdx.x] = 0;
-          sh.w[threadIdx.x] = sh.wv[kstar][threadIdx.x];
-        }
-        __syncthreads();
-        run_seq = true;  // finish the panel here
-      }
-    } else {
-      spec += 1;  // the whole panel on the sequential path
-      spec_kind = 3;
-    }
-  }
-  int nontrivial = 0;
   // prefetched raw values of column k for this thread's rows
   constexpr int kPF = 4;
   double pf[kPF];
@@ -562,7 +386,310 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     }
   };
 
-  while (run_seq && k < pe) {
+  // ---- the panel: speculative runs of 1x1 pivots at k, verified against
+  // lambda after the fact (see the file comment), and one sequential
+  // decision at each pivot where a run stopped; a sequential decision that
+  // turns out to be a plain 1x1 at k starts the next speculative run (a
+  // restart: the panel's earlier pivots enter as a rank-p0 correction of the
+  // restart's columns).
+  int spec_carry = S.spec;  // consecutive panels whose first speculation failed at its first pivot
+  bool try_spec = spec_carry < kSpecRetry;
+  bool first_spec = true, spec_tried = false, any_seq = false, any_accept = false;
+  int restarts = 0;
+  double* lblk = stage;               // restart: L of the block rows for the earlier pivots (np x p0)
+  double* wblk = stage + kStageHalf;  // restart: D L(block row, :)^T (np x p0)
+  while (k < pe) {
+    if (try_spec) {
+      try_spec = false;
+      spec_tried = true;
+      const int k0 = k, p0 = k0 - ps, np = pe - k0;
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      const int r0 = max(base, pe);
+      if (!first_spec) ++restarts;
+      pf_col = -1;
+      // warp 0 stages the raw diagonal block (lower triangle) and factors it
+      // as soon as it lands; warps 1.. stage the raw block columns of this
+      // CTA's rows below the block into Lr (columns p0 ..) meanwhile
+      // rows [s0, e0): the CTA's rows below the block widened to whole
+      // 16-byte pairs (the extra slot before r0 and after rend is spare)
+      const int s0 = r0 & ~1, e0 = (rend + 1) & ~1;
+      const bool have_rows = r0 < rend;
+      if (warp == 0) {
+        for (int j = 0; j < np; ++j)
+          for (int i = j + lane; i < np; i += 32) cp_async8(&sh.db[i][j], F + static_cast<int64_t>(k0 + j) * ld + k0 + i);
+        cp_async_commit();
+      } else if (threadIdx.x == 32 && have_rows) {
+        const uint32_t bytes = static_cast<uint32_t>(e0 - s0) * sizeof(double);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&rows_bar)),
+                     "r"(bytes * static_cast<uint32_t>(np))
+                     : "memory");
+        for (int c = 0; c < np; ++c)
+          bulk_copy_g2s(Lr + (p0 + c) * R + (s0 - base), F + static_cast<int64_t>(k0 + c) * ld + s0, bytes, &rows_bar);
+      }
+      if (p0 > 0) {
+        // restart: every CTA receives the L rows of the block from their
+        // owners and forms W = D L_blk^T itself (D is replicated)
+        const int lo = max(base, k0), hi = min(rend, pe);
+        const int cnt = hi > lo ? (hi - lo) * p0 : 0;
+        for (int t = threadIdx.x; t < cnt; t += kCT) {
+          const int i = lo + t / p0, tt = t % p0;
+          const double v = Lr[tt * R + (i - base)];
+          for (int dd = 0; dd < CS; ++dd) remote(lblk, dd)[(i - k0) * p0 + tt] = v;
+        }
+        __threadfence();
+        cluster.sync();
+        for (int t = threadIdx.x; t < np * p0; t += kCT) {
+          const double* lr = lblk + (t / p0) * p0;
+          const int tt = t % p0;
+          const int kind = sh.pk[tt];
+          double v;
+          if (kind == 0)
+            v = sh.Dd[tt] * lr[tt];
+          else if (kind == 1)
+            v = sh.Dd[tt] * lr[tt] + sh.Do[tt] * lr[tt + 1];
+          else
+            v = sh.Do[tt - 1] * lr[tt - 1] + sh.Dd[tt] * lr[tt];
+          wblk[t] = v;
+        }
+      }
+      if (p0 > 0) __syncthreads();  // wblk complete before any warp reads it
+      if (warp == 0) {
+        cp_async_wait_all();
+        __syncwarp();
+        if (p0 > 0) {
+          // current values of the diagonal block: raw - L_blk W^T
+          for (int t = lane; t < np * np; t += 32) {
+            const int i = t / np, j = t % np;
+            if (j <= i) {
+              double acc = 0.0;
+              for (int tt = 0; tt < p0; ++tt) acc += lblk[i * p0 + tt] * wblk[j * p0 + tt];
+              sh.db[i][j] -= acc;
+            }
+          }
+          __syncwarp();
+        }
+      } else {
+        if (have_rows) {
+          if (!mbar_wait_bounded(&rows_bar, rows_phase)) {
+            atomicCAS(&g->error, 0, kPanelErrTimeout);
+            mbar_wait_bounded(&rows_bar, rows_phase);  // the copies must land before the CTA moves on
+          }
+        }
+        if (p0 > 0) {
+          // this warp's own staged rows: subtract the earlier pivots, L_row W^T
+          for (int c = 0; c < np; ++c)
+            for (int i = r0 + threadIdx.x - 32; i < rend; i += kCT - 32) {
+              const int li = i - base;
+              double acc = 0.0;
+              for (int tt = 0; tt < p0; ++tt) acc += Lr[tt * R + li] * wblk[c * p0 + tt];
+              Lr[(p0 + c) * R + li] -= acc;
+            }
+        }
+      }
+      if (have_rows) rows_phase ^= 1;  // every thread: the barrier's phase of this staging is consumed
+      // diagonal block, left-looking: warp 0 of every CTA, lane = row (the
+      // row lives in sh.db, conflict-free with the odd row stride). The sums
+      // use four partial accumulators to shorten the dependency chain; |a| of
+      // the column values go to shared memory and are reduced afterwards.
+      if (warp == 0) {
+        const double floorv = fmax(o.static_abs_floor, o.static_rel_floor * orig_max);
+        const int lr = lane < np ? lane : 0;
+        for (int c = 0; c < np; ++c) {
+          double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+          int t = 0;
+          for (; t + 4 <= c; t += 4) {
+            s0 = fma(sh.db[lr][t], sh.wv[c][t], s0);
+            s1 = fma(sh.db[lr][t + 1], sh.wv[c][t + 1], s1);
+            s2 = fma(sh.db[lr][t + 2], sh.wv[c][t + 2], s2);
+            s3 = fma(sh.db[lr][t + 3], sh.wv[c][t + 3], s3);
+          }
+          for (; t < c; ++t) s0 = fma(sh.db[lr][t], sh.wv[c][t], s0);
+          const double a = sh.db[lr][c] - ((s0 + s1) + (s2 + s3));
+          const double akk = __shfl_sync(0xffffffffu, a, c);
+          double d = akk, applied = 0.0;
+          if (o.mode == 1) {
+            // static pivoting (dense_kernel.hpp:982-1034), as in the sequential path
+            const int sign = o.sign_final ? o.sign_final[f.fidx[k0 + c]] : 0;
+            bool need;
+            if (sign > 0)
+              need = akk < floorv;
+            else if (sign < 0)
+              need = akk > -floorv;
+            else
+              need = fabs(akk) < floorv;
+            if (need) {
+              const double sg = (sign != 0) ? static_cast<double>(sign) : (akk >= 0.0 ? 1.0 : -1.0);
+              d = akk + sg * S.delta;
+              applied = d - akk;
+            }
+          }
+          const double inv = __drcp_rn(d);
+          __syncwarp();
+          if (lane > c && lane < np) {
+            const double l = a * inv;
+            sh.db[lane][c] = l;
+            sh.aabs[c][lane] = fabs(a);
+            sh.wv[lane][c] = d * l;
+          } else if (lane == c) {
+            sh.db[c][c] = d;
+          }
+          if (lane == 0) {
+            sh.dv[c] = d;
+            sh.iv[c] = inv;
+            sh.pv[c] = applied;
+          }
+          __syncwarp();
+        }
+      }
+      __syncthreads();
+      // lambda and running-max parts of the diagonal-block rows
+      if (threadIdx.x < np) {
+        const int c = threadIdx.x;
+        double lm = 0.0, rv = fabs(sh.dv[c]);
+        for (int i = c + 1; i < np; ++i) {
+          const double v = sh.aabs[c][i];
+          if (k0 + i < effEnd) lm = fmax(lm, v);
+          rv = fmax(rv, v);
+        }
+        sh.lamd[c] = lm;
+        sh.rmd[c] = rv;
+      }
+      // rows below the block, left-looking: the raw block columns of this
+      // CTA's rows are in Lr (staged above; a restart first subtracts the
+      // earlier pivots, L_row W^T), then each thread takes one row at a time
+      // into registers and walks it pivot by pivot, touching only its own
+      // rows, so no synchronisation is needed between pivots; the L(c, t) are
+      // warp-uniform (broadcast) shared loads. Lr receives the current values
+      // a_ic = raw_ic - sum_t a_it L_ct (L = a_ic / d_c on write-back). Columns
+      // past np compute unused values (column c depends on columns t < c only).
+      for (int i = r0 + threadIdx.x; i < rend; i += kCT) {
+        const int li = i - base;
+        double a[kSpecMax];
+#pragma unroll
+        for (int c = 0; c < kSpecMax; ++c) a[c] = (c < np) ? Lr[(p0 + c) * R + li] : 0.0;
+#pragma unroll
+        for (int c = 1; c < kSpecMax; ++c) {
+          // sum_t L_it d_t L_ct = sum_t a_it L_ct (a_it = L_it d_t): even and
+          // odd t in two partial sums
+          double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+          for (int t = 0; t < c; ++t) {
+            if (t & 1)
+              s1 = fma(a[t], sh.db[c][t], s1);
+            else
+              s0 = fma(a[t], sh.db[c][t], s0);
+          }
+          a[c] -= s0 + s1;
+          asm volatile("" ::: "memory");  // keep the next pivot's loads from being hoisted (registers)
+        }
+#pragma unroll
+        for (int c = 0; c < kSpecMax; ++c)
+          if (c < np) Lr[(p0 + c) * R + li] = a[c];
+      }
+      __syncthreads();
+      // per pivot and warp: lambda part (eligible rows) and running-max part
+      // (all rows) of this CTA's rows below the block
+      for (int c = warp; c < np; c += kCT / 32) {
+        double lm = 0.0, rv = 0.0;
+        for (int i = r0 + lane; i < rend; i += 32) {
+          const double v = fabs(Lr[(p0 + c) * R + (i - base)]);
+          if (i < effEnd) lm = fmax(lm, v);
+          rv = fmax(rv, v);
+        }
+        lm = warp_max_nonneg(lm);
+        rv = warp_max_nonneg(rv);
+        if (lane == 0) {
+          sh.lamw[0][c] = lm;
+          sh.rvw[0][c] = rv;
+        }
+      }
+      __syncthreads();
+      int kstar = np;
+      if (o.mode != 1) {
+        // lambda per pivot: this CTA's part to every CTA of the cluster
+        if (threadIdx.x < np) {
+          const double lc = sh.lamw[0][threadIdx.x];
+          for (int dd = 0; dd < CS; ++dd) *cluster.map_shared_rank(&sh.lamx[q][threadIdx.x], dd) = lc;
+        }
+        cluster.sync();
+        if (warp == 0) {
+          // the sequential path's 1x1-at-k decision (dense_kernel.hpp:576-600),
+          // one lane per pivot; the first failing pivot ends the accepted prefix
+          bool fail = false;
+          if (lane < np) {
+            const double isolatedFloor = fmax(o.zero_tol, o.rel_floor * orig_max);
+            double lam = sh.lamd[lane];
+            for (int dd = 0; dd < CS; ++dd) lam = fmax(lam, sh.lamx[dd][lane]);
+            const double akk = sh.dv[lane];
+            const bool pass = (lam <= o.zero_tol) ? (fabs(akk) > isolatedFloor) : (fabs(akk) >= kAlphaBK * lam);
+            fail = !pass;
+          }
+          const unsigned bad = __ballot_sync(0xffffffffu, fail);
+          if (lane == 0) sh.kstar = bad ? __ffs(bad) - 1 : np;
+        }
+        __syncthreads();
+        kstar = sh.kstar;
+      }
+      if (first_spec) spec_carry = kstar > 0 ? 0 : spec_carry + 1;
+      first_spec = false;
+      if (kstar > 0) {
+        any_accept = true;
+        for (int c = 0; c < kstar; ++c) {
+          const double iv = sh.iv[c];
+          for (int i = r0 + threadIdx.x; i < rend; i += kCT)
+            F[static_cast<int64_t>(k0 + c) * ld + i] = Lr[(p0 + c) * R + (i - base)] * iv;
+        }
+        if (q == 0) {
+          for (int c = 0; c < kstar; ++c)
+            for (int i = c + threadIdx.x; i < np; i += kCT) F[static_cast<int64_t>(k0 + c) * ld + k0 + i] = sh.db[i][c];
+          for (int c = threadIdx.x; c < kstar; c += kCT) {
+            f.Dd[k0 + c] = sh.dv[c];
+            f.Do[k0 + c] = 0.0;
+            f.pk[k0 + c] = 0;
+          }
+        }
+        for (int c = 0; c < kstar; ++c) {
+          const double d = sh.dv[c];
+          if (d > 0)
+            ++n_pos;
+          else if (d < 0)
+            ++n_neg;
+          else
+            ++n_zero;
+          if (sh.pv[c] != 0.0) {
+            pert += fabs(sh.pv[c]);
+            ++nPert;
+          }
+        }
+        if (threadIdx.x < kstar) {
+          // running max of the accepted columns (one thread per column)
+          thread_rmax = fmax(thread_rmax, fmax(sh.rmd[threadIdx.x], sh.rvw[0][threadIdx.x]));
+        }
+        k = k0 + kstar;
+        if (k < pe) {
+          // The sequential decision at k needs, for the accepted pivots: L
+          // of this CTA's rows in Lr (below the block: a / d as written to F;
+          // block rows: sh.db), D in sh.Dd/Do/pk, and w = D L(k, :)^T (the
+          // earlier pivots' part from wblk, the run's part from sh.wv).
+          for (int c = 0; c < kstar; ++c) {
+            const double iv = sh.iv[c];
+            for (int i = r0 + threadIdx.x; i < rend; i += kCT) Lr[(p0 + c) * R + (i - base)] *= iv;
+            for (int i = max(base, k0 + c + 1) + threadIdx.x; i < min(rend, pe); i += kCT)
+              Lr[(p0 + c) * R + (i - base)] = sh.db[i - k0][c];
+          }
+          if (threadIdx.x < kstar) {
+            sh.Dd[p0 + threadIdx.x] = sh.dv[threadIdx.x];
+            sh.Do[p0 + threadIdx.x] = 0.0;
+            sh.pk[p0 + threadIdx.x] = 0;
+            sh.w[p0 + threadIdx.x] = sh.wv[kstar][threadIdx.x];
+          }
+          for (int t = threadIdx.x; t < p0; t += kCT) sh.w[t] = wblk[kstar * p0 + t];
+          __syncthreads();
+        }
+      }
+      if (k >= pe) break;
+    }
+    any_seq = true;
     const int p = k - ps;
     const int b = step & 1;
     ++step;
@@ -624,6 +751,7 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
       if (haveNext) local_w_next(p, d, sh.fx_row[b], sh.fx_k1[b]);
       __syncthreads();
       ++k;
+      try_spec = true;
       continue;
     }
 
@@ -685,7 +813,6 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
       cluster.sync();
     }
     if (q == 0 && threadIdx.x == 0 && dec <= 2) atomicAdd(&g->seq_dec[dec_kind], 1);
-    if (dec != 0) ++nontrivial;
     if (dec == 3) {
       stopped = true;
       break;
@@ -699,6 +826,8 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
       if (haveNext) local_w_next(p, akk, sh.fx_row[b], sh.fx_k1[b]);
       __syncthreads();
       k += 1;
+      // a plain 1x1 at k by the first test: the next pivots likely are too
+      try_spec = dec_kind == 0;
       continue;
     }
     pf_col = -1;  // an interchange invalidates the prefetched column
@@ -802,14 +931,13 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
     W.ob = S.ob;
     W.ob_end = S.ob_end;
     W.far = (done || flush || k >= S.ob_end) ? 1 : 0;
-    // a whole sequential panel without interchanges or 2x2 pivots: try
-    // speculation again next time
-    W.spec = (spec >= kSpecRetry && run_seq && nontrivial == 0) ? 0 : spec;
-    int* counter = spec_kind == 1 ? &g->spec_full
-                   : spec_kind == 2 ? &g->spec_partial
-                   : spec_kind == 3 ? &g->spec_failed
-                                    : &g->seq_panels;
+    W.spec = spec_carry < kSpecRetry ? spec_carry : kSpecRetry;
+    int* counter = !spec_tried ? &g->seq_panels
+                   : !any_seq  ? &g->spec_full
+                   : any_accept ? &g->spec_partial
+                                : &g->spec_failed;
     atomicAdd(counter, 1);
+    if (restarts) atomicAdd(&g->spec_restarts, restarts);
     int flags = flush ? kFlagFlush : 0;
     if (done) {
       flags |= kFlagDone;
@@ -829,10 +957,20 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
   cluster.sync();
 }
 
+// Rows per CTA slot of the cluster panel's shared arrays: the rows a CTA
+// holds, plus a spare slot at each end of a column for the 16-byte widened
+// bulk copies, rounded to even.
+int cluster_rows(int max_m, int cs) { return (((max_m + cs - 1) / cs) + 2 + 1) & ~1; }
+
+size_t cluster_panel_smem(int max_m, int nb, int cs) {
+  const int R = cluster_rows(max_m, cs);
+  return (2 + static_cast<size_t>(nb + 4) * R + 2 * kStageHalf) * sizeof(double);
+}
+
 bool cluster_size_fits(int max_m, int cs, int nb) {
   const size_t limit = 184 * 1024;  // + the static ClusterShared (~38 KB) <= 227 KB
   return (cs == 2 || cs == 4 || cs == 8 || cs == 16) && nb >= 1 && nb <= kNBMax - 2 &&
-         static_cast<size_t>((max_m + cs - 1) / cs) * (nb + 4) * sizeof(double) <= limit;
+         cluster_panel_smem(max_m, nb, cs) <= limit;
 }
 
 int panel_width_for(int max_m, int count) {
@@ -862,11 +1000,6 @@ int cluster_size_for(int max_m, int count, int nb) {
   return best;  // 0: too large for the cluster kernel
 }
 
-size_t cluster_panel_smem(int max_m, int nb, int cs) {
-  const int R = (max_m + cs - 1) / cs;
-  return static_cast<size_t>(nb + 4) * R * sizeof(double);
-}
-
 cudaError_t configure_cluster_panel() {
   cudaError_t e = cudaFuncSetAttribute(cluster_panel_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 184 * 1024);
   if (e != cudaSuccess) return e;
@@ -885,7 +1018,7 @@ cudaError_t launch_cluster_panel(const FrontDesc* fronts, FrontState* st, const 
   if (count <= 0) return cudaSuccess;
   const int cs = cluster_size_fits(max_m, cs_choice, nb) ? cs_choice : cluster_size_for(max_m, count, nb);
   if (cs == 0) return cudaErrorInvalidValue;
-  const int R = (max_m + cs - 1) / cs;
+  const int R = cluster_rows(max_m, cs);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cs * count);
   cfg.blockDim = dim3(kCT);
