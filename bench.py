@@ -15,8 +15,12 @@ not shard, so N GPUs run N independent replicas). e2e = the same step through
 the C ABI with host buffers, host<->device copies included.
 
 --impl reference times the project's CPU restatement of the reference
-(oracle/) on the host cores: the reference itself needs Eigen, SuiteSparse AMD
-and LAPACK, none of which are installed, so it cannot be built here.
+(oracle/: the reference's dense kernel, multifrontal driver, OpenMP task DAG,
+solve and refinement) on the host cores, on the same 64^3 workload, one
+whole factorize + solve + refinement per timed step: the reference itself
+needs Eigen, SuiteSparse AMD and LAPACK, none of which are installed, so it
+cannot be built here. Its host analysis is compiled into the oracle library
+from the same sources, so that arm does not load the product library.
 """
 from __future__ import annotations
 
@@ -90,6 +94,12 @@ def clocks_stop(handle):
             "samples": len(sms)}
 
 
+def shared_config(k, nrhs):
+    """The workload keys both arms report (identical in the two lines)."""
+    return {"workload": f"L27({k}^3)-3I (n={k ** 3}), METIS ND, nrhs={nrhs}, factorize+solve+refine to 1e-12",
+            "n": k ** 3, "nrhs": nrhs, "ordering": "metis", "target_backward_error": 1e-12}
+
+
 def build_problem(k, nrhs):
     from ma57_b200 import matrices as M
     A, B = M.config3(k, nrhs=nrhs)
@@ -98,15 +108,9 @@ def build_problem(k, nrhs):
 
 def cpu_reference(k_sample: int, nrhs: int, reps: int, flop_ratio_to: int | None):
     """Oracle (CPU restatement) factorize + solve + refine on cfg3 at k_sample."""
-    import numpy as np
-    from ma57_b200 import OrderingType, SymLDLT
-    from ma57_b200.solver import as_csc
-    from oracle.pyoracle import OracleSymLDLT
+    from oracle.pyoracle import OracleSymLDLT, analyze
     A, B = build_problem(k_sample, nrhs)
-    s = SymLDLT()
-    s.setOrdering(OrderingType.Metis)
-    s.analyzePattern(A)
-    o = OracleSymLDLT(s.symbolicFactor())
+    o = OracleSymLDLT(analyze(A, 1))
     threads = os.cpu_count() or 1
     o.set(parallel=1, num_threads=threads)
     times = []
@@ -152,23 +156,6 @@ def panel_bytes(k):
         if m > 128:
             b += 16.0 * (m * p - p * (p - 1) / 2.0)
     return b
-
-
-def profiled_traffic(kind, units_per_launch):
-    """DRAM bytes per launch of a kernel kind, from the committed ncu summary
-    (profiles/traffic.md: lines 'kind: <kind> dram_bytes_per_unit: <r>', r =
-    measured DRAM bytes of the captured launch / its algorithmic units, flops
-    or bytes), scaled to this run's algorithmic units per launch; or None."""
-    path = os.path.join(ROOT, "profiles", "traffic.md")
-    try:
-        with open(path) as f:
-            for line in f:
-                parts = line.replace("`", "").split()
-                if len(parts) >= 4 and parts[0] == "kind:" and parts[1] == kind and parts[2] == "dram_bytes_per_unit:":
-                    return float(parts[3]) * units_per_launch
-    except OSError:
-        pass
-    return None
 
 
 def run_dense(args):
@@ -378,24 +365,61 @@ def run_learned(args):
 
 
 def run_reference(args):
+    """The reference's CPU path (the oracle restatement, OpenMP task DAG on
+    every host core) on the same workload: each timed step is one whole
+    factorize + multi-RHS solve + refinement to 1e-12 of L27(k^3) - 3I. The
+    analysis (METIS ordering, elimination tree, supernodes) is outside the
+    timed region, as in the GPU arm. One step takes minutes on the host, so
+    the arm times as many of the requested steps as fit in --ref-budget
+    seconds (at least one) and reports the count it ran."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    k_sample = args.cpu_k
-    best, threads, err = cpu_reference(k_sample, args.nrhs, max(1, args.steps), None)
-    ratio = algorithmic_flops(args.k) / algorithmic_flops(k_sample)
-    value = best * ratio
+    import numpy as np
+    from oracle.pyoracle import OracleSymLDLT, analyze
+    threads = os.cpu_count() or 1
+    # warm-up: thread pool and code paths on a small instance (untimed)
+    for _ in range(max(0, args.warmup)):
+        As, Bs = build_problem(12, args.nrhs)
+        o = OracleSymLDLT(analyze(As, 1))
+        o.set(parallel=1, num_threads=threads)
+        o.factorize(As)
+        o.solveWithRefinement(As, Bs, tolerance=1e-12)
+    A, B = build_problem(args.k, args.nrhs)
+    t0 = time.perf_counter()
+    sf = analyze(A, 1)
+    t_analyze = time.perf_counter() - t0
+    o = OracleSymLDLT(sf)
+    o.set(parallel=1, num_threads=threads)
+    times, fac, sol = [], [], []
+    info = d = None
+    t_start = time.perf_counter()
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        o.factorize(A)
+        t1 = time.perf_counter()
+        x, d = o.solveWithRefinement(A, B, tolerance=1e-12)
+        t2 = time.perf_counter()
+        times.append(t2 - t0)
+        fac.append(t1 - t0)
+        sol.append(t2 - t1)
+        info = o.info()
+        if time.perf_counter() - t_start + times[-1] > args.ref_budget:
+            break
+    value = statistics.mean(times)
+    inertia = [info["n_pos"], info["n_neg"], info["n_zero"]]
+    sample = (f"oracle (CPU restatement of the reference; Eigen/SuiteSparse/LAPACK absent) on the full workload, "
+              f"{len(times)} of {args.steps} requested steps (each step minutes long), {threads} OpenMP threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"L27({args.k}^3)-3I (n={args.k ** 3}), METIS ND, nrhs={args.nrhs}, "
-                               f"factorize+solve+refine to 1e-12", "parallelism": "cpu-openmp-task-dag"},
-        "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port",
-                         "sample": f"oracle (CPU restatement; the reference needs Eigen/SuiteSparse/LAPACK, absent) "
-                                   f"factorize+solve+refine on L27({k_sample}^3)-3I, best of {max(1, args.steps)}, "
-                                   f"{best:.3f} s, scaled by the algorithmic flop ratio {ratio:.1f} to {args.k}^3; "
-                                   f"final backward error {err:.2e}"},
+        "steps": len(times), "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": shared_config(args.k, args.nrhs),
+        "details": {"parallelism": f"cpu openmp task dag x{threads}", "analyze_s": t_analyze,
+                    "factorize_s": statistics.mean(fac), "solve_refine_s": statistics.mean(sol),
+                    "inertia": inertia, "backward_error": d["final"], "refine_iterations": d["iterations"],
+                    "warmup": "small instance L27(12^3), untimed"},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -456,6 +480,19 @@ def run_ours(args):
         check(lib.symla_gpu_solve_refine(h, pv, pB, n, nrhs, pX, n, 1, 10, 1e-12, C.byref(rinfo)))
 
     lib.symla_gpu_set_graph(h, int(args.graph))
+
+    def timed_steps(count):
+        """count steps between CUDA events on the library's stream."""
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(count):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) / count
+
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -463,19 +500,32 @@ def run_ours(args):
         dist.barrier()
     lib.symla_gpu_reset_kernel_stats(h)
     clk = clocks_start(local)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    ev0.record(stream)
-    errs = []
-    for _ in range(args.steps):
-        step()
-        errs.append(rinfo.final_relative_residual)
-    ev1.record(stream)
-    torch.cuda.synchronize()
+    ms = timed_steps(args.steps)
     clocks = clocks_stop(clk)
     launches = int(lib.symla_gpu_launch_count(h)) // max(1, args.steps)
-    ms = ev0.elapsed_time(ev1) / args.steps
+    inertia = [info.n_pos, info.n_neg, info.n_zero]
+    refine_iters = rinfo.iterations
+    # the metric's comparison: the same steps with the mixed-precision Schur
+    # update (TF32x3 tensor cores, FP64 pivots and refinement), timed alike
+    comparison = None
+    if not args.no_mixed:
+        other = L.PREC_MIXED if prec == L.PREC_FP64 else L.PREC_FP64
+        opts.precision = other
+        for _ in range(args.warmup):
+            step()
+        ms_other = timed_steps(args.steps)
+        name = "mixed" if other == L.PREC_MIXED else "fp64"
+        comparison = {f"{name}_s": ms_other / 1e3, f"{args.precision}_s": ms / 1e3,
+                      "mixed_over_fp64": (ms_other / ms) if other == L.PREC_MIXED else (ms / ms_other),
+                      f"{name}_inertia": [info.n_pos, info.n_neg, info.n_zero],
+                      f"{name}_refine_iterations": rinfo.iterations,
+                      f"{name}_backward_error": rinfo.final_relative_residual,
+                      "target": "mixed at least 3x faster than fp64 (mixed_over_fp64 <= 1/3)"}
+        opts.precision = prec
+        for _ in range(max(1, args.warmup)):
+            step()
+        torch.cuda.synchronize()
+
     # per-kernel breakdown from extra, instrumented steps (CUDA events around
     # every launch), kept out of the timed region above
     lib.symla_gpu_reset_kernel_stats(h)
@@ -535,11 +585,14 @@ def run_ours(args):
             # for it; measure the FP64 tensor peak of this GPU the same way
             # (register-only MMA loop), and give the bf16 fraction beside it
             fp64 = C.c_double()
-            check(lib.symla_gpu_measure_fp64_tensor_peak(local, C.byref(fp64)))
+            blib = C.CDLL(os.path.join(ROOT, "ma57_b200", "lib", "libsymla_bench.so"))
+            blib.symla_bench_fp64_tensor_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+            if blib.symla_bench_fp64_tensor_peak(local, C.byref(fp64)) != 0:
+                raise RuntimeError("FP64 tensor peak probe failed")
             peak = fp64.value
             roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                        "peak_source": "FP64 DMMA (mma.sync .f64) register-only loop, measured live on this GPU; "
-                                       "no FP64 figure in MEASURED_PEAKS.json",
+                        "peak_source": "FP64 DMMA (mma.sync .f64) register-only loop, measured live on this GPU "
+                                       "(bench tooling, libsymla_bench.so); no FP64 figure in MEASURED_PEAKS.json",
                         "frac_of_bf16_peak": achieved / bf16 if bf16 else None,
                         "algorithmic_flops_per_launch": flops_k / max(1, launches_k)}
         else:
@@ -553,8 +606,7 @@ def run_ours(args):
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "peak_source": f"HBM copy, {peak_kind}",
                     "algorithmic_bytes_per_launch": bytes_k / max(1, launches_k)}
-    units = (flops_k if roofline["unit"] == "TFLOP/s" else bytes_k) / max(1, launches_k)
-    roofline.update({"frac": achieved / peak if peak else None, "traffic": profiled_traffic(dom, units), "kernel": dom,
+    roofline.update({"frac": achieved / peak if peak else None, "traffic": None, "kernel": dom,
                      "launches_per_step": launches_k / steps, "ms_per_step": ms_k / steps,
                      "avg_launch_us": 1e3 * ms_k / max(1, launches_k)})
 
@@ -562,13 +614,14 @@ def run_ours(args):
         "metric": METRIC, "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if prec == L.PREC_FP64 else "f64+mixed-schur", "data": "synthetic",
-        "config": {"workload": f"L27({args.k}^3)-3I (n={n}), METIS ND, nrhs={nrhs}, factorize+solve+refine to 1e-12",
-                   "precision": args.precision, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (fronts 11 GB)", "inertia": [info.n_pos, info.n_neg, info.n_zero],
-                   "backward_error": bw, "refine_iterations": rinfo.iterations,
-                   "analyze_s": t_analyze, "factor_flops": stats.get("factor_flops"),
-                   "kernel_ms_per_step": {k: v[1] / max(1, args.steps) for k, v in kstats.items()},
-                   "panels": {k: v for k, v in stats.items() if k.startswith("panels_")}},
+        "config": shared_config(args.k, nrhs),
+        "details": {"precision": args.precision, "parallelism": f"replicas x{world}",
+                    "l2": "inputs larger than L2 (fronts 11 GB)", "inertia": inertia,
+                    "backward_error": bw, "refine_iterations": refine_iters,
+                    "analyze_s": t_analyze, "factor_flops": stats.get("factor_flops"),
+                    "kernel_ms_per_step": {k: v[1] / max(1, args.steps) for k, v in kstats.items()},
+                    "panels": {k: v for k, v in stats.items() if k.startswith("panels_") or k.startswith("seq_")}},
+        "precision_comparison": comparison,
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(8 * (2 * len(vals) + n * nrhs)),
                 "d2h_bytes_per_step": int(8 * n * nrhs)},
         "gpu_launches": launches,
@@ -579,8 +632,9 @@ def run_ours(args):
         best, threads, err = cpu_reference(args.cpu_k, nrhs, 2, None)
         ratio = algorithmic_flops(args.k) / algorithmic_flops(args.cpu_k)
         line["cpu_baseline"] = {"value": best * ratio, "unit": "s", "cores": threads, "kind": "port",
-                                "sample": f"oracle factorize+solve+refine on L27({args.cpu_k}^3)-3I, best of 2 = "
-                                          f"{best:.3f} s, scaled by the algorithmic flop ratio {ratio:.1f}"}
+                                "sample": f"bounded sample: oracle factorize+solve+refine on L27({args.cpu_k}^3)-3I, "
+                                          f"best of 2 = {best:.3f} s, scaled by the algorithmic flop ratio {ratio:.1f} "
+                                          f"(the reference arm, --impl reference, times the full 64^3 workload)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -599,6 +653,9 @@ def main():
     ap.add_argument("--nrhs", type=int, default=16)
     ap.add_argument("--cpu-k", type=int, default=32)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison run")
+    ap.add_argument("--ref-budget", type=float, default=240.0,
+                    help="reference arm: seconds of timed steps (at least one full step runs)")
     ap.add_argument("--graph", type=int, default=1, help="graph launch of the factorization's static pass")
     ap.add_argument("--workload", default="config3", choices=["config3", "dense", "batched", "learned"])
     ap.add_argument("--curvature-shift", type=float, default=0.0,

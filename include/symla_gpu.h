@@ -349,12 +349,6 @@ int symla_mlp_gradient(symla_mlp* mlp, const double* X, const double* T, int B, 
 int symla_mlp_train(symla_mlp* mlp, const double* X, const double* T, int B, int epochs, int minibatch, double lr,
                     double* final_loss);
 
-/* Diagnostic (no reference counterpart): the FP64 tensor-path (DMMA) peak
- * of `device` in TFLOP/s, measured with a register-only loop of independent
- * mma.sync .f64 instructions on every SM (best of three timed launches);
- * the roofline denominator of the FP64 Schur update. */
-int symla_gpu_measure_fp64_tensor_peak(int device, double* tflops);
-
 /* Relative residual ||B - A X||_inf / (||A||_inf ||X||_inf + ||B||_inf) of
  * a device-resident candidate solution X against device-resident B
  * (column-major, n x nrhs, leading dimensions ldx, ldb >= n), for the matrix

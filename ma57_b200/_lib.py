@@ -114,7 +114,6 @@ _SIGS = {
     "symla_mlp_predict": (_i, [_p, _pd, _i, _pd]),
     "symla_mlp_gradient": (_i, [_p, _pd, _pd, _i, _pd, _pd]),
     "symla_mlp_train": (_i, [_p, _pd, _pd, _i, _i, _i, _d, _pd]),
-    "symla_gpu_measure_fp64_tensor_peak": (_i, [_i, _pd]),
 }
 
 MLP_INPUTS = 8

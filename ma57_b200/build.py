@@ -23,7 +23,10 @@ NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 HOST_SRCS = ["host/symbolic.cpp", "host/amd.cpp", "host/metis_order.cpp"]
-CUDA_SRCS = ["gpu/capi.cu", "gpu/factor_kernels.cu", "gpu/solve_kernels.cu", "gpu/panel_cluster.cu", "gpu/schur_tc.cu", "gpu/noalloc.cu", "gpu/mlp.cu", "gpu/peak.cu"]
+CUDA_SRCS = ["gpu/capi.cu", "gpu/factor_kernels.cu", "gpu/solve_kernels.cu", "gpu/panel_cluster.cu", "gpu/schur_tc.cu", "gpu/noalloc.cu", "gpu/mlp.cu"]
+# benchmark tooling, its own library (bench.py loads it; not part of the C ABI)
+BENCH_SRC = "bench/fp64_peak.cu"
+BENCH_LIB = LIBDIR / "libsymla_bench.so"
 
 
 def _run(cmd: list[str]) -> None:
@@ -73,6 +76,12 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         # --no-undefined: a missing symbol fails the build, not the first dlopen
         _run([NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), str(metis), "-lcudart_static",
               "-Xlinker", "--no-undefined"])
+    bsrc = CSRC / BENCH_SRC
+    bobj = BUILD / "fp64_peak.o"
+    if force or _stale(bobj, [bsrc]):
+        _run([NVCC, *ARCH, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-c", str(bsrc), "-o", str(bobj)])
+    if force or _stale(BENCH_LIB, [bobj]):
+        _run([NVCC, *ARCH, "-shared", "-o", str(BENCH_LIB), str(bobj), "-lcudart_static", "-Xlinker", "--no-undefined"])
     return LIB
 
 

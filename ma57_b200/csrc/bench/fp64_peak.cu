@@ -1,17 +1,14 @@
-// FP64 tensor-path peak of this GPU, measured: a register-only loop of
-// independent mma.sync m16n8k8 .f64 (DMMA) instructions on every SM, timed
-// with CUDA events. The measured copy bandwidth and bf16 GEMM peak that the
-// benchmark's roofline uses for HBM- and tensor-bound kernels have no FP64
-// counterpart, and the FP64 Schur update (update_mma_kernel) runs on this
-// pipe, so its roofline denominator is taken with the same kind of
-// microbenchmark. No reference counterpart (a diagnostic).
+// Benchmark tooling, not part of the library: the FP64 tensor-path peak of
+// this GPU, measured with a register-only loop of independent mma.sync
+// m16n8k8 .f64 (DMMA) instructions on every SM, timed with CUDA events. The
+// measured copy bandwidth and bf16 GEMM peak that the benchmark's roofline
+// uses for HBM- and tensor-bound kernels have no FP64 counterpart, and the
+// FP64 Schur update (update_mma_kernel) runs on this pipe, so its roofline
+// denominator is taken with the same kind of microbenchmark. Built into its
+// own library (libsymla_bench.so), which only bench.py loads.
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <string>
-
-#include "../../../include/symla_gpu.h"
-#include "context.hpp"
 
 namespace {
 
@@ -41,21 +38,18 @@ __global__ void __launch_bounds__(32 * kPeakWarps) dmma_peak_kernel(double* out)
 
 }  // namespace
 
-extern "C" int symla_gpu_measure_fp64_tensor_peak(int device, double* tflops) {
-  if (!tflops) return symla_gpu::record_error(SYMLA_ERR_BAD_SIZE, "symla_gpu_measure_fp64_tensor_peak: null output");
-  auto fail = [](cudaError_t e) {
-    return symla_gpu::record_error(SYMLA_ERR_CUDA, std::string("symla_gpu_measure_fp64_tensor_peak: ") +
-                                                       cudaGetErrorString(e));
-  };
+// Returns 0 and the peak in TFLOP/s, or the failing cudaError_t.
+extern "C" int symla_bench_fp64_tensor_peak(int device, double* tflops) {
+  if (!tflops) return static_cast<int>(cudaErrorInvalidValue);
   cudaError_t e = cudaSetDevice(device);
-  if (e != cudaSuccess) return fail(e);
+  if (e != cudaSuccess) return static_cast<int>(e);
   int sms = 0;
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  if (e != cudaSuccess) return fail(e);
+  if (e != cudaSuccess) return static_cast<int>(e);
   const int grid = 2 * sms;
   double* d = nullptr;
   e = cudaMalloc(&d, static_cast<size_t>(grid) * 32 * kPeakWarps * sizeof(double));
-  if (e != cudaSuccess) return fail(e);
+  if (e != cudaSuccess) return static_cast<int>(e);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   float ms = 0.0f;
   double best = 0.0;
@@ -76,7 +70,7 @@ extern "C" int symla_gpu_measure_fp64_tensor_peak(int device, double* tflops) {
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
   cudaFree(d);
-  if (e != cudaSuccess) return fail(e);
+  if (e != cudaSuccess) return static_cast<int>(e);
   *tflops = best;
-  return SYMLA_OK;
+  return 0;
 }

@@ -47,6 +47,10 @@ def load():
             "oracle_front_get": (_i, [_p, _i, _pi, _pd, _pd, _pd, _pi, _pi]),
             "oracle_dense_factor": (_i, [_i, _pd, _i, _i, _i, _d, _d, _i, _d, _d, _d, _pi, _i, _pi, _pd, _pd, _pi,
                                          _pi, _pi, _pd, C.c_char_p, _i]),
+            "oracle_analyze": (_p, [_i, _pi, _pi, _i, _i, _d, C.c_char_p, _i]),
+            "oracle_analysis_sizes": (None, [_p, _pi, _pi, C.POINTER(C.c_longlong)]),
+            "oracle_analysis_get": (None, [_p, _pi, _pi, _pi, _pi, _pi, _pi]),
+            "oracle_analysis_destroy": (None, [_p]),
         }
         for k, (r, a) in sigs.items():
             f = getattr(lib, k)
@@ -66,6 +70,55 @@ def _pd_(a):
 
 class OracleError(Exception):
     pass
+
+
+class _Supernode:
+    def __init__(self, first, ncols, rows):
+        self.firstCol, self.ncols, self.rowPattern = first, ncols, rows
+
+
+class _Etree:
+    def __init__(self, parent):
+        self.parent = parent
+        self.n = len(parent)
+
+
+class OracleAnalysis:
+    """The host symbolic analysis as compiled into the oracle library (same
+    sources as the GPU path's host side): perm, etree.parent and the
+    supernodes, in the shape OracleSymLDLT takes."""
+
+    def __init__(self, perm, parent, supernodes):
+        self.perm = perm
+        self.etree = _Etree(parent)
+        self.supernodes = supernodes
+
+
+def analyze(A, ordering=0, max_relax_size=64, max_relax_fill_fraction=0.25) -> OracleAnalysis:
+    """SymbolicFactor::analyze (symbolic.hpp:195-399) without the product
+    library: ordering 0 AMD, 1 METIS, 2 natural, 3 METIS in the reference's
+    convention."""
+    from ma57_b200.solver import as_csc
+    n, cp, ri, _ = as_csc(A)
+    lib = load()
+    err = C.create_string_buffer(512)
+    h = lib.oracle_analyze(n, _pi_(cp), _pi_(ri), int(ordering), max_relax_size, max_relax_fill_fraction, err, 512)
+    if not h:
+        raise RuntimeError(err.value.decode())
+    try:
+        nn, ns, pl = C.c_int(), C.c_int(), C.c_longlong()
+        lib.oracle_analysis_sizes(h, C.byref(nn), C.byref(ns), C.byref(pl))
+        perm = np.zeros(max(1, nn.value), np.int32)
+        par = np.zeros(max(1, nn.value), np.int32)
+        first = np.zeros(max(1, ns.value), np.int32)
+        ncols = np.zeros(max(1, ns.value), np.int32)
+        ptr = np.zeros(ns.value + 1, np.int32)
+        rows = np.zeros(max(1, pl.value), np.int32)
+        lib.oracle_analysis_get(h, _pi_(perm), _pi_(par), _pi_(first), _pi_(ncols), _pi_(ptr), _pi_(rows))
+    finally:
+        lib.oracle_analysis_destroy(h)
+    sns = [_Supernode(int(first[i]), int(ncols[i]), rows[ptr[i]:ptr[i + 1]].copy()) for i in range(ns.value)]
+    return OracleAnalysis(perm[:nn.value].copy(), par[:nn.value].copy(), sns)
 
 
 def _raise(code, msg):

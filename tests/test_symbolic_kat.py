@@ -231,3 +231,20 @@ def test_metis_pivot_order_fills_less_than_its_inverse():
     fill_nd = R.total_fill(A, computeOrdering(A, OrderingType.Metis))
     fill_ref = R.total_fill(A, computeOrdering(A, OrderingType.MetisIperm))
     assert fill_nd < fill_ref
+
+
+@pytest.mark.parametrize("ordering", [OrderingType.AMD, OrderingType.Metis])
+def test_oracle_library_analysis_is_the_same(ordering):
+    """The oracle library carries its own build of the host analysis (so the
+    CPU baseline runs without the product library); it must give the same
+    permutation, elimination tree and supernodes."""
+    from oracle.pyoracle import analyze
+    A = M.config3(10, nrhs=1)[0]
+    a = analyze(A, int(ordering))
+    sf = globals()["analyze"](A, ordering)
+    np.testing.assert_array_equal(a.perm, sf.perm)
+    np.testing.assert_array_equal(a.etree.parent, sf.etree.parent)
+    assert len(a.supernodes) == len(sf.supernodes)
+    for x, y in zip(a.supernodes, sf.supernodes):
+        assert (x.firstCol, x.ncols) == (y.firstCol, y.ncols)
+        np.testing.assert_array_equal(x.rowPattern, y.rowPattern)
