@@ -56,10 +56,10 @@ struct FrontState {
 enum : int { kFlagDone = 1, kFlagDelayed = 2, kFlagSingularRoot = 4, kFlagFlush = 8 };
 
 // Columns per outer block of the large-front factorization.
-constexpr int kOuterBlock = 128;
+constexpr int kOuterBlock = 256;
 // Pivots per far update the tensor-core workspace holds (>= kOuterBlock + 1,
 // a multiple of 32).
-constexpr int kTcKpad = 160;
+constexpr int kTcKpad = 288;
 // Growth guard of the mixed-precision far update. A block of K pivots goes
 // to the tensor cores only when max|L| * max|L D| over the rows it updates
 // is at most this multiple of max|a_ij| of the original matrix: TF32x3

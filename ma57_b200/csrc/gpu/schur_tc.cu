@@ -44,7 +44,7 @@ constexpr int kThreads = 128;  // 4 warps: one per 32-lane TMEM quarter
 constexpr int kStageBytes = 4 * kTM * kBoxK * 4;  // A_hi, A_lo, B_hi, B_lo
 constexpr int kStages = 2;
 constexpr int kMaxFronts = 512;
-constexpr int kSplitRows = 16;  // rows per pass of the split pre-pass
+constexpr int kSplitRows = 8;   // rows per pass of the split pre-pass (4 x 8 x (kTcKpad + 1) floats of static shared memory)
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
