@@ -369,7 +369,12 @@ int symla_mlp_train(symla_mlp* mlp, const double* X, const double* T, int B, int
  * clears the accumulators it needs at its start, so calls whose work
  * overlaps on the GPU (from several threads, contexts or streams) race and
  * must be serialised by the caller. Runs on the context's stream and
- * returns after it synchronises. */
+ * returns after it synchronises. That stream does not synchronise with the
+ * legacy default stream or any other stream: X and B must be complete
+ * before the call (synchronise their producer, or record an event after it
+ * and make symla_gpu_stream(ctx) wait on it). The array's device address is
+ * looked up on a device's first call and kept; a cudaDeviceReset of that
+ * device afterwards is not supported. */
 #define SYMLA_NOALLOC_RESIDUAL_MAX_ENTRIES (1 << 20)
 int symla_gpu_relative_residual_noalloc(symla_gpu_ctx* ctx, const double* X, int ldx, const double* B, int ldb,
                                         int nrhs, double* rel_residual);

@@ -29,11 +29,14 @@ def _refine(lib, h, B, iterations):
     return X, info
 
 
-def _noalloc(lib, h, dXt, dBt):
-    """dXt, dBt: (nrhs, n) contiguous device tensors, i.e. column-major n x nrhs."""
-    nrhs, n = dXt.shape
+def _noalloc(lib, h, dXt, dBt, n=None):
+    """dXt, dBt: (nrhs, ld) contiguous device tensors, i.e. column-major
+    ld x nrhs with the first n rows used (n defaults to ld)."""
+    nrhs, ldx = dXt.shape
+    ldb = dBt.shape[1]
+    n = ldx if n is None else n
     out = C.c_double(-1.0)
-    rc = lib.symla_gpu_relative_residual_noalloc(h, C.c_void_p(dXt.data_ptr()), n, C.c_void_p(dBt.data_ptr()), n,
+    rc = lib.symla_gpu_relative_residual_noalloc(h, C.c_void_p(dXt.data_ptr()), ldx, C.c_void_p(dBt.data_ptr()), ldb,
                                                   nrhs, C.byref(out))
     assert rc == L.SYMLA_OK, L.last_error()
     return out.value
@@ -81,3 +84,29 @@ def test_noalloc_residual_rejects_sizes_beyond_its_scratch():
                                                   nrhs, C.byref(out))
     assert rc == L.SYMLA_ERR_BAD_SIZE
     assert "exceeds the fixed scratch" in L.last_error()
+
+
+def test_noalloc_residual_with_leading_dimensions_beyond_n():
+    """X and B with leading dimensions larger than n: the rows past n of
+    each column are padding filled with huge values, which must not enter
+    the residual or the norms."""
+    import torch
+    A, _ = M.config1(10)
+    n = A.shape[0]
+    nrhs = 2
+    B = np.asfortranarray(np.random.default_rng(11).standard_normal((n, nrhs)))
+    s = SymLDLT()
+    s.analyzePattern(A)
+    s.factorize(A)
+    lib = L.load()
+    h = s._ctx.h
+    X, info = _refine(lib, h, B, 0)
+    dev = torch.device("cuda", 0)
+    for ldx, ldb in ((n + 5, n + 3), (n + 1, n)):
+        Xp = np.full((nrhs, ldx), 1e30)
+        Bp = np.full((nrhs, ldb), -1e30)
+        Xp[:, :n] = X.T
+        Bp[:, :n] = B.T
+        value = _noalloc(lib, h, torch.from_numpy(Xp).to(dev), torch.from_numpy(Bp).to(dev), n=n)
+        expected = info.initial_relative_residual
+        assert abs(value - expected) <= 1e-12 * expected, (ldx, ldb, value, expected)
