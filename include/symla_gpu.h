@@ -214,6 +214,26 @@ typedef struct {
 int symla_gpu_solve_refine(symla_gpu_ctx* ctx, const double* values, const double* B, int ldb, int nrhs, double* X,
                            int ldx, int on_device, int max_iterations, double tolerance, symla_refine_info* info);
 
+/* GMRES-IR (no counterpart in the reference; refine.hpp:52-57 records
+ * fixed-precision refinement as its limitation): refinement on the FP64
+ * residual with iterativeRefine's stopping and acceptance rules, each
+ * correction solved by restarted GMRES (`restart` in [1, 64] Krylov vectors
+ * per outer step) preconditioned by the device LDL^T solve. It converges
+ * where fixed-precision refinement stagnates with a factor that is only an
+ * approximate inverse: the mixed-precision factorization, or a static-pivot
+ * factorization with large perturbations. Keeps (restart + 1) x n x nrhs
+ * doubles of Krylov vectors on the device. */
+typedef struct {
+  int outer_iterations;
+  int inner_iterations;         /* GMRES steps over all outer iterations (one solve + one SpMV each) */
+  double initial_relative_residual;
+  double final_relative_residual;
+} symla_gmres_info;
+
+int symla_gpu_solve_gmres_refine(symla_gpu_ctx* ctx, const double* values, const double* B, int ldb, int nrhs,
+                                 double* X, int ldx, int on_device, int max_outer, int restart, double tolerance,
+                                 symla_gmres_info* info);
+
 /* Final-order indices of the columns that could not be pivoted anywhere
  * (NumericFactor::singularCols, sorted). Returns the count; writes at most
  * cap entries. */

@@ -70,6 +70,11 @@ class RefineInfo(C.Structure):
     _fields_ = [("iterations", _i), ("initial_relative_residual", _d), ("final_relative_residual", _d)]
 
 
+class GmresInfo(C.Structure):
+    _fields_ = [("outer_iterations", _i), ("inner_iterations", _i), ("initial_relative_residual", _d),
+                ("final_relative_residual", _d)]
+
+
 _SIGS = {
     "symla_last_error": (C.c_char_p, []),
     "symla_analyze": (_i, [_i, _pi, _pi, _i, _i, _d, C.POINTER(_p)]),
@@ -88,6 +93,7 @@ _SIGS = {
                                              C.POINTER(RegularizeInfo)]),
     "symla_gpu_solve": (_i, [_p, _pd, _i, _i, _pd, _i, _i]),
     "symla_gpu_solve_refine": (_i, [_p, _pd, _pd, _i, _i, _pd, _i, _i, _i, _d, C.POINTER(RefineInfo)]),
+    "symla_gpu_solve_gmres_refine": (_i, [_p, _pd, _pd, _i, _i, _pd, _i, _i, _i, _i, _d, C.POINTER(GmresInfo)]),
     "symla_gpu_singular_cols": (_i, [_p, _pi, _i]),
     "symla_gpu_num_fronts": (_i, [_p]),
     "symla_gpu_front_size": (_i, [_p, _i, _pi, _pi]),

@@ -1486,7 +1486,8 @@ extern "C" void symla_gpu_destroy(symla_gpu_ctx* c) {
                   c->d_front_delta, c->d_perm, c->d_rowptr, c->d_colind, c->d_vidx, c->d_srowptr, c->d_svidx, c->d_W,
                   c->d_Bp, c->d_Z, c->d_Xf, c->d_B, c->d_X, c->d_R, c->d_dX, c->d_Xn, c->d_Rn, c->d_norms,
                   c->d_scratch_int, c->d_flag_base, c->d_flags, c->d_solve_err, c->d_counter,
-                  c->d_tcws, c->d_tc_err, c->d_tc_guard, c->d_hflags, c->d_hscratch};
+                  c->d_tcws, c->d_tc_err, c->d_tc_guard, c->d_hflags, c->d_hscratch,
+                  c->d_gmres, c->d_zero, c->d_gpart, c->d_gcoef};
   for (void* p : ptrs) dfree(p);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
@@ -1763,6 +1764,209 @@ extern "C" int symla_gpu_solve_refine(symla_gpu_ctx* c, const double* values, co
     collect_pending(c);
     check_solve_error(c);
     if (info) *info = ri;
+  });
+}
+
+// GMRES-IR (no counterpart in the reference, which lists fixed-precision
+// refinement as its limitation, refine.hpp:52-57): outer refinement on the
+// FP64 residual with iterativeRefine's stopping and acceptance rules
+// (refine.hpp:109-141); each correction A d = r is solved by restarted GMRES
+// on M^-1 A, M^-1 the device LDL^T solve, all right-hand sides together
+// (classical Gram-Schmidt applied twice; Givens rotations on the host).
+extern "C" int symla_gpu_solve_gmres_refine(symla_gpu_ctx* c, const double* values, const double* B, int ldb,
+                                            int nrhs, double* X, int ldx, int on_device, int max_outer, int restart,
+                                            double tolerance, symla_gmres_info* info) {
+  if (!c) return set_error(SYMLA_ERR_NOT_FACTORIZED, "symla::SymLDLT::solve: factorize() must be called before solve()");
+  return guarded([&] {
+    check_solvable(c);
+    if (nrhs < 0 || ldb < c->n || ldx < c->n)
+      throw SymlaError(SYMLA_ERR_BAD_SIZE, "symla::SymLDLT::solve: B.rows() must match the factorized matrix size");
+    if (restart < 1 || restart > 64)
+      throw SymlaError(SYMLA_ERR_INVALID, "symla_gpu_solve_gmres_refine: restart must be in [1, 64]");
+    CK(cudaSetDevice(c->device));
+    const int n = c->n;
+    symla_gmres_info gi{};
+    if (nrhs == 0 || n == 0) {
+      if (info) *info = gi;
+      return;
+    }
+    cudaStream_t st = c->stream;
+    ensure_vectors(c, nrhs);
+    const long long len = static_cast<long long>(n) * nrhs;
+    const size_t need = static_cast<size_t>(restart + 1) * len;
+    if (need > c->gmres_cap) {
+      dfree(c->d_gmres);
+      c->d_gmres = nullptr;
+      c->d_gmres = dalloc<double>(need);
+      c->gmres_cap = need;
+    }
+    if (c->zero_len < n) {
+      dfree(c->d_zero);
+      c->d_zero = nullptr;
+      c->d_zero = dalloc<double>(n);
+      c->zero_len = n;
+    }
+    CK(cudaMemsetAsync(c->d_zero, 0, n * sizeof(double), st));
+    const int G = multi_dot_blocks(n);
+    const size_t pcap = static_cast<size_t>(restart + 1) * nrhs * G;
+    if (pcap > c->gpart_cap) {
+      dfree(c->d_gpart);
+      c->d_gpart = nullptr;
+      c->d_gpart = dalloc<double>(pcap);
+      c->gpart_cap = pcap;
+    }
+    const size_t ccap = static_cast<size_t>(restart + 1) * nrhs;
+    if (ccap > c->gcoef_cap) {
+      dfree(c->d_gcoef);
+      c->d_gcoef = nullptr;
+      c->d_gcoef = dalloc<double>(ccap);
+      c->gcoef_cap = ccap;
+    }
+    double* V = c->d_gmres;
+    const long long vs = len;
+    if (on_device)
+      launch_copy2d(n, nrhs, B, ldb, c->d_B, n, st);
+    else
+      CK(cudaMemcpy2DAsync(c->d_B, n * sizeof(double), B, static_cast<size_t>(ldb) * sizeof(double),
+                           n * sizeof(double), nrhs, cudaMemcpyHostToDevice, st));
+    if (values) upload_values(c, values, on_device);
+    CK(cudaMemsetAsync(c->d_norms, 0, 8 * sizeof(double), st));
+    launch_rowsum_max(n, c->d_srowptr, c->d_svidx, c->d_values, c->d_norms + 0, st);
+    launch_absmax(c->d_B, len, c->d_norms + 1, st);
+    device_solve(c, c->d_B, n, nrhs, c->d_X, n);
+    auto residual_of = [&](const double* Xd, double* Rd) {
+      CK(cudaMemsetAsync(c->d_norms + 2, 0, 2 * sizeof(double), st));
+      launch_residual(n, nrhs, c->d_rowptr, c->d_colind, c->d_vidx, c->d_values, Xd, n, c->d_B, n, Rd, st);
+      launch_absmax(Rd, len, c->d_norms + 2, st);
+      launch_absmax(Xd, len, c->d_norms + 3, st);
+      double h[4];
+      CK(cudaMemcpyAsync(h, c->d_norms, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      const double denom = h[0] * h[3] + h[1];
+      return denom > 0.0 ? h[2] / denom : h[2];
+    };
+    std::vector<double> part(pcap), coef(ccap);
+    // out[i nrhs + cc] = V_i[:, cc] . W[:, cc], partials summed in a fixed order
+    auto dots = [&](int nvec, const double* Vb, const double* W, std::vector<double>& out) {
+      launch_multi_dot(n, nrhs, nvec, Vb, vs, W, c->d_gpart, st);
+      CK(cudaMemcpyAsync(part.data(), c->d_gpart, static_cast<size_t>(nvec) * nrhs * G * sizeof(double),
+                         cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      out.assign(static_cast<size_t>(nvec) * nrhs, 0.0);
+      for (size_t t = 0; t < out.size(); ++t) {
+        double sum = 0.0;
+        for (int b = 0; b < G; ++b) sum += part[t * G + b];
+        out[t] = sum;
+      }
+    };
+    auto sub = [&](int nvec, const double* Vb, const std::vector<double>& cf, double* W) {
+      CK(cudaMemcpyAsync(c->d_gcoef, cf.data(), static_cast<size_t>(nvec) * nrhs * sizeof(double),
+                         cudaMemcpyHostToDevice, st));
+      launch_multi_axpy(n, nrhs, nvec, Vb, vs, c->d_gcoef, W, st);
+    };
+    auto scale = [&](const std::vector<double>& alpha, double* W) {
+      CK(cudaMemcpyAsync(c->d_gcoef, alpha.data(), nrhs * sizeof(double), cudaMemcpyHostToDevice, st));
+      launch_col_scale(n, nrhs, c->d_gcoef, W, W, st);
+    };
+    double res = residual_of(c->d_X, c->d_R);
+    gi.initial_relative_residual = gi.final_relative_residual = res;
+    const int ldh = restart + 1;
+    std::vector<double> H(static_cast<size_t>(nrhs) * ldh * restart), g(static_cast<size_t>(nrhs) * ldh),
+        cs(static_cast<size_t>(nrhs) * restart), sn(static_cast<size_t>(nrhs) * restart), beta(nrhs), nn, d1, hs,
+        alpha(nrhs);
+    for (int outer = 0; outer < max_outer && res > tolerance; ++outer) {
+      // z = M^-1 r into v_0, normalised per column
+      device_solve(c, c->d_R, n, nrhs, V, n);
+      dots(1, V, V, nn);
+      for (int cc = 0; cc < nrhs; ++cc) {
+        beta[cc] = std::sqrt(std::max(nn[cc], 0.0));
+        alpha[cc] = beta[cc] > 0.0 ? 1.0 / beta[cc] : 0.0;
+        std::fill(g.begin() + static_cast<size_t>(cc) * ldh, g.begin() + static_cast<size_t>(cc + 1) * ldh, 0.0);
+        g[static_cast<size_t>(cc) * ldh] = beta[cc];
+      }
+      scale(alpha, V);
+      std::vector<char> active(nrhs);
+      for (int cc = 0; cc < nrhs; ++cc) active[cc] = beta[cc] > 0.0;
+      int kdone = 0;
+      for (int k = 0; k < restart; ++k) {
+        double* vk1 = V + static_cast<long long>(k + 1) * vs;
+        // u = M^-1 (0 - A v_k) = -M^-1 A v_k
+        launch_residual(n, nrhs, c->d_rowptr, c->d_colind, c->d_vidx, c->d_values, V + static_cast<long long>(k) * vs,
+                        n, c->d_zero, 0, c->d_Rn, st);
+        device_solve(c, c->d_Rn, n, nrhs, vk1, n);
+        hs.assign(static_cast<size_t>(k + 1) * nrhs, 0.0);
+        for (int pass = 0; pass < 2; ++pass) {  // classical Gram-Schmidt, twice
+          dots(k + 1, V, vk1, d1);
+          sub(k + 1, V, d1, vk1);
+          for (size_t t = 0; t < hs.size(); ++t) hs[t] += d1[t];
+        }
+        dots(1, vk1, vk1, nn);
+        bool all_done = true;
+        for (int cc = 0; cc < nrhs; ++cc) {
+          double* Hc = H.data() + static_cast<size_t>(cc) * ldh * restart;
+          double* gc = g.data() + static_cast<size_t>(cc) * ldh;
+          double* csc = cs.data() + static_cast<size_t>(cc) * restart;
+          double* snc = sn.data() + static_cast<size_t>(cc) * restart;
+          const double hk1 = std::sqrt(std::max(nn[cc], 0.0));
+          alpha[cc] = hk1 > 0.0 ? -1.0 / hk1 : 0.0;  // v_{k+1} = w / h = -u / h
+          if (!active[cc]) continue;
+          for (int i = 0; i <= k; ++i) Hc[i + k * ldh] = -hs[static_cast<size_t>(i) * nrhs + cc];
+          Hc[k + 1 + k * ldh] = hk1;
+          for (int i = 0; i < k; ++i) {
+            const double t = csc[i] * Hc[i + k * ldh] + snc[i] * Hc[i + 1 + k * ldh];
+            Hc[i + 1 + k * ldh] = -snc[i] * Hc[i + k * ldh] + csc[i] * Hc[i + 1 + k * ldh];
+            Hc[i + k * ldh] = t;
+          }
+          const double a = Hc[k + k * ldh], b = Hc[k + 1 + k * ldh];
+          const double r = std::hypot(a, b);
+          csc[k] = r > 0.0 ? a / r : 1.0;
+          snc[k] = r > 0.0 ? b / r : 0.0;
+          Hc[k + k * ldh] = r;
+          Hc[k + 1 + k * ldh] = 0.0;
+          gc[k + 1] = -snc[k] * gc[k];
+          gc[k] = csc[k] * gc[k];
+          // this column's Krylov space is exhausted or its residual estimate
+          // is below the inner tolerance
+          if (hk1 == 0.0 || std::fabs(gc[k + 1]) <= 1e-13 * beta[cc]) active[cc] = 0;
+          all_done = all_done && !active[cc];
+        }
+        scale(alpha, vk1);
+        kdone = k + 1;
+        ++gi.inner_iterations;
+        if (all_done) break;
+      }
+      // y = R^-1 g per column (upper triangular, kdone x kdone); x += V y
+      for (int cc = 0; cc < nrhs; ++cc) {
+        const double* Hc = H.data() + static_cast<size_t>(cc) * ldh * restart;
+        const double* gc = g.data() + static_cast<size_t>(cc) * ldh;
+        std::vector<double> y(kdone, 0.0);
+        if (beta[cc] > 0.0)
+          for (int i = kdone - 1; i >= 0; --i) {
+            double t = gc[i];
+            for (int j = i + 1; j < kdone; ++j) t -= Hc[i + j * ldh] * y[j];
+            y[i] = Hc[i + i * ldh] != 0.0 ? t / Hc[i + i * ldh] : 0.0;
+          }
+        for (int i = 0; i < kdone; ++i) coef[static_cast<size_t>(i) * nrhs + cc] = -y[i];
+      }
+      CK(cudaMemcpyAsync(c->d_Xn, c->d_X, len * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      sub(kdone, V, coef, c->d_Xn);
+      const double resNew = residual_of(c->d_Xn, c->d_Rn);
+      gi.outer_iterations = outer + 1;
+      if (!(resNew < res)) break;  // keep the better iterate (refine.hpp:121-141)
+      std::swap(c->d_X, c->d_Xn);
+      std::swap(c->d_R, c->d_Rn);
+      res = resNew;
+      gi.final_relative_residual = res;
+    }
+    if (on_device)
+      launch_copy2d(n, nrhs, c->d_X, n, X, ldx, st);
+    else
+      CK(cudaMemcpy2DAsync(X, static_cast<size_t>(ldx) * sizeof(double), c->d_X, n * sizeof(double),
+                           n * sizeof(double), nrhs, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    collect_pending(c);
+    check_solve_error(c);
+    if (info) *info = gi;
   });
 }
 

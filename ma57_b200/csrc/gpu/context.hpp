@@ -172,6 +172,17 @@ struct symla_gpu_ctx {
   // with work possibly outstanding, so no further work is run on the context
   bool unusable = false;
 
+  // GMRES-IR workspace: Krylov vectors (restart + 1) x n x nrhs, a zero
+  // column, fixed-order partial sums and per-column coefficients
+  double* d_gmres = nullptr;
+  size_t gmres_cap = 0;
+  double* d_zero = nullptr;
+  int zero_len = 0;
+  double* d_gpart = nullptr;
+  size_t gpart_cap = 0;
+  double* d_gcoef = nullptr;
+  size_t gcoef_cap = 0;
+
   // state
   bool factorized = false;
   bool singular = false;

@@ -107,5 +107,15 @@ void launch_rowsum_max(int n, const int* srowptr, const int* svidx, const double
 // X += dX (len entries)
 void launch_axpy(long long len, const double* dx, double* x, cudaStream_t stream);
 void launch_copy2d(int rows, int cols, const double* src, int lds, double* dst, int ldd, cudaStream_t stream);
+// GMRES-IR vector work over all right-hand sides at once; vector i, column c
+// at V + i * vs + c * n. multi_dot writes nvec x nrhs x multi_dot_blocks(n)
+// fixed-order partial sums of V_i[:, c] . W[:, c]; multi_axpy: W[:, c] -=
+// sum_i coef[i nrhs + c] V_i[:, c]; col_scale: Y[:, c] = alpha[c] X[:, c].
+int multi_dot_blocks(int n);
+void launch_multi_dot(int n, int nrhs, int nvec, const double* V, long long vs, const double* W, double* partial,
+                      cudaStream_t stream);
+void launch_multi_axpy(int n, int nrhs, int nvec, const double* V, long long vs, const double* coef, double* W,
+                       cudaStream_t stream);
+void launch_col_scale(int n, int nrhs, const double* alpha, const double* X, double* Y, cudaStream_t stream);
 
 }  // namespace symla_gpu

@@ -28,6 +28,8 @@
 // (sum of the children's minus L_bottom * y), so the parent adds them.
 #include <cmath>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "factor_kernels.h"
 #include "reduce.cuh"
@@ -556,6 +558,52 @@ __global__ void copy2d_kernel(int rows, int cols, const double* __restrict__ src
   dst[i + static_cast<long long>(c) * ldd] = src[i + static_cast<long long>(c) * lds];
 }
 
+// ---------------------------------------------------------------------------
+// Column-wise vector kernels of GMRES-IR. The Krylov vectors of all
+// right-hand sides advance together: vector i, right-hand side c is
+// V + i * vs + c * n (n rows, compact).
+
+// partial[(i * nrhs + c) * G + b] = sum over block b's rows of
+// V_i[:, c] . W[:, c], with G = gridDim.x; every block sums its rows in a
+// fixed order (the host adds the partials in a fixed order too).
+__global__ void multi_dot_kernel(int n, int nrhs, const double* __restrict__ V, long long vs,
+                                 const double* __restrict__ W, double* __restrict__ partial) {
+  __shared__ double red[8];
+  const int c = blockIdx.y, i = blockIdx.z;
+  const double* v = V + i * vs + static_cast<long long>(c) * n;
+  const double* w = W + static_cast<long long>(c) * n;
+  double s = 0.0;
+  for (long long r = blockIdx.x * 256LL + threadIdx.x; r < n; r += static_cast<long long>(gridDim.x) * 256)
+    s = fma(v[r], w[r], s);
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < 8; ++k) t += red[k];
+    partial[(static_cast<long long>(i) * nrhs + c) * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// W[:, c] -= sum_i coef[i * nrhs + c] * V_i[:, c]
+__global__ void multi_axpy_kernel(int n, int nrhs, int nvec, const double* __restrict__ V, long long vs,
+                                  const double* __restrict__ coef, double* __restrict__ W) {
+  const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (t >= static_cast<long long>(n) * nrhs) return;
+  const int c = static_cast<int>(t / n);
+  double acc = W[t];
+  for (int i = 0; i < nvec; ++i) acc -= coef[i * nrhs + c] * V[i * vs + t];
+  W[t] = acc;
+}
+
+// Y[:, c] = alpha[c] * X[:, c]
+__global__ void col_scale_kernel(int n, int nrhs, const double* __restrict__ alpha, const double* __restrict__ X,
+                                 double* __restrict__ Y) {
+  const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (t >= static_cast<long long>(n) * nrhs) return;
+  Y[t] = alpha[t / n] * X[t];
+}
+
 namespace {
 inline unsigned grid_for(long long work, int threads) {
   long long g = (work + threads - 1) / threads;
@@ -635,6 +683,23 @@ void launch_axpy(long long len, const double* dx, double* x, cudaStream_t stream
   if (len <= 0) return;
   axpy_kernel<<<grid_for(len, 256), 256, 0, stream>>>(len, dx, x);
 }
+int multi_dot_blocks(int n) { return static_cast<int>(std::min<long long>((n + 255) / 256, 296)); }
+void launch_multi_dot(int n, int nrhs, int nvec, const double* V, long long vs, const double* W, double* partial,
+                      cudaStream_t stream) {
+  if (n <= 0 || nrhs <= 0 || nvec <= 0) return;
+  multi_dot_kernel<<<dim3(multi_dot_blocks(n), nrhs, nvec), 256, 0, stream>>>(n, nrhs, V, vs, W, partial);
+}
+void launch_multi_axpy(int n, int nrhs, int nvec, const double* V, long long vs, const double* coef, double* W,
+                       cudaStream_t stream) {
+  if (n <= 0 || nrhs <= 0 || nvec <= 0) return;
+  multi_axpy_kernel<<<grid_for(static_cast<long long>(n) * nrhs, 256), 256, 0, stream>>>(n, nrhs, nvec, V, vs, coef,
+                                                                                        W);
+}
+void launch_col_scale(int n, int nrhs, const double* alpha, const double* X, double* Y, cudaStream_t stream) {
+  if (n <= 0 || nrhs <= 0) return;
+  col_scale_kernel<<<grid_for(static_cast<long long>(n) * nrhs, 256), 256, 0, stream>>>(n, nrhs, alpha, X, Y);
+}
+
 void launch_copy2d(int rows, int cols, const double* src, int lds, double* dst, int ldd, cudaStream_t stream) {
   if (rows <= 0 || cols <= 0) return;
   copy2d_kernel<<<grid_for(static_cast<long long>(rows) * cols, 256), 256, 0, stream>>>(rows, cols, src, lds, dst, ldd);

@@ -83,6 +83,25 @@ class RefinementResult:
 
 
 @dataclass
+class GmresRefinementOptions:
+    """GMRES-IR (a B200 extension; the reference refines in fixed precision
+    only, refine.hpp:52-57): outer iterations on the FP64 residual, each
+    correction by GMRES with `restart` Krylov vectors preconditioned by the
+    factorization."""
+    max_outer: int = 10
+    restart: int = 8
+    tolerance: float = 1e-14
+
+
+@dataclass
+class GmresResult:
+    outer_iterations: int = 0
+    inner_iterations: int = 0
+    initial_relative_residual: float = 0.0
+    final_relative_residual: float = 0.0
+
+
+@dataclass
 class RefinedSolve:
     x: np.ndarray
     diagnostics: RefinementResult
@@ -501,6 +520,33 @@ class SymLDLT:
                                                    0, int(options.max_iterations), float(options.tolerance),
                                                    C.byref(ri_)))
         diag = RefinementResult(ri_.iterations, ri_.initial_relative_residual, ri_.final_relative_residual)
+        return RefinedSolve(X[:, 0] if vec else X, diag)
+
+    def solveWithGmresRefinement(self, A, B, options: GmresRefinementOptions = None) -> RefinedSolve:
+        """GMRES-IR: like solveWithRefinement (same errors, same backward
+        error measure and acceptance rule) with every correction solved by
+        preconditioned GMRES; diagnostics is a GmresResult."""
+        options = options or GmresRefinementOptions()
+        if not self.factorized_:
+            raise LogicError("symla::SymLDLT::solve: factorize() must be called before solve()")
+        if self.isSingular():
+            raise LogicError("symla::SymLDLT::solve: factorization is numerically singular; refusing to solve")
+        n, cp, ri, vals = as_csc(A)
+        if not self._ctx.same_pattern(cp, ri):
+            raise InvalidArgument("symla::SymLDLT::solveWithRefinement: A's pattern differs from the factorized one")
+        Bf, vec = self._rhs(B)
+        if Bf.shape[0] != n:
+            raise InvalidArgument("symla::SymLDLT::solve: B.rows() must match the factorized matrix size")
+        nrhs = Bf.shape[1]
+        X = np.zeros((n, nrhs), dtype=np.float64, order="F")
+        gi = L.GmresInfo()
+        if nrhs > 0 and n > 0:
+            _check(L.load().symla_gpu_solve_gmres_refine(self._ctx.h, L.ptr_d(vals), L.ptr_d(Bf), n, nrhs,
+                                                         L.ptr_d(X), n, 0, int(options.max_outer),
+                                                         int(options.restart), float(options.tolerance),
+                                                         C.byref(gi)))
+        diag = GmresResult(gi.outer_iterations, gi.inner_iterations, gi.initial_relative_residual,
+                           gi.final_relative_residual)
         return RefinedSolve(X[:, 0] if vec else X, diag)
 
     # --- results (solver.hpp:242-262) ---
