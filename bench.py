@@ -268,7 +268,30 @@ def run_batched(args):
         Af = M.sym_full(A)
         R = B - Af @ Xi
         worst = max(worst, np.abs(R).max() / (abs(A).sum(axis=1).max() * np.abs(Xi).max() + np.abs(B).max()))
-    # per-system latency, one at a time (factorize + solve, device timing)
+
+    # per-system latency when the systems are served in batches of
+    # --batch-size (arrival order): a system's result is ready when its
+    # batch's factorize + solve ends, so its latency is its batch's time
+    # (device events, after a warm-up of the batch's own graph)
+    batch_lat, per_system = [], []
+    for b0 in range(0, count, args.batch_size):
+        sub = mats[b0:b0 + args.batch_size]
+        bb = BatchedSolver(sub, graph=bool(args.graph))
+        Bb = bb.stack(Bs[b0:b0 + args.batch_size])
+        for _ in range(2):
+            bb.factorize()
+            bb.solver.solve(Bb)
+        ts = []
+        for _ in range(3):
+            bb.factorize()
+            bb.solver.solve(Bb)
+            ph = bb.solver.phase_ms()
+            ts.append(ph[6] + ph[7])
+        t = min(ts)
+        batch_lat.append(t)
+        per_system += [t] * len(sub)
+        del bb
+    # single systems, one at a time (factorize + solve, device timing)
     lat = []
     for idx in np.linspace(0, count - 1, 64).astype(int):
         A, B = mats[idx], Bs[idx]
@@ -280,6 +303,40 @@ def run_batched(args):
         si.solve(B)
         ph = si.phase_ms()
         lat.append(ph[6] + ph[7])
+
+    # CPU baseline on a bounded sample of the systems: the oracle (the
+    # reference's algorithm) in a sequential loop over systems, as the
+    # reference, which has no batch API, would run them; and, labelled as not
+    # the reference, the same per-system work in a thread pool over systems
+    cpu = None
+    if not args.no_cpu:
+        from concurrent.futures import ThreadPoolExecutor
+        from oracle.pyoracle import OracleSymLDLT, analyze
+        sample = list(range(min(count, args.cpu_systems)))
+        solvers = []
+        for i in sample:
+            o = OracleSymLDLT(analyze(mats[i], 0))
+            o.set(parallel=0)
+            solvers.append(o)
+
+        def one(i):
+            solvers[i].factorize(mats[sample[i]])
+            solvers[i].solve(Bs[sample[i]])
+
+        t0 = time.perf_counter()
+        for i in range(len(sample)):
+            one(i)
+        t_seq = time.perf_counter() - t0
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as ex:
+            list(ex.map(one, range(len(sample))))
+        t_par = time.perf_counter() - t0
+        cpu = {"value": len(sample) / t_seq, "unit": "systems/s", "cores": 1, "kind": "port",
+               "sample": f"oracle factorize + 8-RHS solve of the first {len(sample)} systems, sequential loop "
+                         f"over systems (analysis excluded)",
+               "harness_thread_pool": {"value": len(sample) / t_par, "threads": threads,
+                                       "note": "project harness, not the reference: systems in a thread pool"}}
     line = {"metric": "batched factorize+solve throughput", "value": count / (ms * 1e-3), "unit": "systems/s",
             "higher_is_better": True, "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
             "n_gpus": 1, "dtype": "f64", "data": "synthetic",
@@ -288,8 +345,14 @@ def run_batched(args):
                        "autotune": {"schedule": {k: {str(b): v for b, v in d.items()} for k, d in schedule.items()},
                                     "default_factor_ms": t_default, "tuned_factor_ms": t_tuned},
                        "graph_stats": s.graphStats(), "max_backward_error_first_256": worst},
-            "per_system_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                              "sample": "64 systems spread over the sizes, factorize + solve each alone"},
+            "per_system_ms": {"p50": float(np.percentile(per_system, 50)),
+                              "p99": float(np.percentile(per_system, 99)),
+                              "how": f"systems served in batches of {args.batch_size} in arrival order; a "
+                                     f"system's latency is its batch's factorize + solve device time",
+                              "batches": len(batch_lat)},
+            "single_system_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                                 "sample": "64 systems spread over the sizes, factorize + solve each alone"},
+            "cpu_baseline": cpu,
             "clocks": clocks}
     print(json.dumps(line), flush=True)
 
@@ -302,13 +365,29 @@ def run_learned(args):
     then run twice from the same state of the sequence, with plain
     escalation and with the network's first-attempt deltas (the network
     fine-tuned, after every matrix whose first attempt failed, on the deltas
-    accepted for the last 20, its training time included). Reported: mean retries and total time
-    (factorize + refinement towards 1e-10)."""
+    accepted for the last 20, its training time included). Reported: mean
+    retries and total time (factorize + refinement towards 1e-10, GMRES-IR by
+    default: the perturbed static-pivot factors are rough inverses), over all
+    matrices and over those both arms refined to 1e-10. The sequence as
+    specified (quasi-definite, c = 0) is run beside the nonconvex variant."""
+    shifts = [0.0] if args.curvature_shift == 0.0 else [0.0, args.curvature_shift]
+    results = {}
+    for c in shifts:
+        results["as_specified" if c == 0.0 else f"curvature_shift_{c:g}"] = learned_experiment(args, c)
+    line = {"metric": "interior-point sequence: mean retries and total time, learned vs plain escalation",
+            "config": {"workload": f"config 5: K_k = [[-E_k, A^T], [A, F_k]] from L7(20^3), {args.ip_steps} "
+                                   f"matrices (train {args.ip_train})", "refinement": args.ip_refine,
+                       "target_backward_error": 1e-10},
+            "results": results, "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+
+
+def learned_experiment(args, curvature_shift):
     import math
     import numpy as np
-    from ma57_b200 import Mode, OrderingType, RefinementOptions, SymLDLT, learned
+    from ma57_b200 import GmresRefinementOptions, Mode, OrderingType, RefinementOptions, SymLDLT, learned
     from ma57_b200 import matrices as M
-    seq = M.InteriorPointSequence(k=20, steps=args.ip_steps, curvature_shift=args.curvature_shift)
+    seq = M.InteriorPointSequence(k=20, steps=args.ip_steps, curvature_shift=curvature_shift)
     signs = np.r_[-np.ones(seq.n1), np.ones(seq.n2)]
 
     def run(steps, model, online=False):
@@ -330,7 +409,11 @@ def run_learned(args):
             s.setInitialRegularizationDelta(base)
             s.setFrontDeltas(None if model is None else model.front_deltas(F, base))
             s.factorize(K)
-            r = s.solveWithRefinement(K, seq.b, RefinementOptions(max_iterations=30, tolerance=1e-10))
+            if args.ip_refine == "gmres":
+                r = s.solveWithGmresRefinement(K, seq.b, GmresRefinementOptions(max_outer=10, restart=20,
+                                                                                   tolerance=1e-10))
+            else:
+                r = s.solveWithRefinement(K, seq.b, RefinementOptions(max_iterations=30, tolerance=1e-10))
             T = np.full(F.shape[0], math.log10(s.lastRegularizationDelta() / base))
             if online:  # the sequence's own retry history keeps the model current
                 model.update(F, T, retries=s.regularizationRetriesUsed())
@@ -352,16 +435,124 @@ def run_learned(args):
     plain = run(range(args.ip_train, args.ip_steps), None)
     seq.logx, seq.st.pos = state
     lrn = run(range(args.ip_train, args.ip_steps), model, online=True)
-    summ = lambda o: {"mean_retries": float(np.mean(o["retries"])), "total_s": float(np.sum(o["ms"]) / 1e3),
-                      "refined_to_1e-10": int(np.sum(np.asarray(o["resid"]) <= 1e-10)),
-                      "median_residual": float(np.median(o["resid"]))}
-    line = {"metric": "interior-point sequence: mean retries and total time, learned vs plain escalation",
-            "config": {"workload": f"config 5: K_k = [[-E_k, A^T], [A, F_k]], n1={seq.n1}, n2={seq.n2}, "
-                                   f"{args.ip_steps} matrices (train {args.ip_train})",
-                       "curvature_shift": args.curvature_shift, "train_samples": int(sum(len(t) for t in train["targets"])),
-                       "train_loss": loss, "train_s": t_train, "margin_decades": model.margin},
-            "plain": summ(plain), "learned": summ(lrn), "data": "synthetic"}
-    print(json.dumps(line), flush=True)
+    both = (np.asarray(plain["resid"]) <= 1e-10) & (np.asarray(lrn["resid"]) <= 1e-10)
+
+    def summ(o, sel=None):
+        sel = np.ones(len(o["retries"]), bool) if sel is None else sel
+        ms = np.asarray(o["ms"])[sel]
+        return {"mean_retries": float(np.mean(np.asarray(o["retries"])[sel])) if sel.any() else None,
+                "total_s": float(np.sum(ms) / 1e3), "matrices": int(sel.sum()),
+                "refined_to_1e-10": int(np.sum(np.asarray(o["resid"])[sel] <= 1e-10)),
+                "median_residual": float(np.median(np.asarray(o["resid"])[sel])) if sel.any() else None}
+
+    return {"curvature_shift": curvature_shift, "n1": seq.n1, "n2": seq.n2,
+            "train_samples": int(sum(len(t) for t in train["targets"])), "train_loss": loss, "train_s": t_train,
+            "margin_decades": model.margin, "plain": summ(plain), "learned": summ(lrn),
+            "both_refined_to_1e-10": {"matrices": int(both.sum()), "plain": summ(plain, both),
+                                      "learned": summ(lrn, both)}}
+
+
+def run_configs(args):
+    """Configs 1 and 2 at their stated sizes, GPU and CPU side by side, one
+    JSON line each. Config 1: L7(20^3) - 2I, AMD, one right-hand side,
+    factorize + solve. Config 2: the KKT system (n = 60000),
+    StaticRegularized with setKKTBlockSizes(40000, 20000), AMD, factorize +
+    refinement to 1e-12. GPU: best of --steps after --warmup, device time of
+    factorize and of solve (+ refinement), and the same step end to end
+    through the Python API with host arrays. CPU: the oracle (the reference's
+    algorithm, C++ with its OpenMP task DAG) with every host thread and with
+    setParallel(false), best of --cpu-reps for config 1 and one run for
+    config 2 (minutes long; --no-cpu skips it); analysis excluded."""
+    import numpy as np
+    from ma57_b200 import Mode, OrderingType, RefinementOptions, SymLDLT
+    from ma57_b200 import matrices as M
+    from oracle.pyoracle import OracleSymLDLT, analyze
+
+    def backward_error(A, X, B):
+        R = B - M.sym_full(A) @ X
+        return float(np.abs(R).max() / (abs(A).sum(axis=1).max() * np.abs(X).max() + np.abs(B).max()))
+
+    A1, b1 = M.config1(20)
+    K, b2, n1, n2 = M.config2()
+    cases = [("config 1: L7(20^3) - 2I, AMD, nrhs 1", A1, b1, None),
+             ("config 2: KKT [[-E, A^T], [A, F]], n = 60000, StaticRegularized (40000, 20000), AMD", K, b2, (n1, n2))]
+    for name, A, B, kkt in cases:
+        clk = clocks_start(0)
+        s = SymLDLT()
+        s.setOrdering(OrderingType.AMD)
+        if kkt:
+            s.setMode(Mode.StaticRegularized)
+            s.setKKTBlockSizes(*kkt)
+        t0 = time.perf_counter()
+        s.analyzePattern(A)
+        t_an = time.perf_counter() - t0
+        ropt = RefinementOptions(max_iterations=10, tolerance=1e-12)
+
+        def step():
+            s.factorize(A)
+            fac = s.phase_ms()[6]
+            t1 = time.perf_counter()
+            if kkt:
+                r = s.solveWithRefinement(A, B, ropt)
+                x, it = r.x, r.diagnostics.iterations
+            else:
+                x, it = s.solve(B), 0
+            return fac, 1e3 * (time.perf_counter() - t1), x, it
+
+        for _ in range(max(3, args.warmup)):
+            step()
+        fac_ms, sol_ms, e2e_ms = [], [], []
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            f, so, x, it = step()
+            e2e_ms.append(1e3 * (time.perf_counter() - t0))
+            fac_ms.append(f)
+            sol_ms.append(so)
+        clocks = clocks_stop(clk)
+        line = {"metric": "factorize + solve time", "value": (min(fac_ms) + min(sol_ms)) / 1e3, "unit": "s",
+                "higher_is_better": False, "steps": len(fac_ms), "warmup": max(3, args.warmup), "n_gpus": 1,
+                "dtype": "f64", "data": "synthetic", "config": {"workload": name, "n": int(A.shape[0])},
+                "gpu": {"factorize_ms": min(fac_ms), "solve_ms": min(sol_ms),
+                        "solve_what": "solveWithRefinement to 1e-12" if kkt else "solve",
+                        "e2e_ms": min(e2e_ms), "e2e_note": "host values and right-hand side through the Python API",
+                        "analyze_s": t_an, "inertia": list(s.inertia().as_tuple()),
+                        "retries": s.regularizationRetriesUsed() if kkt else 0, "refine_iterations": it,
+                        "backward_error": backward_error(A, x, B)},
+                "clocks": clocks}
+        if not args.no_cpu:
+            sf = analyze(A, 0)
+            o = OracleSymLDLT(sf)
+            if kkt:
+                o.set(mode=1)
+                o.setKKTBlockSizes(*kkt)
+            threads = os.cpu_count() or 1
+            cpu = {}
+            for label, par in (("openmp", 1), ("sequential", 0)):
+                if kkt and par == 0:
+                    continue  # tens of minutes: the parallel run alone
+                o.set(parallel=par, num_threads=threads)
+                reps = 1 if kkt else max(1, args.cpu_reps)
+                fs, ss = [], []
+                for _ in range(reps):
+                    t0 = time.perf_counter()
+                    o.factorize(A)
+                    t1 = time.perf_counter()
+                    if kkt:
+                        xo, d = o.solveWithRefinement(A, B, max_iterations=10, tolerance=1e-12)
+                    else:
+                        xo = o.solve(B)
+                    t2 = time.perf_counter()
+                    fs.append(t1 - t0)
+                    ss.append(t2 - t1)
+                cpu[label] = {"factorize_s": min(fs), "solve_s": min(ss), "reps": reps,
+                              "threads": threads if par else 1, "inertia": list(o.inertia()),
+                              "backward_error": backward_error(A, xo, B)}
+            line["cpu_baseline"] = {"value": cpu["openmp"]["factorize_s"] + cpu["openmp"]["solve_s"], "unit": "s",
+                                    "cores": threads, "kind": "port",
+                                    "sample": "oracle on the full configuration, best of reps (analysis excluded)",
+                                    "runs": cpu}
+        print(json.dumps(line), flush=True)
+        del s
 
 
 def run_reference(args):
@@ -620,6 +811,8 @@ def run_ours(args):
                     "backward_error": bw, "refine_iterations": refine_iters,
                     "analyze_s": t_analyze, "factor_flops": stats.get("factor_flops"),
                     "kernel_ms_per_step": {k: v[1] / max(1, args.steps) for k, v in kstats.items()},
+                    "kernel_flops_per_step": {k: v[2] / max(1, args.steps) for k, v in kstats.items() if v[2]},
+                    "kernel_launches_per_step": {k: v[0] / max(1, args.steps) for k, v in kstats.items() if v[0]},
                     "panels": {k: v for k, v in stats.items() if k.startswith("panels_") or k.startswith("seq_")}},
         "precision_comparison": comparison,
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(8 * (2 * len(vals) + n * nrhs)),
@@ -657,13 +850,18 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=240.0,
                     help="reference arm: seconds of timed steps (at least one full step runs)")
     ap.add_argument("--graph", type=int, default=1, help="graph launch of the factorization's static pass")
-    ap.add_argument("--workload", default="config3", choices=["config3", "dense", "batched", "learned"])
+    ap.add_argument("--workload", default="config3", choices=["config3", "dense", "batched", "learned", "configs"])
+    ap.add_argument("--cpu-reps", type=int, default=5, help="configs workload: best-of repetitions on the CPU")
     ap.add_argument("--curvature-shift", type=float, default=0.0,
                     help="learned workload: 0 = config 5 as specified; c > 0 = E_k - c I (nonconvex variant)")
     ap.add_argument("--ip-steps", type=int, default=500)
     ap.add_argument("--ip-train", type=int, default=100)
+    ap.add_argument("--ip-refine", default="gmres", choices=["gmres", "classic"],
+                    help="learned workload: refinement towards 1e-10 (GMRES-IR or fixed-precision)")
     ap.add_argument("--n", type=int, default=4096, help="dense workload: front size")
     ap.add_argument("--systems", type=int, default=4096, help="batched workload: number of systems")
+    ap.add_argument("--batch-size", type=int, default=256, help="batched workload: systems per served batch")
+    ap.add_argument("--cpu-systems", type=int, default=256, help="batched workload: systems in the CPU sample")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -673,6 +871,8 @@ def main():
         run_batched(args)
     elif args.workload == "learned":
         run_learned(args)
+    elif args.workload == "configs":
+        run_configs(args)
     else:
         run_ours(args)
 

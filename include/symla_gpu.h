@@ -313,6 +313,10 @@ int symla_gpu_set_graph(symla_gpu_ctx* ctx, int enable);
  * cluster size too small for the level's fronts falls back to the default. */
 int symla_gpu_level_info(symla_gpu_ctx* ctx, int level, int* out6);
 int symla_gpu_set_level_schedule(symla_gpu_ctx* ctx, int level, int small_threads, int cluster_ctas);
+/* Rows per tile of the level's Schur-complement update (the tile shape
+ * rows x 64): 128, or 64 for levels of small fronts; 0 = 128. */
+int symla_gpu_set_level_update_rows(symla_gpu_ctx* ctx, int level, int rows);
+int symla_gpu_level_update_rows(symla_gpu_ctx* ctx, int level, int* rows);
 int symla_gpu_graph_stats(symla_gpu_ctx* ctx, int* captures, int* resumes);
 int symla_gpu_kernel_stats(symla_gpu_ctx* ctx, int kind, double* out4);
 /* The same per tree level (the per-phase timers the reference keeps under
@@ -398,6 +402,28 @@ int symla_mlp_train(symla_mlp* mlp, const double* X, const double* T, int B, int
 #define SYMLA_NOALLOC_RESIDUAL_MAX_ENTRIES (1 << 20)
 int symla_gpu_relative_residual_noalloc(symla_gpu_ctx* ctx, const double* X, int ldx, const double* B, int ldb,
                                         int nrhs, double* rel_residual);
+
+/* Bounds-checked build (libsymla_b200_checked.so, compiled with
+ * -DSYMLA_GPU_CHECKED; same entry points). Before and after every
+ * factorization and before every solve it validates the device tables
+ * (front descriptors and their storage, row indices, extend-add maps, A's
+ * scatter map, pivot counts, solve workspace slices), and inside the kernels
+ * every access whose index comes from a table is checked before it is made.
+ * A failed check skips the access and records the first failure in a status
+ * word on the device; the call then returns SYMLA_ERR_INTERNAL naming it, and
+ * every later call on the context fails with SYMLA_ERR_CUDA. No check traps
+ * or asserts. No counterpart in the reference (its opt-in sanitizer builds
+ * are CPU-side, test/CMakeLists.txt:141-149).
+ *
+ * symla_gpu_checked_build: 1 in the checked build, 0 in the ordinary one.
+ * symla_gpu_check_status: the status word (failed checks so far, the first
+ * one's code, the front or entry where it happened); always zero in the
+ * ordinary build. Codes: 1 descriptor shape, 2 front storage, 3 row index,
+ * 4 child link, 5 parent-to-child map, 6 child-to-parent map, 7 A scatter
+ * entry, 8 pivot count, 9 contribution-block read, 10 solve permutation,
+ * 11 level-solve row, 12 solve workspace. */
+int symla_gpu_checked_build(void);
+int symla_gpu_check_status(symla_gpu_ctx* ctx, int* count, int* code, long long* where);
 
 #ifdef __cplusplus
 }

@@ -2,7 +2,10 @@
 
 The library is required: importing this module fails loudly when it is
 missing, and every device entry point reports an error (no CPU fallback)
-when no CUDA device is present.
+when no CUDA device is present. With SYMLA_GPU_LIBRARY=checked in the
+environment the process loads the bounds-checked build,
+``lib/libsymla_b200_checked.so`` (same entry points); any other value is
+taken as the path of the library to load.
 """
 from __future__ import annotations
 
@@ -10,7 +13,22 @@ import ctypes as C
 import os
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libsymla_b200.so"
+LIB_DIR = Path(__file__).resolve().parent / "lib"
+PRODUCT_LIB_PATH = LIB_DIR / "libsymla_b200.so"
+CHECKED_LIB_PATH = LIB_DIR / "libsymla_b200_checked.so"
+
+
+def library_path() -> Path:
+    """The library this process loads (see the module docstring)."""
+    choice = os.environ.get("SYMLA_GPU_LIBRARY", "")
+    if not choice:
+        return PRODUCT_LIB_PATH
+    if choice == "checked":
+        return CHECKED_LIB_PATH
+    return Path(choice)
+
+
+LIB_PATH = library_path()
 
 SYMLA_OK = 0
 SYMLA_ERR_NOT_ANALYZED = 1
@@ -105,6 +123,8 @@ _SIGS = {
     "symla_gpu_set_graph": (_i, [_p, _i]),
     "symla_gpu_level_info": (_i, [_p, _i, _pi]),
     "symla_gpu_set_level_schedule": (_i, [_p, _i, _i, _i]),
+    "symla_gpu_set_level_update_rows": (_i, [_p, _i, _i]),
+    "symla_gpu_level_update_rows": (_i, [_p, _i, _pi]),
     "symla_gpu_graph_stats": (_i, [_p, _pi, _pi]),
     "symla_gpu_kernel_stats": (_i, [_p, _i, _pd]),
     "symla_gpu_level_kernel_stats": (_i, [_p, _i, _i, _pd]),
@@ -114,6 +134,8 @@ _SIGS = {
     "symla_gpu_set_wait_limit_ns": (_i, [_p, C.c_ulonglong]),
     "symla_gpu_set_memory_limit": (_i, [C.c_longlong]),
     "symla_gpu_relative_residual_noalloc": (_i, [_p, _p, _i, _p, _i, _i, _pd]),
+    "symla_gpu_checked_build": (_i, []),
+    "symla_gpu_check_status": (_i, [_p, _pi, _pi, C.POINTER(C.c_longlong)]),
     "symla_mlp_create": (_i, [_i, _pd, C.POINTER(_p)]),
     "symla_mlp_destroy": (None, [_p]),
     "symla_mlp_get_params": (_i, [_p, _pd]),

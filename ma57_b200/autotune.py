@@ -1,9 +1,12 @@
 """Front-size-to-tile-shape schedule chosen by measurement.
 
-Two launch shapes depend on front size and have no single best value:
-the width of the small-front kernel (128 or 256 threads per front) and the
+Three launch shapes depend on front size and have no single best value:
+the width of the small-front kernel (128 or 256 threads per front), the
 number of CTAs in the panel cluster of the large fronts (2, 4, 8 or 16; more
-CTAs hold fewer rows each but occupy more SMs). The tree levels are bucketed by
+CTAs hold fewer rows each but occupy more SMs) and the tile shape of their
+Schur-complement update (128 x 64 or 64 x 64: the smaller tile wastes less
+of small fronts' trailing blocks, the larger reuses operands more). The tree
+levels are bucketed by
 the largest front they hold, and a coordinate search times the actual
 factorization (CUDA events around the numeric factorization) for each
 candidate shape of one bucket at a time, keeping the fastest. The result is
@@ -45,12 +48,17 @@ def _bucket(value, edges):
 
 
 def apply(solver, schedule):
-    """schedule: {"small": {bucket: threads}, "large": {bucket: ctas}}."""
+    """schedule: {"small": {bucket: threads}, "large": {bucket: ctas},
+    "update": {bucket: tile rows}} (missing entries: the default shape)."""
     lib = L.load()
     for lv, info in enumerate(level_info(solver)):
         st = schedule["small"].get(_bucket(info["small_max_m"], SMALL_BUCKETS), 0) if info["small"] else 0
-        cl = schedule["large"].get(_bucket(info["large_max_m"], LARGE_BUCKETS), 0) if info["large"] else 0
+        lb = _bucket(info["large_max_m"], LARGE_BUCKETS)
+        cl = schedule["large"].get(lb, 0) if info["large"] else 0
+        ur = schedule.get("update", {}).get(lb, 0) if info["large"] else 0
         if lib.symla_gpu_set_level_schedule(solver._ctx.h, lv, st, cl) != L.SYMLA_OK:
+            raise RuntimeError(L.last_error())
+        if lib.symla_gpu_set_level_update_rows(solver._ctx.h, lv, ur) != L.SYMLA_OK:
             raise RuntimeError(L.last_error())
 
 
@@ -69,14 +77,15 @@ def tune(solver, A, reps: int = 2):
     info = level_info(solver)
     small_b = sorted({_bucket(i["small_max_m"], SMALL_BUCKETS) for i in info if i["small"]})
     large_b = sorted({_bucket(i["large_max_m"], LARGE_BUCKETS) for i in info if i["large"]})
-    schedule = {"small": {}, "large": {}}
+    schedule = {"small": {}, "large": {}, "update": {}}
     apply(solver, schedule)
     base = _factor_ms(solver, A, reps)
     best = base
-    for kind, buckets, cands in (("small", small_b, (128, 256)), ("large", large_b, (2, 4, 8, 16))):
+    for kind, buckets, cands in (("small", small_b, (128, 256)), ("large", large_b, (2, 4, 8, 16)),
+                                 ("update", large_b, (64, 128))):
         for b in buckets:
             for cand in cands:
-                trial = {"small": dict(schedule["small"]), "large": dict(schedule["large"])}
+                trial = {k: dict(v) for k, v in schedule.items()}
                 trial[kind][b] = cand
                 apply(solver, trial)
                 t = _factor_ms(solver, A, reps)

@@ -18,6 +18,7 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIBDIR = PKG / "lib"
 LIB = LIBDIR / "libsymla_b200.so"
+CHECKED_LIB = LIBDIR / "libsymla_b200_checked.so"
 CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -49,33 +50,41 @@ def _headers() -> list[Path]:
     return hs
 
 
-def build(verbose: bool = False, force: bool = False) -> Path:
-    """Compile every source that changed and link the shared library."""
-    BUILD.mkdir(exist_ok=True)
-    LIBDIR.mkdir(exist_ok=True)
+def _build_library(lib: Path, objdir: Path, defines: list[str], verbose: bool, force: bool) -> None:
+    objdir.mkdir(parents=True, exist_ok=True)
     hdrs = _headers()
     objs: list[Path] = []
     for src in HOST_SRCS:
         s = CSRC / src
-        o = BUILD / (s.stem + ".o")
+        o = BUILD / (s.stem + ".o")  # host code is the same in both builds
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
             _run(["g++", "-std=c++17", "-O3", "-fPIC", "-Wall", "-c", str(s), "-o", str(o)])
     for src in CUDA_SRCS:
         s = CSRC / src
-        o = BUILD / (s.stem + ".o")
+        o = objdir / (s.stem + ".o")
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
             cmd = [NVCC, *ARCH, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC",
-                   "--expt-relaxed-constexpr", "-c", str(s), "-o", str(o)]
+                   "--expt-relaxed-constexpr", *defines, "-c", str(s), "-o", str(o)]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
             _run(cmd)
     metis = CUDA_HOME / "lib64" / "libmetis_static.a"
-    if force or _stale(LIB, objs):
+    if force or _stale(lib, objs):
         # --no-undefined: a missing symbol fails the build, not the first dlopen
-        _run([NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), str(metis), "-lcudart_static",
+        _run([NVCC, *ARCH, "-shared", "-o", str(lib), *map(str, objs), str(metis), "-lcudart_static",
               "-Xlinker", "--no-undefined"])
+
+
+def build(verbose: bool = False, force: bool = False, checked: bool = True) -> Path:
+    """Compile every source that changed and link the shared library, and
+    (checked=True) its bounds-checked variant (-DSYMLA_GPU_CHECKED)."""
+    BUILD.mkdir(exist_ok=True)
+    LIBDIR.mkdir(exist_ok=True)
+    _build_library(LIB, BUILD, [], verbose, force)
+    if checked:
+        _build_library(CHECKED_LIB, BUILD / "checked", ["-DSYMLA_GPU_CHECKED"], verbose, force)
     bsrc = CSRC / BENCH_SRC
     bobj = BUILD / "fp64_peak.o"
     if force or _stale(bobj, [bsrc]):
@@ -87,8 +96,9 @@ def build(verbose: bool = False, force: bool = False) -> Path:
 
 def clean() -> None:
     shutil.rmtree(BUILD, ignore_errors=True)
-    if LIB.exists():
-        LIB.unlink()
+    for lib in (LIB, CHECKED_LIB):
+        if lib.exists():
+            lib.unlink()
 
 
 if __name__ == "__main__":

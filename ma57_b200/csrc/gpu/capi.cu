@@ -687,6 +687,7 @@ void build_plan(symla_gpu_ctx* c, const symla_host::SymbolicFactor& sf, const in
 void free_dynamic(symla_gpu_ctx* c) {
   for (void* p : c->dyn_allocs) dfree(p);
   c->dyn_allocs.clear();
+  c->dyn_front_blocks.clear();
 }
 
 // Reset descriptors / links to the static plan (start of every factorize).
@@ -738,7 +739,71 @@ KernelOpts make_kernel_opts(symla_gpu_ctx* c, const symla_factor_opts* o) {
   k.a_j = c->d_a_j;
   k.a_pos = c->d_a_pos;
   k.a_idx = c->d_a_idx;
+  k.nnz = c->nnz;
+  k.chk = c->d_check;
   return k;
+}
+
+// ---- checked build: table validation and the status word --------------------
+const char* check_code_name(int code) {
+  switch (code) {
+    case kChkFrontShape: return "front descriptor shape";
+    case kChkFrontStorage: return "front storage outside its allocation";
+    case kChkRowIndex: return "front row index outside [0, n)";
+    case kChkChildLink: return "child link";
+    case kChkInvMap: return "parent-to-child map entry";
+    case kChkRelMap: return "child-to-parent map entry";
+    case kChkAEntry: return "A scatter entry";
+    case kChkPivots: return "pivot count";
+    case kChkGather: return "contribution-block read";
+    case kChkPermute: return "solve permutation entry";
+    case kChkSolveRow: return "level-solve row index";
+    case kChkWorkspace: return "solve workspace slice";
+    default: return "unknown check";
+  }
+}
+
+void check_status_word(symla_gpu_ctx* c, const char* when) {
+  if constexpr (!kCheckedBuild) return;
+  CheckWord w{};
+  CK(cudaMemcpyAsync(&w, c->d_check, sizeof w, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (w.count != 0) {
+    c->unusable = true;
+    throw SymlaError(SYMLA_ERR_INTERNAL, std::string("bounds check failed ") + when + ": " +
+                                             check_code_name(w.code) + " (front or entry " +
+                                             std::to_string(w.where) + ", " + std::to_string(w.count) +
+                                             " failed checks); the context is no longer usable");
+  }
+}
+
+// Validate every front's tables (phase as launch_validate_fronts), then, with
+// sync, read the status word: a failure marks the context unusable.
+void validate_tables(symla_gpu_ctx* c, int phase, const KernelOpts& ko, const char* when) {
+  if constexpr (!kCheckedBuild) return;
+  cudaStream_t st = c->stream;
+  c->h_ranges.clear();
+  c->h_ranges.push_back(c->d_arena);
+  c->h_ranges.push_back(c->d_arena + c->arena_doubles);
+  for (const auto& b : c->dyn_front_blocks) {
+    c->h_ranges.push_back(b.first);
+    c->h_ranges.push_back(b.first + b.second);
+  }
+  if (c->h_ranges.size() > c->ranges_cap) {
+    dfree(c->d_ranges);
+    c->ranges_cap = c->h_ranges.size() * 2;
+    c->d_ranges = dalloc<const double*>(c->ranges_cap);
+  }
+  CK(cudaMemcpyAsync(c->d_ranges, c->h_ranges.data(), c->h_ranges.size() * sizeof(const double*),
+                     cudaMemcpyHostToDevice, st));
+  long long wtotal = 0;
+  for (int s = 0; s < c->numSN; ++s) wtotal += static_cast<long long>(c->hdesc[s].m) * c->w_nrhs;
+  launch_validate_fronts(c->d_desc, c->d_links, c->d_state, nullptr, c->numSN, c->numSN, c->n, c->d_a_colptr, ko,
+                         c->d_ranges, static_cast<int>(c->h_ranges.size() / 2), c->d_W, c->d_W + wtotal, c->w_nrhs,
+                         phase, st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  check_status_word(c, when);
 }
 
 void launch_panel_iteration(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
@@ -761,12 +826,14 @@ void launch_panel_iteration(symla_gpu_ctx* c, const LevelLists& L, int level, co
     // FP64: near and far updates in one launch (disjoint column ranges);
     // timed as the far (Schur-complement) kind
     timed(c, SYMLA_KERNEL_TRAILING, 0.0, 0.0, [&] {
-      launch_update_both(c->d_desc, c->d_state, d_large, nl, L.trailing_grid, c->d_glob, level, dynamic, st);
+      launch_update_both(c->d_desc, c->d_state, d_large, nl, L.trailing_grid, c->d_glob, level, dynamic, st,
+                         L.update_rows == 64 ? 64 : 128);
     });
     return;
   }
   timed(c, SYMLA_KERNEL_NEAR, 0.0, 0.0, [&] {
-    launch_update(false, c->d_desc, c->d_state, d_large, nl, L.trailing_grid, c->d_glob, level, dynamic, st);
+    launch_update(false, c->d_desc, c->d_state, d_large, nl, L.trailing_grid, c->d_glob, level, dynamic, st,
+                  nullptr, L.update_rows == 64 ? 64 : 128);
   });
   if (ko.precision == SYMLA_PREC_MIXED) {
     timed(c, SYMLA_KERNEL_TRAILING, 0.0, 0.0, [&] {
@@ -781,12 +848,13 @@ void launch_panel_iteration(symla_gpu_ctx* c, const LevelLists& L, int level, co
                       dynamic, c->d_tc_err, st);
         // blocks the growth guard kept off the tensor cores
         launch_update(true, c->d_desc, c->d_state, d_large + b, cnt, L.trailing_grid, c->d_glob, level, dynamic,
-                      st, guard);
+                      st, guard, L.update_rows == 64 ? 64 : 128);
       }
     });
   } else {
     timed(c, SYMLA_KERNEL_TRAILING, 0.0, 0.0, [&] {
-      launch_update(true, c->d_desc, c->d_state, d_large, nl, L.trailing_grid, c->d_glob, level, dynamic, st);
+      launch_update(true, c->d_desc, c->d_state, d_large, nl, L.trailing_grid, c->d_glob, level, dynamic, st,
+                    nullptr, L.update_rows == 64 ? 64 : 128);
     });
   }
 }
@@ -971,6 +1039,7 @@ void replan_front(symla_gpu_ctx* c, int s) {
   FrontDesc d = c->hdesc[s];
   double* F = dalloc<double>(static_cast<size_t>(f.ld) * f.m);
   c->dyn_allocs.push_back(F);
+  c->dyn_front_blocks.push_back({F, static_cast<size_t>(f.ld) * f.m});
   int* fidx = dupload(frontIdx, c->stream);
   c->dyn_allocs.push_back(fidx);
   int* lperm = dalloc<int>(f.m);
@@ -1046,6 +1115,7 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
   reset_to_static(c);
   const KernelOpts ko = make_kernel_opts(c, o);
   CK(cudaMemsetAsync(c->d_state, 0, c->numSN * sizeof(FrontState), st));
+  validate_tables(c, 0, ko, "before the factorization");
   FactorGlobals g0{INT_MAX, 0, -1, INT_MAX, 0.0, 0.0, 0.0, 0, 0, 0, 0, c->wait_ns, {0, 0, 0, 0}, 0};
   CK(cudaMemcpyAsync(c->d_glob, &g0, sizeof g0, cudaMemcpyHostToDevice, st));
   const bool mixed = o->precision == SYMLA_PREC_MIXED;
@@ -1107,6 +1177,7 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
           c->tc_guard_cap = L.large.size();
         }
       }
+      validate_tables(c, 0, ko, "after re-planning delayed pivots");
       launch_level(c, L, l, ko, 1, L.d_small, L.d_large, L.d_tasks);
       read_states(c);
       free_level_device(L);
@@ -1115,6 +1186,7 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
   CK(cudaEventRecord(c->ev[1], st));
   CK(cudaEventSynchronize(c->ev[1]));
   collect_pending(c);
+  validate_tables(c, 1, ko, "after the factorization");
   if (c->profiling) {
     FactorGlobals gf;
     CK(cudaMemcpy(&gf, c->d_glob, sizeof gf, cudaMemcpyDeviceToHost));
@@ -1137,6 +1209,8 @@ void run_factorization(symla_gpu_ctx* c, const symla_factor_opts* o, symla_facto
     for (int i = 0; i < 4; ++i) c->seq_dec_counts[i] = gp.seq_dec[i];
     if (gp.error == kPanelErrTimeout)
       throw SymlaError(SYMLA_ERR_TIMEOUT, "panel factorization: a bulk copy of the panel rows did not complete");
+    if (gp.error == kUpdateErrTimeout)
+      throw SymlaError(SYMLA_ERR_TIMEOUT, "Schur update: a bulk copy of the staging ring did not complete");
   }
   if (mixed) {
     int tcerr = 0;
@@ -1308,8 +1382,18 @@ void device_solve(symla_gpu_ctx* c, const double* dB, int ldb, int nrhs, double*
   ensure_vectors(c, nrhs);
   ensure_workspace(c, nrhs);
   ensure_solve_tasks(c);
+  if constexpr (kCheckedBuild) {
+    KernelOpts ko;
+    std::memset(&ko, 0, sizeof ko);
+    ko.a_j = c->d_a_j;
+    ko.a_pos = c->d_a_pos;
+    ko.a_idx = c->d_a_idx;
+    ko.nnz = c->nnz;
+    ko.chk = c->d_check;
+    validate_tables(c, 2, ko, "before the solve");
+  }
   const int n = c->n;
-  launch_permute_in(n, nrhs, c->d_perm, dB, ldb, c->d_Bp, st);
+  launch_permute_in(n, nrhs, c->d_perm, dB, ldb, c->d_Bp, st, c->d_check);
   CK(cudaEventRecord(c->ev[2], st));
   const int chunk = solve_rhs_chunk();
   for (int c0 = 0; c0 < nrhs; c0 += chunk) {
@@ -1340,7 +1424,7 @@ void device_solve(symla_gpu_ctx* c, const double* dB, int ldb, int nrhs, double*
   }
   c->cur_level = -1;
   CK(cudaEventRecord(c->ev[4], st));
-  launch_permute_out(n, nrhs, c->d_perm, c->d_Xf, dX, ldx, st);
+  launch_permute_out(n, nrhs, c->d_perm, c->d_Xf, dX, ldx, st, c->d_check);
   CK(cudaGetLastError());
 }
 
@@ -1348,16 +1432,26 @@ void check_solve_error(symla_gpu_ctx* c) {
   int err = 0;
   CK(cudaMemcpyAsync(&err, c->d_solve_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (err == kSolveErrBounds) {
+    c->unusable = true;
+    const CheckWord w{1, kChkSolveRow, -1};  // the level kernels report through the solve's error word
+    CK(cudaMemcpy(c->d_check, &w, sizeof w, cudaMemcpyHostToDevice));
+    throw SymlaError(SYMLA_ERR_INTERNAL,
+                     "bounds check failed in the level solve: a row index or a child's workspace row out of range; "
+                     "the context is no longer usable");
+  }
   if (err != 0) {
     CK(cudaMemsetAsync(c->d_solve_err, 0, sizeof(int), c->stream));
     throw SymlaError(SYMLA_ERR_TIMEOUT, "solve: a pipelined block wait timed out");
   }
+  check_status_word(c, "in the solve");
 }
 
 void check_usable(symla_gpu_ctx* c) {
   if (c->unusable)
     throw SymlaError(SYMLA_ERR_CUDA,
-                     "symla_gpu: the context is no longer usable (a tensor-core tile's drain timed out); destroy it");
+                     "symla_gpu: the context is no longer usable (an earlier call left its device state untrusted: "
+                     "a tensor-core tile's drain timed out, or a bounds check failed); destroy it");
 }
 
 void check_solvable(symla_gpu_ctx* c) {
@@ -1463,7 +1557,9 @@ extern "C" int symla_gpu_create(const symla_symbolic* sym, int n, const int* col
     CK(solve_max_resident(device, &c->fwd_resident, &c->bwd_resident));
     c->d_solve_err = dalloc<int>(1);
     c->d_counter = dalloc<int>(1);
+    c->d_check = dalloc<CheckWord>(1);
     CK(cudaMemsetAsync(c->d_solve_err, 0, sizeof(int), c->stream));
+    CK(cudaMemsetAsync(c->d_check, 0, sizeof(CheckWord), c->stream));
     build_plan(c, sym->sf, colptr, rowind);
   });
   tl_alloc_budget = -1;
@@ -1487,7 +1583,7 @@ extern "C" void symla_gpu_destroy(symla_gpu_ctx* c) {
                   c->d_Bp, c->d_Z, c->d_Xf, c->d_B, c->d_X, c->d_R, c->d_dX, c->d_Xn, c->d_Rn, c->d_norms,
                   c->d_scratch_int, c->d_flag_base, c->d_flags, c->d_solve_err, c->d_counter,
                   c->d_tcws, c->d_tc_err, c->d_tc_guard, c->d_hflags, c->d_hscratch,
-                  c->d_gmres, c->d_zero, c->d_gpart, c->d_gcoef};
+                  c->d_gmres, c->d_zero, c->d_gpart, c->d_gcoef, c->d_check, c->d_ranges};
   for (void* p : ptrs) dfree(p);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
@@ -2090,6 +2186,27 @@ extern "C" int symla_gpu_set_level_schedule(symla_gpu_ctx* c, int level, int sma
   return SYMLA_OK;
 }
 
+extern "C" int symla_gpu_set_level_update_rows(symla_gpu_ctx* c, int level, int rows) {
+  if (!c || level < 0 || level >= c->numLevels) return set_error(SYMLA_ERR_INVALID, "level out of range");
+  if (rows != 0 && rows != 64 && rows != 128)
+    return set_error(SYMLA_ERR_INVALID, "symla_gpu_set_level_update_rows: rows in {0, 64, 128}");
+  auto& L = c->levels[level];
+  if (L.update_rows != rows) {
+    L.update_rows = rows;
+    if (c->graph_exec) {  // the captured launches used the old shape
+      cudaGraphExecDestroy(c->graph_exec);
+      c->graph_exec = nullptr;
+    }
+  }
+  return SYMLA_OK;
+}
+
+extern "C" int symla_gpu_level_update_rows(symla_gpu_ctx* c, int level, int* rows) {
+  if (!c || !rows || level < 0 || level >= c->numLevels) return set_error(SYMLA_ERR_INVALID, "level out of range");
+  *rows = c->levels[level].update_rows == 64 ? 64 : 128;
+  return SYMLA_OK;
+}
+
 extern "C" int symla_gpu_set_memory_limit(long long bytes) {
   if (bytes < 0) return set_error(SYMLA_ERR_INVALID, "symla_gpu_set_memory_limit: negative limit");
   g_create_limit.store(bytes);
@@ -2162,3 +2279,17 @@ extern "C" void symla_gpu_reset_kernel_stats(symla_gpu_ctx* c) {
 }
 
 extern "C" long long symla_gpu_launch_count(symla_gpu_ctx* c) { return c ? c->launches : 0; }
+
+extern "C" int symla_gpu_checked_build(void) { return kCheckedBuild ? 1 : 0; }
+
+extern "C" int symla_gpu_check_status(symla_gpu_ctx* c, int* count, int* code, long long* where) {
+  if (!c || !count || !code || !where) return set_error(SYMLA_ERR_INVALID, "symla_gpu_check_status: NULL argument");
+  return guarded([&] {
+    CheckWord w{};
+    CK(cudaMemcpyAsync(&w, c->d_check, sizeof w, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *count = w.count;
+    *code = w.code;
+    *where = w.where;
+  });
+}

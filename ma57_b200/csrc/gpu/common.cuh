@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "checked.cuh"
+
 namespace symla_gpu {
 
 // One frontal matrix (supernode) as the kernels see it. All pointers are
@@ -75,11 +77,16 @@ __host__ __device__ inline bool tc_block_ok(int K, double lmax, double wmax, dou
   return K <= kTcKpad && lmax * wmax <= kTcGrowthGuard * amax;
 }
 
-// Error word of the pipelined solve kernels.
+// Error word of the pipelined solve kernels: a wait ran out; (checked build)
+// a row index or a child's workspace row was out of range.
 constexpr int kSolveErrTimeout = 1;
+constexpr int kSolveErrBounds = 8;
 // FactorGlobals::error: a panel's bulk staging of its rows did not complete
 // within the default wait limit.
 constexpr int kPanelErrTimeout = 3;
+// FactorGlobals::error: a bulk copy of the FP64 Schur update's staging ring
+// did not complete within the default wait limit.
+constexpr int kUpdateErrTimeout = 5;
 // Error bits of the tensor-core Schur update: a pipeline wait ran out (the
 // CTA abandoned its tile), and the drain after such an abandonment could not
 // confirm that the CTA's copies and tensor-core operations had finished before
@@ -135,6 +142,8 @@ struct KernelOpts {
   const int* a_j;               // A entry: local column
   const int* a_pos;             // A entry: rowPattern position
   const int* a_idx;             // A entry: index into values
+  long long nnz;                // number of A values
+  CheckWord* chk;               // status word of the bounds checks (checked build)
 };
 
 }  // namespace symla_gpu

@@ -33,6 +33,7 @@ struct LevelLists {
   int large_max_m = 0;
   int small_threads = 0;       // tile schedule (autotuner): small-front kernel width, 0 = by size
   int cluster_ctas = 0;        // panel cluster size, 0 = by size
+  int update_rows = 0;         // rows per Schur-update tile (64 or 128), 0 = 128
   int panels = 0;              // panel iterations needed
   int panel_width = 32;        // pivots per panel (narrower for fronts too tall for a full-width cluster panel)
   double* d_panel_cols = nullptr;  // single-CTA panel kernel, fronts too tall for shared memory: 2 m per front
@@ -164,6 +165,17 @@ struct symla_gpu_ctx {
 
   // dynamic (delayed-pivot) allocations for the current factorization
   std::vector<void*> dyn_allocs;
+  // front storage allocated by re-planning (pointer, doubles), for the
+  // checked build's storage check
+  std::vector<std::pair<double*, size_t>> dyn_front_blocks;
+
+  // bounds checks of the checked build: status word (allocated in every
+  // build, written only by the checked one) and the front allocations as
+  // (lo, hi) pairs on the device
+  symla_gpu::CheckWord* d_check = nullptr;
+  const double** d_ranges = nullptr;
+  size_t ranges_cap = 0;
+  std::vector<const double*> h_ranges;
 
   // bound of every device-side wait on another CTA (solve flags, tensor-core
   // mbarriers), global-timer ns; set by symla_gpu_set_wait_limit_ns

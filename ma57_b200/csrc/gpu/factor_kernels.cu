@@ -36,7 +36,8 @@ __device__ __forceinline__ bool level_aborted(const FactorGlobals* g, int level,
 // Child contribution to parent entry (i, j) (i >= j in the parent's local
 // order), summed over children in their fixed order.
 __device__ __forceinline__ double gather_children(const FrontDesc* fronts, const ChildLink* links,
-                                                  const FrontState* st, int ch_begin, int ch_end, int i, int j) {
+                                                  const FrontState* st, int ch_begin, int ch_end, int i, int j,
+                                                  CheckWord* chk) {
   double v = 0.0;
   for (int c = ch_begin; c < ch_end; ++c) {
     const ChildLink L = links[c];
@@ -47,13 +48,20 @@ __device__ __forceinline__ double gather_children(const FrontDesc* fronts, const
     const FrontDesc& cf = fronts[L.child];
     const int np = st[L.child].npiv;
     const int r = a > b ? a : b, cc = a > b ? b : a;
+    if (!check(np >= 0 && np + r < cf.m, chk, kChkGather, L.child)) continue;
     v += cf.F[static_cast<int64_t>(np + cc) * cf.ld + np + r];
   }
   return v;
 }
 
-__device__ __forceinline__ int a_local_row(int pos, int ncols, int nextra) {
-  return pos < ncols ? pos : pos + nextra;
+// A stored entry e of the front's own columns: (local column, local row,
+// value index), or false (checked build) when it lies outside the front.
+__device__ __forceinline__ bool a_entry(const KernelOpts& o, const FrontDesc& f, int e, int& j, int& i, int& idx) {
+  j = o.a_j[e];
+  const int pos = o.a_pos[e];
+  idx = o.a_idx[e];
+  i = pos < f.ncols ? pos : pos + f.nextra;
+  return check(a_entry_ok(j, pos, idx, f.ncols, f.nextra, f.m, o.nnz), o.chk, kChkAEntry, e);
 }
 
 }  // namespace
@@ -82,6 +90,7 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(const FrontDesc* __res
   __shared__ const double* s_cb[kAsmMaxChildren];
   __shared__ int64_t s_ld[kAsmMaxChildren];
   __shared__ int s_b[kAsmMaxChildren][32];
+  __shared__ int s_lim[kAsmMaxChildren];  // checked build: contribution-block rows of each child
   const int4 task = reinterpret_cast<const int4*>(tasks)[blockIdx.x];
   const int s = task.x, j0 = task.y, i0 = task.z;  // i0 >= j0
   const FrontDesc f = fronts[s];
@@ -97,6 +106,8 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(const FrontDesc* __res
       s_inv[threadIdx.x] = L.invmap;
       s_cb[threadIdx.x] = cf.F + static_cast<int64_t>(np) * cf.ld + np;  // contribution block origin
       s_ld[threadIdx.x] = cf.ld;
+      if constexpr (kCheckedBuild)
+        s_lim[threadIdx.x] = check(np >= 0 && np <= cf.m, o.chk, kChkPivots, L.child) ? cf.m - np : 0;
     }
     __syncthreads();
     for (int t = threadIdx.x; t < nch * 32; t += blockDim.x) {
@@ -123,7 +134,7 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(const FrontDesc* __res
           const int b = s_b[c][h0 + jj];
           if (b >= 0 && j0 + h0 + jj <= i) {
             const int r = a > b ? a : b, cc = a > b ? b : a;
-            acc[jj] += cb[static_cast<int64_t>(cc) * cld + r];
+            if (check(r < s_lim[c], o.chk, kChkGather, s)) acc[jj] += cb[static_cast<int64_t>(cc) * cld + r];
           }
         }
       }
@@ -135,7 +146,7 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(const FrontDesc* __res
     for (int j = j0; j < j1; ++j) {
       double* col = f.F + static_cast<int64_t>(j) * f.ld;
       for (int i = max(j, i0) + threadIdx.x; i < iend; i += blockDim.x)
-        col[i] = gather_children(fronts, links, st, f.ch_begin, f.ch_end, i, j);
+        col[i] = gather_children(fronts, links, st, f.ch_begin, f.ch_end, i, j, o.chk);
     }
   }
   __syncthreads();
@@ -143,9 +154,8 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(const FrontDesc* __res
     const int jend = min(j1, f.ncols);
     const int e0 = a_colptr[f.a_begin + j0], e1 = a_colptr[f.a_begin + jend];
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-      const int j = o.a_j[e];
-      const int i = a_local_row(o.a_pos[e], f.ncols, f.nextra);
-      if (i >= i0 && i < iend) f.F[static_cast<int64_t>(j) * f.ld + i] += o.values[o.a_idx[e]];
+      int j, i, idx;
+      if (a_entry(o, f, e, j, i, idx) && i >= i0 && i < iend) f.F[static_cast<int64_t>(j) * f.ld + i] += o.values[idx];
     }
   }
   // max |entry| of the assembled front (dense_kernel.hpp:413), folded here
@@ -174,6 +184,37 @@ struct SmallFront {
   // symmetric read from lower storage
   __device__ double sym(int i, int j) { return i >= j ? S[j * lds + i] : S[i * lds + j]; }
 };
+
+// Calls fn(i, j) once for every entry i >= j of a t x t lower triangle,
+// spread over the CTA's NT threads. The triangle is folded into a
+// (t + 1) x ceil(t / 2) rectangle: rectangle column c holds triangle column
+// c (rows c..t-1) in its rows c..t-1 and triangle column t-1-c in the rest
+// (rows 0..c-1 -> triangle rows t-c..t-1, row t -> the diagonal), the middle
+// column of an odd t only once. Consecutive threads take consecutive
+// rectangle rows (consecutive rows of one column: no shared-memory bank
+// conflicts), and each thread's position advances by a precomputed step, so
+// there is one integer division per call instead of one per entry, and no
+// thread idles on the upper half.
+template <int NT, class Fn>
+__device__ __forceinline__ void for_lower(int t, Fn&& fn) {
+  const int R = t + 1, C = (t + 1) >> 1;
+  int q = threadIdx.x % R, c = threadIdx.x / R;  // position c R + q, advancing by NT
+  const int dq = NT % R, dc = NT / R;
+  while (c < C) {
+    if (q >= c && q < t) {
+      fn(q, c);
+    } else {
+      const int c2 = t - 1 - c;
+      if (c2 != c) fn(q == t ? c2 : c2 + 1 + q, c2);
+    }
+    q += dq;
+    c += dc;
+    if (q >= R) {
+      q -= R;
+      ++c;
+    }
+  }
+}
 
 // Symmetric swap of positions i < j in lower storage over the whole front.
 template <int NT>
@@ -234,11 +275,9 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
   int* lp = fi + m;  // local pivot permutation
 
   // ---- assembly (multifrontal.hpp:498-535), children summed in fixed order
-  for (int t = threadIdx.x; t < m * m; t += NT) {
-    const int i = t % m, j = t / m;
-    if (i < j) continue;
-    F.at(i, j) = gather_children(fronts, links, st, f.ch_begin, f.ch_end, i, j);
-  }
+  for_lower<NT>(m, [&](int i, int j) {
+    F.at(i, j) = gather_children(fronts, links, st, f.ch_begin, f.ch_end, i, j, o.chk);
+  });
   for (int t = threadIdx.x; t < m; t += NT) {
     fi[t] = f.fidx[t];
     lp[t] = t;
@@ -247,19 +286,15 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
   {
     const int e0 = a_colptr[f.a_begin], e1 = a_colptr[f.a_begin + f.ncols];
     for (int e = e0 + threadIdx.x; e < e1; e += NT) {
-      const int j = o.a_j[e];
-      const int i = a_local_row(o.a_pos[e], f.ncols, f.nextra);
-      F.at(i, j) += o.values[o.a_idx[e]];
+      int j, i, idx;
+      if (a_entry(o, f, e, j, i, idx)) F.at(i, j) += o.values[idx];
     }
   }
   __syncthreads();
 
   // ---- orig_max over the whole front (dense_kernel.hpp:413, :934)
   double tmax = 0.0;
-  for (int t = threadIdx.x; t < m * m; t += NT) {
-    const int i = t % m, j = t / m;
-    if (i >= j) tmax = fmax(tmax, fabs(F.at(i, j)));
-  }
+  for_lower<NT>(m, [&](int i, int j) { tmax = fmax(tmax, fabs(F.at(i, j))); });
   double orig_max = block_max<NT>(tmax, red_v);
   const bool isStatic = (o.mode == 1);
   if (isStatic) {
@@ -314,15 +349,12 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
         F.at(i, k) = a / d;
       }
       __syncthreads();
-      const int mt = m - k - 1;
-      for (int t = threadIdx.x; t < mt * mt; t += NT) {
-        const int ii = t % mt, jj = t / mt;
-        if (ii < jj) continue;
+      for_lower<NT>(m - k - 1, [&](int ii, int jj) {
         const int i = k + 1 + ii, j = k + 1 + jj;
         const double v = F.at(i, j) - (F.at(i, k) * d) * F.at(j, k);
         F.at(i, j) = v;
         thread_rmax = fmax(thread_rmax, fabs(v));
-      }
+      });
       __syncthreads();
     }
     for (int t = threadIdx.x; t < effEnd; t += NT) {
@@ -383,15 +415,12 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
           f.pk[k] = 0;
         }
         __syncthreads();
-        const int mt = m - k - 1;
-        for (int t = threadIdx.x; t < mt * mt; t += NT) {
-          const int ii = t % mt, jj = t / mt;
-          if (ii < jj) continue;
+        for_lower<NT>(m - k - 1, [&](int ii, int jj) {
           const int i = k + 1 + ii, j = k + 1 + jj;
           const double v = F.at(i, j) - (F.at(i, k) * d) * F.at(j, k);
           F.at(i, j) = v;
           thread_rmax = fmax(thread_rmax, fabs(v));
-        }
+        });
         __syncthreads();
         k += 1;
         continue;
@@ -434,10 +463,7 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
         f.pk[k + 1] = 2;
       }
       __syncthreads();
-      const int mt = m - k - 2;
-      for (int t = threadIdx.x; t < mt * mt; t += NT) {
-        const int ii = t % mt, jj = t / mt;
-        if (ii < jj) continue;
+      for_lower<NT>(m - k - 2, [&](int ii, int jj) {
         const int i = k + 2 + ii, j = k + 2 + jj;
         const double l0i = F.at(i, k), l1i = F.at(i, k + 1);
         const double w0 = l0i * d11 + l1i * d21;
@@ -445,7 +471,7 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
         const double v = F.at(i, j) - (w0 * F.at(j, k) + w1 * F.at(j, k + 1));
         F.at(i, j) = v;
         thread_rmax = fmax(thread_rmax, fabs(v));
-      }
+      });
       __syncthreads();
       k += 2;
     }
@@ -453,10 +479,7 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
 
   // ---- write back (lower triangle of the whole front, permuted indices)
   __syncthreads();
-  for (int t = threadIdx.x; t < m * m; t += NT) {
-    const int i = t % m, j = t / m;
-    if (i >= j) f.F[static_cast<int64_t>(j) * f.ld + i] = F.at(i, j);
-  }
+  for_lower<NT>(m, [&](int i, int j) { f.F[static_cast<int64_t>(j) * f.ld + i] = F.at(i, j); });
   for (int t = threadIdx.x; t < m; t += NT) {
     f.fidx[t] = fi[t];
     f.lperm[t] = lp[t];
@@ -857,7 +880,6 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* _
 // C(i, j) -= sum_q L(i, q) (L D)(j, q) for i >= j, over the tiles of every
 // front of the level (one tile space).
 namespace {
-constexpr int kTT = 128;        // tile height (rows)
 constexpr int kMaxUpdateFronts = 1024;  // fronts per update launch
 }  // namespace
 
@@ -878,47 +900,46 @@ __device__ __forceinline__ bool update_range(const FrontState& S, int m, bool fa
   return q1 > q0 && c1 > c0;
 }
 
-__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc, bool valid) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
-  const int n = valid ? 8 : 0;  // zero-fill rows beyond the front
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(n) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
 // Tiles of front s's update region: column tiles of width tj over [c0, c1),
-// each with kTT-row tiles from its diagonal down to m.
-__device__ __forceinline__ int update_tiles(int m, int c0, int c1, int tj) {
+// each with tm-row tiles from its diagonal down to m.
+__device__ __forceinline__ int update_tiles(int m, int c0, int c1, int tj, int tm) {
   int n = 0;
-  for (int j = c0; j < c1; j += tj) n += (m - j + kTT - 1) / kTT;
+  for (int j = c0; j < c1; j += tj) n += (m - j + tm - 1) / tm;
   return n;
 }
 
 // ---------------------------------------------------------------------------
 // The near / far updates on the FP64 tensor path: mma.sync m16n8k8 .f64
-// (DMMA; the 5th-gen tcgen05 MMA has no FP64 kind). 128 x 64 tiles, 8 warps
-// of 32 x 32 (2 x 4 MMA tiles, 4 accumulators each per lane), two CTAs per
-// SM, so that one CTA's C load and store overlap the other's MMAs. A chunk
-// of 16 pivots of the A rows (L(i, q)) and of the B rows (L(j, q) with one
-// halo column each side, for D's 2 x 2 blocks) is staged pivot-major as in
-// the front (coalesced, conflict-free cp.async) with strides of 132 and 68
-// doubles, which also make the fragment loads conflict-free (lanes 0-15 of
-// a 64-bit load hit 16 distinct bank pairs); a ring of three stages keeps
-// two chunks in flight.
-// W(j, q) = -(L D)(j, q) is formed once per chunk in shared memory and the L
-// fragment accumulates onto the C tile held in registers.
+// (DMMA; the 5th-gen tcgen05 MMA has no FP64 kind). TM x 64 tiles: TM = 128,
+// 8 warps of 32 x 32 (2 x 4 MMA tiles, 4 accumulators each per lane), or
+// TM = 64 for small fronts, 8 warps of 32 x 16 (the autotuner picks per
+// level); two CTAs per SM, so that one CTA's C load and store overlap the
+// other's MMAs.
+//
+// A chunk of 16 pivots of the A rows (L(i, q)) and of the B rows (L(j, q),
+// with the 2 x 2 partner columns either side) is staged pivot-major, as the
+// front stores it, by bulk copies (cp.async.bulk, one per pivot column, no
+// multicast) that one thread issues and an mbarrier per stage counts, in a
+// ring of three stages (two chunks in flight). A column's copy starts at the
+// even row at or before the tile's first row (16-byte alignment; fronts have
+// an even leading dimension) and the tile is read at that parity offset.
+// W(j, q) = -(L D)(j, q) is formed once per chunk in shared memory (double
+// buffered, D read from global) and the L fragment accumulates onto the C
+// tile held in registers: one block barrier per chunk.
 namespace {
 constexpr int kTJ = 64;   // column tile width
 constexpr int kKM = 16;   // K chunk
-constexpr int kAS = 132;  // pivot-major stride of the staged A rows (doubles)
 constexpr int kBS = 68;   // pivot-major stride of the staged B rows and W
-constexpr int kMThreads = 256;  // 8 warps of 32 x 32
+constexpr int kMThreads = 256;  // 8 warps
 constexpr int kMStages = 3;  // staging ring depth (two chunks in flight)
-constexpr size_t kMmaSmem =
-    static_cast<size_t>(kMStages * (kKM * kAS + (kKM + 2) * kBS) + kKM * kBS) * sizeof(double);
+// pivot-major stride of the staged A rows (doubles): TM + 4 keeps the
+// fragment loads conflict-free and holds the parity offset
+template <int TM>
+constexpr int kAS = TM + 4;
+template <int TM>
+constexpr size_t mma_smem() {
+  return static_cast<size_t>(kMStages * (kKM * kAS<TM> + (kKM + 2) * kBS) + 2 * kKM * kBS) * sizeof(double);
+}
 
 // c (16 x 8) += a (16 x 8) * b (8 x 8); lane (g, t) = (lane >> 2, lane & 3):
 // a_r = A(g + 8 (r & 1), t + 4 (r >> 1)), b_r = B(t + 4 r, g),
@@ -929,40 +950,91 @@ __device__ __forceinline__ void dmma16x8x8(double* c, const double* a, const dou
                : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-// A rows i (pivots kc .. kc + kn) and B rows j (pivots kc - 1 .. kc + kn,
-// valid inside [q0, q1)) into pivot-major tiles, zero-filled outside.
-__device__ __forceinline__ void mma_stage(const double* F, int64_t ld, int m, int q0, int q1, int kc, int kn, int i0,
-                                          int j0, double* As, double* Bs) {
-  for (int t = threadIdx.x; t < kKM * kTT; t += kMThreads) {
-    const int k = t / kTT, r = t % kTT;
-    const int gi = i0 + r;
-    const bool ok = k < kn && gi < m;
-    cp_async8(As + k * kAS + r, F + (ok ? (kc + k) * ld + gi : 0), ok);
+__device__ __forceinline__ uint32_t u_smem(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+// Bounded wait for the mbarrier phase `parity`: at most kDefaultWaitNs / 8
+// probes (each a few ns or more, so at least about a second); false when
+// they run out.
+__device__ __forceinline__ bool u_mbar_wait(uint64_t* bar, uint32_t parity) {
+  constexpr uint32_t kMaxProbes = static_cast<uint32_t>(kDefaultWaitNs / 8);
+  for (uint32_t it = 0; it < kMaxProbes; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(u_smem(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
   }
-  for (int t = threadIdx.x; t < (kKM + 2) * kTJ; t += kMThreads) {
-    const int kp = t / kTJ, r = t % kTJ;
-    const int pq = kc + kp - 1;
-    const int gj = j0 + r;
-    const bool ok = gj < m && pq >= q0 && pq < q1 && kp <= kn + 1;  // halo: 2 x 2 partners either side
-    cp_async8(Bs + kp * kBS + r, F + (ok ? pq * ld + gj : 0), ok);
+  return false;
+}
+
+// One bulk copy (no multicast) of `bytes` (a multiple of 16; both addresses
+// 16-byte aligned) into this CTA's shared memory, counted on `bar`.
+__device__ __forceinline__ void u_copy(double* dst, const double* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(u_smem(dst)),
+      "l"(src), "r"(bytes), "r"(u_smem(bar))
+      : "memory");
+}
+
+// Row ranges of the tile being staged (thread 0 sets them at the tile's
+// start; only warp 0 reads them): A rows [ra, ra + na) and B rows
+// [rb, rb + nb), both starting on an even row, with na, nb even.
+struct UpdateCopyRows {
+  int ra, na, rb, nb;
+};
+
+// Issue the copies of chunk kc (kn pivots) into one ring stage: A columns
+// kc .. kc + kn, B columns kc - 1 .. kc + kn (those inside [q0, q1)), rows
+// as in cr. Warp 0: lane 0 registers the bytes on the stage's mbarrier, then
+// every lane issues one or two of the (at most 34) column copies.
+template <int TM>
+__device__ __forceinline__ void u_issue(const double* F, int64_t ld, int q0, int q1, int kc, int kn,
+                                        const UpdateCopyRows& cr, double* As, double* Bs, uint64_t* bar, int lane) {
+  const int qa = max(kc - 1, q0), qb = min(kc + kn + 1, q1);
+  const uint32_t per_a = static_cast<uint32_t>(cr.na) * sizeof(double);
+  const uint32_t per_b = static_cast<uint32_t>(cr.nb) * sizeof(double);
+  if (lane == 0) {
+    const uint32_t total = per_a * kn + per_b * (qb - qa);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(u_smem(bar)), "r"(total) : "memory");
+  }
+  __syncwarp();
+  for (int t = lane; t < kn + (qb - qa); t += 32) {
+    if (t < kn)
+      u_copy(As + t * kAS<TM>, F + (kc + t) * ld + cr.ra, per_a, bar);
+    else
+      u_copy(Bs + (qa + t - kn - kc + 1) * kBS, F + (qa + t - kn) * ld + cr.rb, per_b, bar);
   }
 }
 }  // namespace
 
-template <int MODE>
+template <int MODE, int TM>
 __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
                                                                const int* __restrict__ front_list, int count,
                                                                FactorGlobals* g, int level, int dynamic,
                                                                const double* __restrict__ tc_guard) {
   if (level_aborted(g, level, dynamic)) return;
-  extern __shared__ double usm[];
-  // stage b of the ring: A rows at As_of(b), B rows at Bs_of(b)
-  auto As_of = [&](int b) { return usm + b * kKM * kAS; };
-  auto Bs_of = [&](int b) { return usm + kMStages * kKM * kAS + b * (kKM + 2) * kBS; };
-  double* Ws = usm + kMStages * (kKM * kAS + (kKM + 2) * kBS);
-  __shared__ double dd[kKM], dlo[kKM], dhi[kKM];
-  __shared__ int8_t kk[kKM];
+  constexpr int AS = kAS<TM>;
+  constexpr int WROWS = TM / 32;       // warps along the tile's rows
+  constexpr int WCOLS = 8 / WROWS;     // warps along its 64 columns
+  constexpr int WN = kTJ / WCOLS;      // columns per warp (32 or 16)
+  constexpr int CT = WN / 8;           // 8-column MMA tiles per warp
+  extern __shared__ __align__(16) double usm[];
+  // stage b of the ring: A rows at As_of(b), B rows at Bs_of(b); W double buffered
+  auto As_of = [&](int b) { return usm + b * kKM * AS; };
+  auto Bs_of = [&](int b) { return usm + kMStages * kKM * AS + b * (kKM + 2) * kBS; };
+  auto Ws_of = [&](int b) { return usm + kMStages * (kKM * AS + (kKM + 2) * kBS) + b * kKM * kBS; };
+  __shared__ __align__(8) uint64_t full[kMStages];
+  __shared__ UpdateCopyRows copy_rows;
   __shared__ int tile_end[2 * kMaxUpdateFronts];
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < kMStages; ++b)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(u_smem(&full[b])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
   const int nent = (MODE == 2) ? 2 * count : count;
   auto entry_far = [&](int e) { return MODE == 1 || (MODE == 2 && e >= count); };
   for (int t = threadIdx.x; t < nent; t += kMThreads) {
@@ -973,7 +1045,7 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
     bool use = update_range(S, fronts[sf].m, far, c0, c1, q0, q1);
     if (far && use && tc_guard && tc_block_ok(q1 - q0, tc_guard[2 * t], tc_guard[2 * t + 1], g->amax))
       use = false;  // the tensor-core kernel applied this block
-    tile_end[t] = use ? update_tiles(fronts[sf].m, c0, c1, kTJ) : 0;
+    tile_end[t] = use ? update_tiles(fronts[sf].m, c0, c1, kTJ, TM) : 0;
     if (blockIdx.x == 0 && tile_end[t] > 0) {
       const double nc = c1 - c0, mm = fronts[sf].m;
       const double entries = nc * mm - (static_cast<double>(c0) + c1 - 1) * nc / 2.0;
@@ -986,13 +1058,14 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
   __syncthreads();
   const int total = nent > 0 ? tile_end[nent - 1] : 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wr = warp >> 1, wc = warp & 1;          // warp's 32 x 32 sub-tile
+  const int wr = warp / WCOLS, wc = warp % WCOLS;   // warp's 32 x WN sub-tile
   const int lg = lane >> 2, lt = lane & 3;          // fragment coordinates
   double tmax = 0.0;
   int cur = -1, s = -1;
-  double* Fp = nullptr;
+  const double* Fp = nullptr;
   int m = 0, c0 = 0, c1 = 0, q0 = 0, q1 = 0, nchunks = 0;
   int64_t ld = 0;
+  unsigned u = 0;  // chunks consumed by this CTA so far (ring stage u % 3, phase (u / 3) & 1)
   for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
     int fi = 0;
     while (tile >= tile_end[fi]) ++fi;
@@ -1013,23 +1086,37 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
     int rem = tile - (fi > 0 ? tile_end[fi - 1] : 0);
     int tj = 0;
     for (;;) {
-      const int nr = (m - (c0 + tj * kTJ) + kTT - 1) / kTT;
+      const int nr = (m - (c0 + tj * kTJ) + TM - 1) / TM;
       if (rem < nr) break;
       rem -= nr;
       ++tj;
     }
-    const int j0 = c0 + tj * kTJ, i0 = j0 + rem * kTT;
-    __syncthreads();  // previous tile done with the buffers
-    mma_stage(Fp, ld, m, q0, q1, q0, min(kKM, q1 - q0), i0, j0, As_of(0), Bs_of(0));
-    cp_async_commit();
-    if (nchunks > 1) mma_stage(Fp, ld, m, q0, q1, q0 + kKM, min(kKM, q1 - q0 - kKM), i0, j0, As_of(1), Bs_of(1));
-    cp_async_commit();
+    const int j0 = c0 + tj * kTJ, i0 = j0 + rem * TM;
+    const int sa = i0 & 1, sb = j0 & 1;  // parity offsets of the staged rows
+    __syncthreads();  // previous tile done with every stage
+    if (warp == 0) {
+      // rows from the even row at or before the tile's first row, rounded up
+      // to whole 16-byte pairs (the extra row of an odd m is the padding row
+      // of the front's even leading dimension)
+      if (lane == 0) {
+        copy_rows.ra = i0 & ~1;
+        copy_rows.na = ((min(i0 + TM, m) + 1) & ~1) - copy_rows.ra;
+        copy_rows.rb = j0 & ~1;
+        copy_rows.nb = ((min(j0 + kTJ, m) + 1) & ~1) - copy_rows.rb;
+      }
+      __syncwarp();
+      for (int c = 0; c < 2 && c < nchunks; ++c) {
+        const int kc = q0 + c * kKM;
+        const unsigned b = (u + c) % kMStages;
+        u_issue<TM>(Fp, ld, q0, q1, kc, min(kKM, q1 - kc), copy_rows, As_of(b), Bs_of(b), &full[b], lane);
+      }
+    }
     // C tile into the accumulators (lane holds rows gi0 + 16 rt + 8 v,
     // columns gj0 + 8 ct + h as acc[rt][ct][2 v + h])
-    const int gi0 = i0 + wr * 32 + lg, gj0 = j0 + wc * 32 + 2 * lt;
-    double acc[2][4][4];
+    const int gi0 = i0 + wr * 32 + lg, gj0 = j0 + wc * WN + 2 * lt;
+    double acc[2][CT][4];
 #pragma unroll
-    for (int ct = 0; ct < 4; ++ct)
+    for (int ct = 0; ct < CT; ++ct)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int gj = gj0 + ct * 8 + h;
@@ -1042,65 +1129,69 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
             acc[rt][ct][2 * v + h] = (gj < c1 && gi < m && gi >= gj) ? colp[gi] : 0.0;
           }
       }
-    for (int c = 0; c < nchunks; ++c) {
+    for (int c = 0; c < nchunks; ++c, ++u) {
       const int kc = q0 + c * kKM, kn = min(kKM, q1 - kc);
-      if (c + 2 < nchunks) {
-        const int kc2 = kc + 2 * kKM;
-        mma_stage(Fp, ld, m, q0, q1, kc2, min(kKM, q1 - kc2), i0, j0, As_of((c + 2) % kMStages),
-                  Bs_of((c + 2) % kMStages));
+      const unsigned b = u % kMStages;
+      if (!u_mbar_wait(&full[b], (u / kMStages) & 1)) {
+        // a copy did not land within the wait limit: record it (the
+        // factorization then fails with a timeout) and wait once more,
+        // bounded, for this stage's copies before going on
+        atomicCAS(&g->error, 0, kUpdateErrTimeout);
+        u_mbar_wait(&full[b], (u / kMStages) & 1);
       }
-      cp_async_commit();  // (possibly empty) group c + 2
-      if (threadIdx.x < kn) {
-        const int pq = kc + threadIdx.x;
-        const FrontDesc& fd = fronts[s];
-        const int8_t kind = fd.pk[pq];
-        kk[threadIdx.x] = kind;
-        dd[threadIdx.x] = fd.Dd[pq];
-        dlo[threadIdx.x] = (kind == 2) ? fd.Do[pq - 1] : 0.0;
-        dhi[threadIdx.x] = (kind == 1) ? fd.Do[pq] : 0.0;
-      }
-      cp_async_wait<2>();  // chunk c landed; c + 1 and c + 2 may be in flight
-      __syncthreads();
-      const double* As = As_of(c % kMStages);
-      const double* Bs = Bs_of(c % kMStages);
-      // W(j, q) = -(L D)(j, q); zero past the chunk (the MMAs run over
-      // 8-pivot steps; A is zero-filled past kn)
+      double* As = As_of(b);
+      const double* Bs = Bs_of(b) + sb;
+      double* Ws = Ws_of(c & 1);
+      // the MMAs run over 8-pivot steps: A columns past kn are zeroed (the
+      // stage's copies did not write them), W rows past kn are zero
       const int kn8 = (kn + 7) & ~7;
-      for (int t = threadIdx.x; t < kn8 * kTJ; t += kMThreads) {
-        const int q = t / kTJ, r = t % kTJ;
-        double w = 0.0;
-        if (q < kn) {
-          const double* col = Bs + (q + 1) * kBS + r;
-          w = dd[q] * col[0];
-          if (kk[q] == 1) w += dhi[q] * col[kBS];
-          if (kk[q] == 2) w += dlo[q] * col[-kBS];
+      for (int t = threadIdx.x; t < (kn8 - kn) * AS; t += kMThreads) As[kn * AS + t] = 0.0;
+      // W(j, q) = -(L D)(j, q)
+      {
+        const FrontDesc& fd = fronts[s];
+        for (int t = threadIdx.x; t < kn8 * kTJ; t += kMThreads) {
+          const int q = t / kTJ, r = t % kTJ;
+          double w = 0.0;
+          if (q < kn) {
+            const int pq = kc + q;
+            const double* col = Bs + (q + 1) * kBS + r;
+            const int8_t kind = fd.pk[pq];
+            w = fd.Dd[pq] * col[0];
+            if (kind == 1) w += fd.Do[pq] * col[kBS];
+            if (kind == 2) w += fd.Do[pq - 1] * col[-kBS];
+          }
+          Ws[q * kBS + r] = -w;
         }
-        Ws[q * kBS + r] = -w;
       }
-      __syncthreads();
+      __syncthreads();  // W and the zeroed columns ready; every thread is past chunk c - 1
+      if (warp == 0 && c + 2 < nchunks) {
+        const int kc2 = kc + 2 * kKM;
+        const unsigned b2 = (u + 2) % kMStages;
+        u_issue<TM>(Fp, ld, q0, q1, kc2, min(kKM, q1 - kc2), copy_rows, As_of(b2), Bs_of(b2), &full[b2], lane);
+      }
+      const double* Aq = As + sa;
       for (int k0 = 0; k0 < kn8; k0 += 8) {
-        double b[4][2];
+        double bq[CT][2];
 #pragma unroll
-        for (int ct = 0; ct < 4; ++ct)
+        for (int ct = 0; ct < CT; ++ct)
 #pragma unroll
-          for (int r = 0; r < 2; ++r) b[ct][r] = Ws[(k0 + lt + 4 * r) * kBS + wc * 32 + ct * 8 + lg];
+          for (int r = 0; r < 2; ++r) bq[ct][r] = Ws[(k0 + lt + 4 * r) * kBS + wc * WN + ct * 8 + lg];
 #pragma unroll
         for (int rt = 0; rt < 2; ++rt) {
           double a[4];
 #pragma unroll
-          for (int r = 0; r < 4; ++r) a[r] = As[(k0 + lt + 4 * (r >> 1)) * kAS + wr * 32 + rt * 16 + lg + 8 * (r & 1)];
+          for (int r = 0; r < 4; ++r) a[r] = Aq[(k0 + lt + 4 * (r >> 1)) * AS + wr * 32 + rt * 16 + lg + 8 * (r & 1)];
 #pragma unroll
-          for (int ct = 0; ct < 4; ++ct) dmma16x8x8(acc[rt][ct], a, b[ct]);
+          for (int ct = 0; ct < CT; ++ct) dmma16x8x8(acc[rt][ct], a, bq[ct]);
         }
       }
-      __syncthreads();
     }
 #pragma unroll
-    for (int ct = 0; ct < 4; ++ct)
+    for (int ct = 0; ct < CT; ++ct)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int gj = gj0 + ct * 8 + h;
-        double* colp = Fp + static_cast<int64_t>(gj < c1 ? gj : 0) * ld;
+        double* colp = const_cast<double*>(Fp) + static_cast<int64_t>(gj < c1 ? gj : 0) * ld;
 #pragma unroll
         for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
@@ -1193,31 +1284,106 @@ void launch_mark_unfinished(const FrontState* st, const int* list, int count, Fa
   mark_unfinished_kernel<<<1, 256, 0, stream>>>(st, list, count, g, level);
 }
 
-void launch_update(bool far, const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
-                   FactorGlobals* g, int level, int dynamic, cudaStream_t stream, const double* tc_guard) {
-  if (count <= 0 || grid_x <= 0) return;
-  const size_t sm = kMmaSmem;
-  grid_x = std::min(2 * grid_x, 2 * 148);  // two 128 x 64 tiles per 128 x 128, two CTAs per SM
+namespace {
+template <int MODE, int TM>
+void launch_update_t(const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
+                     FactorGlobals* g, int level, int dynamic, cudaStream_t stream, const double* tc_guard) {
   for (int b = 0; b < count; b += kMaxUpdateFronts) {
     const int cnt = count - b < kMaxUpdateFronts ? count - b : kMaxUpdateFronts;
+    update_mma_kernel<MODE, TM><<<grid_x, kMThreads, mma_smem<TM>(), stream>>>(
+        fronts, st, list + b, cnt, g, level, dynamic, (MODE == 1 && tc_guard) ? tc_guard + 2 * b : nullptr);
+  }
+}
+}  // namespace
+
+void launch_update(bool far, const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
+                   FactorGlobals* g, int level, int dynamic, cudaStream_t stream, const double* tc_guard,
+                   int tile_rows) {
+  if (count <= 0 || grid_x <= 0) return;
+  grid_x = std::min(2 * grid_x, 2 * 148);  // two tiles per 128 x 128, two CTAs per SM
+  if (tile_rows == 64) {
     if (far)
-      update_mma_kernel<1><<<grid_x, kMThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic,
-                                                              tc_guard ? tc_guard + 2 * b : nullptr);
+      launch_update_t<1, 64>(fronts, st, list, count, grid_x, g, level, dynamic, stream, tc_guard);
     else
-      update_mma_kernel<0><<<grid_x, kMThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic,
-                                                              nullptr);
+      launch_update_t<0, 64>(fronts, st, list, count, grid_x, g, level, dynamic, stream, nullptr);
+  } else {
+    if (far)
+      launch_update_t<1, 128>(fronts, st, list, count, grid_x, g, level, dynamic, stream, tc_guard);
+    else
+      launch_update_t<0, 128>(fronts, st, list, count, grid_x, g, level, dynamic, stream, nullptr);
   }
 }
 
 void launch_update_both(const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
-                        FactorGlobals* g, int level, int dynamic, cudaStream_t stream) {
+                        FactorGlobals* g, int level, int dynamic, cudaStream_t stream, int tile_rows) {
   if (count <= 0 || grid_x <= 0) return;
-  const size_t sm = kMmaSmem;
-  grid_x = std::min(2 * grid_x, 2 * 148);  // two 128 x 64 tiles per 128 x 128, two CTAs per SM
-  for (int b = 0; b < count; b += kMaxUpdateFronts) {
-    const int cnt = count - b < kMaxUpdateFronts ? count - b : kMaxUpdateFronts;
-    update_mma_kernel<2><<<grid_x, kMThreads, sm, stream>>>(fronts, st, list + b, cnt, g, level, dynamic, nullptr);
+  grid_x = std::min(2 * grid_x, 2 * 148);  // two tiles per 128 x 128, two CTAs per SM
+  if (tile_rows == 64)
+    launch_update_t<2, 64>(fronts, st, list, count, grid_x, g, level, dynamic, stream, nullptr);
+  else
+    launch_update_t<2, 128>(fronts, st, list, count, grid_x, g, level, dynamic, stream, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// Table validation of the checked build: one CTA per front of the list (or
+// of all fronts). Phase 0 (before the level launches): descriptor shape,
+// storage inside one of the front allocations, row indices, child links and
+// their maps, the front's A entries. Phase 1 (after the factorization): the
+// pivot counts and the (now permuted) row indices. Phase 2 (before a solve):
+// the row indices and the solve workspace slice. Reads the tables only.
+__global__ void validate_fronts_kernel(const FrontDesc* __restrict__ fronts, const ChildLink* __restrict__ links,
+                                       const FrontState* __restrict__ st, const int* __restrict__ list,
+                                       int num_fronts, int n, const int* __restrict__ a_colptr, KernelOpts o,
+                                       const double* const* __restrict__ ranges, int nranges, const double* wlo,
+                                       const double* whi, int wcols, int phase) {
+  __shared__ int s_ok;
+  const int s = list ? list[blockIdx.x] : static_cast<int>(blockIdx.x);
+  CheckWord* chk = o.chk;
+  if (threadIdx.x == 0) {
+    bool ok = check(in_range(s, 0, num_fronts), chk, kChkFrontShape, s);
+    if (ok) {
+      const FrontDesc f = fronts[s];
+      ok = check(front_shape_ok(f.m, f.ld, f.ncols, f.nelig, f.nextra), chk, kChkFrontShape, s);
+      if (ok) {
+        bool inside = false;
+        for (int r = 0; r < nranges && !inside; ++r) inside = storage_ok(f.F, f.m, f.ld, ranges[2 * r], ranges[2 * r + 1]);
+        ok = check(inside, chk, kChkFrontStorage, s);
+      }
+      if (ok && phase == 0)
+        ok = check(in_range(f.a_begin, 0, n + 1) && f.a_begin + f.ncols <= n && f.ch_begin <= f.ch_end, chk,
+                   kChkFrontShape, s);
+      if (ok && phase == 1) ok = check(in_range(st[s].npiv, 0, f.nelig + 1), chk, kChkPivots, s);
+      if (ok && phase == 2)
+        ok = check(f.wld >= f.m && storage_ok(f.W, wcols, f.wld, wlo, whi), chk, kChkWorkspace, s);
+    }
+    s_ok = ok;
   }
+  __syncthreads();
+  if (!s_ok) return;
+  const FrontDesc f = fronts[s];
+  for (int i = threadIdx.x; i < f.m; i += blockDim.x) check(in_range(f.fidx[i], 0, n), chk, kChkRowIndex, s);
+  if (phase != 0) return;
+  for (int c = f.ch_begin; c < f.ch_end; ++c) {
+    const ChildLink L = links[c];
+    if (!check(in_range(L.child, 0, num_fronts) && L.child != s, chk, kChkChildLink, s)) continue;
+    if (!check(L.cb >= 0 && L.cb <= fronts[L.child].m, chk, kChkChildLink, L.child)) continue;
+    for (int i = threadIdx.x; i < f.m; i += blockDim.x) check(in_range(L.invmap[i], -1, L.cb), chk, kChkInvMap, s);
+    for (int i = threadIdx.x; i < L.cb; i += blockDim.x) check(in_range(L.relmap[i], 0, f.m), chk, kChkRelMap, s);
+  }
+  const int e0 = a_colptr[f.a_begin], e1 = a_colptr[f.a_begin + f.ncols];
+  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    int j, i, idx;
+    a_entry(o, f, e, j, i, idx);
+  }
+}
+
+void launch_validate_fronts(const FrontDesc* fronts, const ChildLink* links, const FrontState* st, const int* list,
+                            int count, int num_fronts, int n, const int* a_colptr, const KernelOpts& o,
+                            const double* const* ranges, int nranges, const double* wlo, const double* whi,
+                            int wcols, int phase, cudaStream_t stream) {
+  if (count <= 0) return;
+  validate_fronts_kernel<<<count, 256, 0, stream>>>(fronts, links, st, list, num_fronts, n, a_colptr, o, ranges,
+                                                     nranges, wlo, whi, wcols, phase);
 }
 
 cudaError_t configure_factor_kernels() {
@@ -1228,8 +1394,12 @@ cudaError_t configure_factor_kernels() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kPanelSmemMax));
   if (e != cudaSuccess) return e;
-  for (auto fn : {update_mma_kernel<0>, update_mma_kernel<1>, update_mma_kernel<2>}) {
-    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMmaSmem);
+  for (auto fn : {update_mma_kernel<0, 128>, update_mma_kernel<1, 128>, update_mma_kernel<2, 128>}) {
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(mma_smem<128>()));
+    if (e != cudaSuccess) return e;
+  }
+  for (auto fn : {update_mma_kernel<0, 64>, update_mma_kernel<1, 64>, update_mma_kernel<2, 64>}) {
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(mma_smem<64>()));
     if (e != cudaSuccess) return e;
   }
   return e;

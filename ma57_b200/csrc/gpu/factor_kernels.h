@@ -61,6 +61,15 @@ void launch_tc_far(const FrontDesc* fronts, FrontState* st, const int* list, int
                    const double* guard, int grid, FactorGlobals* g, int level, int dynamic, int* err,
                    cudaStream_t stream);
 
+// Checked build: validate the tables of `count` fronts (list, or all fronts
+// when list is null) into o.chk. ranges: device array of nranges (lo, hi)
+// pairs, the front allocations; phase 0 before the factorization, 1 after
+// it, 2 before a solve (W slices of wcols columns inside [wlo, whi)).
+void launch_validate_fronts(const FrontDesc* fronts, const ChildLink* links, const FrontState* st, const int* list,
+                            int count, int num_fronts, int n, const int* a_colptr, const KernelOpts& o,
+                            const double* const* ranges, int nranges, const double* wlo, const double* whi,
+                            int wcols, int phase, cudaStream_t stream);
+
 // graph launches: atomicMin(g->unfinished_level, level) if a front of the
 // list is not finished
 void launch_mark_unfinished(const FrontState* st, const int* list, int count, FactorGlobals* g, int level,
@@ -70,15 +79,20 @@ void launch_count_unfinished(const FrontState* st, const int* list, int count, i
 // near (far = false) / far (far = true) Schur-complement update, FP64. With
 // tc_guard (far only; the split pre-pass's maxima, 2 per list entry) it
 // applies just the blocks that tc_block_ok sends away from the tensor cores.
+// tile_rows: 128 (default) or 64 rows per update tile.
 void launch_update(bool far, const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
-                   FactorGlobals* g, int level, int dynamic, cudaStream_t stream, const double* tc_guard = nullptr);
+                   FactorGlobals* g, int level, int dynamic, cudaStream_t stream, const double* tc_guard = nullptr,
+                   int tile_rows = 128);
 // near and far updates of every front in one launch (FP64 path)
 void launch_update_both(const FrontDesc* fronts, FrontState* st, const int* list, int count, int grid_x,
-                        FactorGlobals* g, int level, int dynamic, cudaStream_t stream);
+                        FactorGlobals* g, int level, int dynamic, cudaStream_t stream, int tile_rows = 128);
 
 // Solve
-void launch_permute_in(int n, int nrhs, const int* perm, const double* B, int ldb, double* Bp, cudaStream_t stream);
-void launch_permute_out(int n, int nrhs, const int* perm, const double* X, double* Xout, int ldx, cudaStream_t stream);
+// chk: status word of the checked build's permutation-entry checks (or null)
+void launch_permute_in(int n, int nrhs, const int* perm, const double* B, int ldb, double* Bp, cudaStream_t stream,
+                       CheckWord* chk = nullptr);
+void launch_permute_out(int n, int nrhs, const int* perm, const double* X, double* Xout, int ldx, cudaStream_t stream,
+                        CheckWord* chk = nullptr);
 // Pipelined level solves (one cooperative launch per level; see
 // solve_kernels.cu). tasks: int4 (see the kernels); flags indexed by
 // flag_base[front] + block, compared against epoch; every wait on another

@@ -97,19 +97,32 @@ __device__ __forceinline__ void publish(int* flags, int idx, int epoch) {
 }  // namespace
 
 __global__ void permute_in_kernel(int n, int nrhs, const int* __restrict__ perm, const double* __restrict__ B, int ldb,
-                                  double* __restrict__ Bp) {
+                                  double* __restrict__ Bp, CheckWord* chk) {
   const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   if (t >= static_cast<long long>(n) * nrhs) return;
   const int i = static_cast<int>(t % n), c = static_cast<int>(t / n);
-  Bp[t] = B[perm[i] + static_cast<long long>(c) * ldb];
+  const int p = perm[i];
+  Bp[t] = check(in_range(p, 0, n), chk, kChkPermute, i) ? B[p + static_cast<long long>(c) * ldb] : 0.0;
 }
 
 __global__ void permute_out_kernel(int n, int nrhs, const int* __restrict__ perm, const double* __restrict__ X,
-                                   double* __restrict__ Xout, int ldx) {
+                                   double* __restrict__ Xout, int ldx, CheckWord* chk) {
   const long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   if (t >= static_cast<long long>(n) * nrhs) return;
   const int i = static_cast<int>(t % n), c = static_cast<int>(t / n);
-  Xout[perm[i] + static_cast<long long>(c) * ldx] = X[t];
+  const int p = perm[i];
+  if (check(in_range(p, 0, n), chk, kChkPermute, i)) Xout[p + static_cast<long long>(c) * ldx] = X[t];
+}
+
+// Checked build: a row index or a child workspace row out of range raises
+// the solve's error word (the other CTAs then stop waiting) and the access
+// is skipped. The ordinary build compiles this to true.
+__device__ __forceinline__ bool solve_index_ok(bool ok, int* err) {
+  if constexpr (kCheckedBuild) {
+    if (!ok) atomicCAS(err, 0, kSolveErrBounds);
+    return ok;
+  }
+  return true;
 }
 
 // Shared-memory layout of both pipelined kernels (dynamic, doubles):
@@ -182,7 +195,11 @@ __device__ bool forward_block(const FrontDesc* __restrict__ fronts, const ChildL
   for (int t = threadIdx.x; t < nr * nc; t += kST) {
     const int ii = t % nr, c = t / nr;
     const int i = r0 + ii;
-    double v = (i < np) ? Bp[f.fidx[i] + static_cast<int64_t>(c0 + c) * n] : 0.0;
+    double v = 0.0;
+    if (i < np) {
+      const int gi = f.fidx[i];
+      if (solve_index_ok(in_range(gi, 0, n), err)) v = Bp[gi + static_cast<int64_t>(c0 + c) * n];
+    }
     const int pre = f.lperm[i];
     for (int ch = f.ch_begin; ch < f.ch_end; ++ch) {
       const ChildLink L = links[ch];
@@ -190,7 +207,7 @@ __device__ bool forward_block(const FrontDesc* __restrict__ fronts, const ChildL
       if (a < 0) continue;
       const FrontDesc& cf = fronts[L.child];
       const int cnp = st[L.child].npiv;
-      v += cf.W[cnp + a + static_cast<int64_t>(c0 + c) * cf.wld];
+      if (solve_index_ok(cnp >= 0 && cnp + a < cf.m, err)) v += cf.W[cnp + a + static_cast<int64_t>(c0 + c) * cf.wld];
     }
     acc[ii * kAccStride + c] = v;
   }
@@ -387,7 +404,12 @@ __device__ bool backward_block(const FrontDesc* __restrict__ fronts, const Front
       const int ni = i1 - i0;
       for (int t = threadIdx.x; t < kRB * nc; t += kST) {
         const int ii = t % kRB, c = t / kRB;
-        xb[ii * kAccStride + c] = (ii < ni) ? X[f.fidx[i0 + ii] + static_cast<int64_t>(c0 + c) * n] : 0.0;
+        double xv = 0.0;
+        if (ii < ni) {
+          const int gi = f.fidx[i0 + ii];
+          if (solve_index_ok(in_range(gi, 0, n), err)) xv = X[gi + static_cast<int64_t>(c0 + c) * n];
+        }
+        xb[ii * kAccStride + c] = xv;
       }
       if (more)
         scp_wait<1>();
@@ -462,7 +484,8 @@ __device__ bool backward_block(const FrontDesc* __restrict__ fronts, const Front
   } else {
     for (int t = threadIdx.x; t < nq * nc; t += kST) {
       const int qq = t % nq, c = t / nq;
-      X[f.fidx[q0 + qq] + static_cast<int64_t>(c0 + c) * n] = acc[qq * kAccStride + c];
+      const int gi = f.fidx[q0 + qq];
+      if (solve_index_ok(in_range(gi, 0, n), err)) X[gi + static_cast<int64_t>(c0 + c) * n] = acc[qq * kAccStride + c];
     }
     publish(flags, flag_base[s] + cb, epoch);
   }
@@ -657,11 +680,15 @@ cudaError_t launch_backward_pipelined(const FrontDesc* fronts, const FrontState*
                                      args, kSolveSmem, stream);
 }
 
-void launch_permute_in(int n, int nrhs, const int* perm, const double* B, int ldb, double* Bp, cudaStream_t stream) {
-  permute_in_kernel<<<grid_for(static_cast<long long>(n) * nrhs, 256), 256, 0, stream>>>(n, nrhs, perm, B, ldb, Bp);
+void launch_permute_in(int n, int nrhs, const int* perm, const double* B, int ldb, double* Bp, cudaStream_t stream,
+                       CheckWord* chk) {
+  permute_in_kernel<<<grid_for(static_cast<long long>(n) * nrhs, 256), 256, 0, stream>>>(n, nrhs, perm, B, ldb, Bp,
+                                                                                         chk);
 }
-void launch_permute_out(int n, int nrhs, const int* perm, const double* X, double* Xout, int ldx, cudaStream_t stream) {
-  permute_out_kernel<<<grid_for(static_cast<long long>(n) * nrhs, 256), 256, 0, stream>>>(n, nrhs, perm, X, Xout, ldx);
+void launch_permute_out(int n, int nrhs, const int* perm, const double* X, double* Xout, int ldx, cudaStream_t stream,
+                        CheckWord* chk) {
+  permute_out_kernel<<<grid_for(static_cast<long long>(n) * nrhs, 256), 256, 0, stream>>>(n, nrhs, perm, X, Xout, ldx,
+                                                                                          chk);
 }
 void launch_residual(int n, int nrhs, const int* rowptr, const int* colind, const int* vidx, const double* vals,
                      const double* X, int ldx, const double* B, int ldb, double* R, cudaStream_t stream) {

@@ -87,4 +87,31 @@ def test_autotuned_schedule_keeps_results():
     assert s.inertia().as_tuple() == inertia
     assert backward_error(A, s.solve(B), B) <= 10 * max(backward_error(A, X0, B), 1e-16)
     info = autotune.level_info(s)
-    assert any(i["small_threads"] or i["cluster_ctas"] for i in info) or schedule == {"small": {}, "large": {}}
+    assert any(i["small_threads"] or i["cluster_ctas"] for i in info) or not (schedule["small"] or schedule["large"])
+
+
+@pytest.mark.parametrize("rows", [64, 128])
+def test_update_tile_rows_keep_results(rows):
+    """Both Schur-update tile shapes (rows x 64) give the same inertia and a
+    backward error as small as the default's (the summation order within a
+    tile is the same; only the tiling of the trailing block differs)."""
+    import ctypes as C
+    from ma57_b200 import _lib as L
+    A, B = M.config3(20, nrhs=2)
+    s = SymLDLT()
+    s.setOrdering(OrderingType.Metis)
+    s.analyzePattern(A)
+    s.factorize(A)
+    inertia, X0 = s.inertia().as_tuple(), s.solve(B)
+    lib = L.load()
+    nlev = int(s.plan_stats()["levels"])
+    for lv in range(nlev):
+        assert lib.symla_gpu_set_level_update_rows(s._ctx.h, lv, rows) == L.SYMLA_OK
+    out = C.c_int()
+    assert lib.symla_gpu_level_update_rows(s._ctx.h, 0, C.byref(out)) == L.SYMLA_OK and out.value == rows
+    assert lib.symla_gpu_set_level_update_rows(s._ctx.h, 0, 32) == L.SYMLA_ERR_INVALID
+    s.factorize(A)
+    assert s.inertia().as_tuple() == inertia
+    X = s.solve(B)
+    assert backward_error(A, X, B) <= 10 * max(backward_error(A, X0, B), 1e-16)
+    np.testing.assert_allclose(X, X0, rtol=0, atol=1e-9 * np.abs(X0).max())
