@@ -41,6 +41,11 @@ METRIC = "factorize+solve s at backward error ≤1e-12: mixed/learned vs plain F
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
+# Bytes of DRAM traffic per algorithmic flop of the FP64 Schur update,
+# measured by ncu on config 3 at k = 40 (see roofline below).
+UPDATE_DRAM_BYTES_PER_FLOP = 1.2578e9 / 25.8151e9
+
+
 def load_peaks():
     try:
         with open(PEAKS_PATH) as f:
@@ -480,6 +485,7 @@ def run_configs(args):
         clk = clocks_start(0)
         s = SymLDLT()
         s.setOrdering(OrderingType.AMD)
+        s.setGraphLaunch(bool(args.graph))
         if kkt:
             s.setMode(Mode.StaticRegularized)
             s.setKKTBlockSizes(*kkt)
@@ -797,7 +803,18 @@ def run_ours(args):
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "peak_source": f"HBM copy, {peak_kind}",
                     "algorithmic_bytes_per_launch": bytes_k / max(1, launches_k)}
-    roofline.update({"frac": achieved / peak if peak else None, "traffic": None, "kernel": dom,
+    # DRAM traffic per launch: ncu's dram__bytes_read.sum + dram__bytes_write.sum
+    # of every FP64 update launch of config 3 at k = 40 (1.257 GB per
+    # factorization for 25.8 GFLOP: 0.0487 bytes per flop), scaled to this
+    # run's average launch by its flops; those metrics take several replay
+    # passes, so the 64^3 workload itself is not captured with them
+    traffic = None
+    if dom == "far_update" and prec == L.PREC_FP64:
+        traffic = {"bytes_per_launch": UPDATE_DRAM_BYTES_PER_FLOP * flops_k / max(1, launches_k),
+                   "source": "ncu DRAM bytes of all update launches at k=40 (0.0487 B/flop), scaled by flops"}
+    roofline.update({"frac": achieved / peak if peak else None,
+                     "traffic": traffic["bytes_per_launch"] if traffic else None,
+                     "traffic_source": traffic["source"] if traffic else None, "kernel": dom,
                      "launches_per_step": launches_k / steps, "ms_per_step": ms_k / steps,
                      "avg_launch_us": 1e3 * ms_k / max(1, launches_k)})
 

@@ -1052,10 +1052,8 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
       atomicAdd(far ? &g->flops_far : &g->flops_near, 2.0 * (q1 - q0) * entries);
     }
   }
-  __syncthreads();
-  if (threadIdx.x == 0)
-    for (int t = 1; t < nent; ++t) tile_end[t] += tile_end[t - 1];
-  __syncthreads();
+  __shared__ int scan_tot[kMThreads / 32];
+  block_inclusive_scan<kMThreads, 2 * kMaxUpdateFronts / kMThreads>(tile_end, nent, scan_tot);
   const int total = nent > 0 ? tile_end[nent - 1] : 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wr = warp / WCOLS, wc = warp % WCOLS;   // warp's 32 x WN sub-tile
@@ -1066,9 +1064,16 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
   int m = 0, c0 = 0, c1 = 0, q0 = 0, q1 = 0, nchunks = 0;
   int64_t ld = 0;
   unsigned u = 0;  // chunks consumed by this CTA so far (ring stage u % 3, phase (u / 3) & 1)
+  // the CTA's tiles increase, so the entry fi, its column tile tj and that
+  // column tile's first tile (tj_first, counted within the entry) only move
+  // forward: each is advanced from where the previous tile left it
+  int fi = 0, tj = 0, tj_first = 0;
   for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
-    int fi = 0;
-    while (tile >= tile_end[fi]) ++fi;
+    while (tile >= tile_end[fi]) {
+      ++fi;
+      tj = 0;
+      tj_first = 0;
+    }
     if (fi != cur) {
       if (cur >= 0) {
         tmax = warp_max(tmax);
@@ -1083,15 +1088,14 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
       update_range(st[s], m, entry_far(fi), c0, c1, q0, q1);
       nchunks = (q1 - q0 + kKM - 1) / kKM;
     }
-    int rem = tile - (fi > 0 ? tile_end[fi - 1] : 0);
-    int tj = 0;
+    const int rel = tile - (fi > 0 ? tile_end[fi - 1] : 0);
     for (;;) {
       const int nr = (m - (c0 + tj * kTJ) + TM - 1) / TM;
-      if (rem < nr) break;
-      rem -= nr;
+      if (rel < tj_first + nr) break;
+      tj_first += nr;
       ++tj;
     }
-    const int j0 = c0 + tj * kTJ, i0 = j0 + rem * TM;
+    const int j0 = c0 + tj * kTJ, i0 = j0 + (rel - tj_first) * TM;
     const int sa = i0 & 1, sb = j0 & 1;  // parity offsets of the staged rows
     __syncthreads();  // previous tile done with every stage
     if (warp == 0) {

@@ -90,4 +90,47 @@ __device__ __forceinline__ double nan_sticky_absmax(double m, double x) {
   return (a > m || a != a) ? (m != m ? m : a) : m;
 }
 
+// In-place inclusive prefix sum of a[0, n) (n <= PER * NT) by the whole CTA
+// of NT threads: each thread sums PER consecutive entries, the per-thread
+// sums are scanned with warp shuffles and one pass over the warp totals,
+// and each thread rewrites its entries. Every thread must call it; it starts
+// and ends with a block barrier.
+template <int NT, int PER>
+__device__ __forceinline__ void block_inclusive_scan(int* a, int n, int* warp_tot) {
+  static_assert(NT % 32 == 0 && NT / 32 <= 32, "block size");
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int b0 = threadIdx.x * PER;
+  int loc = 0;
+#pragma unroll
+  for (int i = 0; i < PER; ++i)
+    if (b0 + i < n) loc += a[b0 + i];
+  int x = loc;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < NT / 32 ? warp_tot[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < NT / 32) warp_tot[lane] = w;
+  }
+  __syncthreads();
+  int run = x - loc + (warp > 0 ? warp_tot[warp - 1] : 0);
+#pragma unroll
+  for (int i = 0; i < PER; ++i)
+    if (b0 + i < n) {
+      run += a[b0 + i];
+      a[b0 + i] = run;
+    }
+  __syncthreads();
+}
+
 }  // namespace symla_gpu

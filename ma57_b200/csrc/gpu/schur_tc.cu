@@ -271,10 +271,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_far_update_kernel(const FrontD
       atomicAdd(&g->flops_far, 2.0 * (q1 - q0) * entries);
     }
   }
-  __syncthreads();
-  if (threadIdx.x == 0)
-    for (int t = 1; t < count; ++t) tile_end[t] += tile_end[t - 1];
-  __syncthreads();
+  __shared__ int scan_tot[kThreads / 32];
+  block_inclusive_scan<kThreads, kMaxFronts / kThreads>(tile_end, count, scan_tot);
   const int total = count > 0 ? tile_end[count - 1] : 0;
   if (static_cast<int>(blockIdx.x) >= total) return;
 
@@ -303,23 +301,29 @@ __global__ void __launch_bounds__(kThreads, 1) tc_far_update_kernel(const FrontD
   int loading[kStages] = {0, 0};  // TMA loads into stage s not yet observed complete
   bool ok = true;
 
+  // the CTA's tiles increase: the front entry and its column tile advance
+  // from where the previous tile left them
+  int fi = 0, tj = 0, tj_first = 0;
   for (int tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
-    int fi = 0;
-    while (tile >= tile_end[fi]) ++fi;
+    while (tile >= tile_end[fi]) {
+      ++fi;
+      tj = 0;
+      tj_first = 0;
+    }
     const int s = list[fi];
     const FrontDesc f = fronts[s];
     const FrontState S = st[s];
     int c0, q0, q1;
     far_range(S, f.m, c0, q0, q1);
     const int m = f.m;
-    int rem = tile - (fi > 0 ? tile_end[fi - 1] : 0), tj = 0;
+    const int rel = tile - (fi > 0 ? tile_end[fi - 1] : 0);
     for (;;) {
       const int nr = (m - (c0 + tj * kTN) + kTM - 1) / kTM;
-      if (rem < nr) break;
-      rem -= nr;
+      if (rel < tj_first + nr) break;
+      tj_first += nr;
       ++tj;
     }
-    const int j0 = c0 + tj * kTN, i0 = j0 + rem * kTM;
+    const int j0 = c0 + tj * kTN, i0 = j0 + (rel - tj_first) * kTM;
     const int K = q1 - q0;
     const int nchunks = (K + kBoxK - 1) / kBoxK;
     const CUtensorMap* map = maps + fi;

@@ -239,6 +239,7 @@ __device__ bool forward_block(const FrontDesc* __restrict__ fronts, const ChildL
       if (row < nr) {
         double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
         const int cb4 = cg * 4;
+#pragma unroll 8
         for (int jj = 0; jj < nj; ++jj) {
           const double l = T[row * kTileStride + jj];
           const double* y = xb + jj * kAccStride + cb4;
@@ -263,17 +264,34 @@ __device__ bool forward_block(const FrontDesc* __restrict__ fronts, const ChildL
       if (threadIdx.x < npv - 1 && f.pk[r0 + threadIdx.x] == 1)
         T[(threadIdx.x + 1) * kTileStride + threadIdx.x] = 0.0;  // d21 slot of a 2x2 pivot
       __syncthreads();
+      // a warp takes right-hand sides c and c + 8 together: the two
+      // substitution chains interleave (each step is a shuffle and an FMA)
       const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-      for (int c = warp; c < nc; c += kST / 32) {
+      constexpr int NW = kST / 32;
+      for (int c = warp; c < nc; c += 2 * NW) {
+        const int cb = c + NW;
+        const bool two = cb < nc;
         double y0 = (lane < nr) ? acc[lane * kAccStride + c] : 0.0;
         double y1 = (lane + 32 < nr) ? acc[(lane + 32) * kAccStride + c] : 0.0;
+        double z0 = (two && lane < nr) ? acc[lane * kAccStride + cb] : 0.0;
+        double z1 = (two && lane + 32 < nr) ? acc[(lane + 32) * kAccStride + cb] : 0.0;
         for (int jj = 0; jj < npv; ++jj) {
           const double yj = __shfl_sync(0xffffffffu, jj < 32 ? y0 : y1, jj & 31);
-          if (lane > jj) y0 -= T[lane * kTileStride + jj] * yj;
-          if (lane + 32 > jj) y1 -= T[(lane + 32) * kTileStride + jj] * yj;
+          const double zj = __shfl_sync(0xffffffffu, jj < 32 ? z0 : z1, jj & 31);
+          const double t0 = T[lane * kTileStride + jj], t1 = T[(lane + 32) * kTileStride + jj];
+          if (lane > jj) {
+            y0 -= t0 * yj;
+            z0 -= t0 * zj;
+          }
+          if (lane + 32 > jj) {
+            y1 -= t1 * yj;
+            z1 -= t1 * zj;
+          }
         }
         if (lane < nr) acc[lane * kAccStride + c] = y0;
         if (lane + 32 < nr) acc[(lane + 32) * kAccStride + c] = y1;
+        if (two && lane < nr) acc[lane * kAccStride + cb] = z0;
+        if (two && lane + 32 < nr) acc[(lane + 32) * kAccStride + cb] = z1;
       }
       __syncthreads();
     }
@@ -422,6 +440,7 @@ __device__ bool backward_block(const FrontDesc* __restrict__ fronts, const Front
       if (col < nq) {
         double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
         const int cb4 = cg * 4;
+#pragma unroll 8
         for (int ii = 0; ii < ni; ++ii) {
           const double l = T[ii * kTileStride + col];
           const double* x = xb + ii * kAccStride + cb4;
@@ -457,18 +476,33 @@ __device__ bool backward_block(const FrontDesc* __restrict__ fronts, const Front
       if (threadIdx.x < nq - 1 && f.pk[q0 + threadIdx.x] == 1)
         T[(threadIdx.x + 1) * kTileStride + threadIdx.x] = 0.0;  // d21 slot of a 2x2 pivot
       __syncthreads();
-      for (int c = warp; c < nc; c += NW) {
+      // right-hand sides c and c + NW together (interleaved chains)
+      for (int c = warp; c < nc; c += 2 * NW) {
+        const int cb = c + NW;
+        const bool two = cb < nc;
         double x0 = (lane < nq) ? acc[lane * kAccStride + c] : 0.0;
         double x1 = (lane + 32 < nq) ? acc[(lane + 32) * kAccStride + c] : 0.0;
+        double u0 = (two && lane < nq) ? acc[lane * kAccStride + cb] : 0.0;
+        double u1 = (two && lane + 32 < nq) ? acc[(lane + 32) * kAccStride + cb] : 0.0;
         for (int jj = nq - 1; jj >= 0; --jj) {
           // x[jj] is final once every row below it has been applied; row jj
           // of Ltop then updates the unknowns above it
           const double xj = __shfl_sync(0xffffffffu, jj < 32 ? x0 : x1, jj & 31);
-          if (lane < jj) x0 -= T[jj * kTileStride + lane] * xj;
-          if (lane + 32 < jj) x1 -= T[jj * kTileStride + lane + 32] * xj;
+          const double uj = __shfl_sync(0xffffffffu, jj < 32 ? u0 : u1, jj & 31);
+          const double t0 = T[jj * kTileStride + lane], t1 = T[jj * kTileStride + lane + 32];
+          if (lane < jj) {
+            x0 -= t0 * xj;
+            u0 -= t0 * uj;
+          }
+          if (lane + 32 < jj) {
+            x1 -= t1 * xj;
+            u1 -= t1 * uj;
+          }
         }
         if (lane < nq) acc[lane * kAccStride + c] = x0;
         if (lane + 32 < nq) acc[(lane + 32) * kAccStride + c] = x1;
+        if (two && lane < nq) acc[lane * kAccStride + cb] = u0;
+        if (two && lane + 32 < nq) acc[(lane + 32) * kAccStride + cb] = u1;
       }
       __syncthreads();
     }
