@@ -159,12 +159,23 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(const FrontDesc* __res
     }
   }
   // max |entry| of the assembled front (dense_kernel.hpp:413), folded here
-  // so the panel kernel does not rescan the front
+  // so the panel kernel does not rescan the front: a thread takes a row and
+  // reads its (up to) 32 entries of the task's columns with independent
+  // loads (consecutive rows across a warp), then the next row
   __syncthreads();
   double tmax = 0.0;
-  for (int j = j0; j < j1; ++j) {
-    const double* col = f.F + static_cast<int64_t>(j) * f.ld;
-    for (int i = max(j, i0) + threadIdx.x; i < iend; i += blockDim.x) tmax = fmax(tmax, fabs(col[i]));
+  const double* blk = f.F + static_cast<int64_t>(j0) * f.ld;
+  for (int i = i0 + threadIdx.x; i < iend; i += blockDim.x) {
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+#pragma unroll
+    for (int jj = 0; jj < 32; jj += 4) {
+      const double* p = blk + static_cast<int64_t>(jj) * f.ld + i;
+      if (jj + 0 < nj && j0 + jj + 0 <= i) t0 = fmax(t0, fabs(p[0]));
+      if (jj + 1 < nj && j0 + jj + 1 <= i) t1 = fmax(t1, fabs(p[f.ld]));
+      if (jj + 2 < nj && j0 + jj + 2 <= i) t2 = fmax(t2, fabs(p[2 * static_cast<int64_t>(f.ld)]));
+      if (jj + 3 < nj && j0 + jj + 3 <= i) t3 = fmax(t3, fabs(p[3 * static_cast<int64_t>(f.ld)]));
+    }
+    tmax = fmax(tmax, fmax(fmax(t0, t1), fmax(t2, t3)));
   }
   tmax = warp_max(tmax);
   if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&st[s].orig_max, tmax);

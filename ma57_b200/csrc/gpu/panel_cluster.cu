@@ -648,17 +648,26 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
             f.pk[k0 + c] = 0;
           }
         }
-        for (int c = 0; c < kstar; ++c) {
-          const double d = sh.dv[c];
-          if (d > 0)
-            ++n_pos;
-          else if (d < 0)
-            ++n_neg;
-          else
-            ++n_zero;
-          if (sh.pv[c] != 0.0) {
-            pert += fabs(sh.pv[c]);
-            ++nPert;
+        // inertia of the accepted pivots (only thread 0's counters are
+        // written back): one ballot each over warp 0's lanes; the
+        // perturbations (static mode) are summed in pivot order
+        if (warp == 0) {
+          const bool in = lane < kstar;
+          const double d = in ? sh.dv[lane] : 0.0;
+          const unsigned pos = __ballot_sync(0xffffffffu, in && d > 0);
+          const unsigned neg = __ballot_sync(0xffffffffu, in && d < 0);
+          const unsigned zer = __ballot_sync(0xffffffffu, in && !(d > 0) && !(d < 0));
+          const unsigned per = __ballot_sync(0xffffffffu, in && sh.pv[lane] != 0.0);
+          if (lane == 0) {
+            n_pos += __popc(pos);
+            n_neg += __popc(neg);
+            n_zero += __popc(zer);
+            if (per)
+              for (int c = 0; c < kstar; ++c)
+                if (sh.pv[c] != 0.0) {
+                  pert += fabs(sh.pv[c]);
+                  ++nPert;
+                }
           }
         }
         if (threadIdx.x < kstar) {
