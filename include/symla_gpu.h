@@ -308,9 +308,12 @@ int symla_gpu_set_graph(symla_gpu_ctx* ctx, int enable);
 /* Tile schedule per tree level (no reference counterpart; chosen by the
  * autotuner in ma57_b200/autotune.py). level_info: out6 = {small fronts,
  * their max m, large fronts, their max m, small-front kernel threads, panel
- * cluster CTAs}. set_level_schedule: small-front kernel threads in {128,
- * 256} and panel cluster size in {2, 4, 8, 16}, 0 = chosen by front size; a
- * cluster size too small for the level's fronts falls back to the default. */
+ * cluster CTAs}. set_level_schedule: small-front kernel threads in {32
+ * (one warp per front, eight fronts per CTA; fronts of at most 32 rows),
+ * 128, 256} and panel cluster size in {2, 4, 8, 16}, or 1 for the single-CTA
+ * panel kernel (no cluster barriers: faster for levels whose panels decide
+ * many pivots one at a time), 0 = chosen by front size; a cluster size too
+ * small for the level's fronts falls back to the default. */
 int symla_gpu_level_info(symla_gpu_ctx* ctx, int level, int* out6);
 int symla_gpu_set_level_schedule(symla_gpu_ctx* ctx, int level, int small_threads, int cluster_ctas);
 /* Rows per tile of the level's Schur-complement update (the tile shape

@@ -1,9 +1,12 @@
 """Front-size-to-tile-shape schedule chosen by measurement.
 
 Three launch shapes depend on front size and have no single best value:
-the width of the small-front kernel (128 or 256 threads per front), the
+the width of the small-front kernel (a warp per front for fronts of at most
+32 rows, or 128 or 256 threads per front), the
 number of CTAs in the panel cluster of the large fronts (2, 4, 8 or 16; more
-CTAs hold fewer rows each but occupy more SMs) and the tile shape of their
+CTAs hold fewer rows each but occupy more SMs; or 1, the single-CTA panel
+kernel, whose pivot-by-pivot decisions need no cluster barriers) and the
+tile shape of their
 Schur-complement update (128 x 64 or 64 x 64: the smaller tile wastes less
 of small fronts' trailing blocks, the larger reuses operands more). The tree
 levels are bucketed by
@@ -81,7 +84,7 @@ def tune(solver, A, reps: int = 2):
     apply(solver, schedule)
     base = _factor_ms(solver, A, reps)
     best = base
-    for kind, buckets, cands in (("small", small_b, (128, 256)), ("large", large_b, (2, 4, 8, 16)),
+    for kind, buckets, cands in (("small", small_b, (32, 128, 256)), ("large", large_b, (1, 2, 4, 8, 16)),
                                  ("update", large_b, (64, 128))):
         for b in buckets:
             for cand in cands:

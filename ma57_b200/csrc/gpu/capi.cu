@@ -806,13 +806,25 @@ void validate_tables(symla_gpu_ctx* c, int phase, const KernelOpts& ko, const ch
   check_status_word(c, when);
 }
 
+// Default choice of the single-CTA panel kernel (see launch_panel_iteration).
+constexpr int kSinglePanelMaxFronts = 148;
+constexpr int kSinglePanelMaxM = 1024;
+
 void launch_panel_iteration(symla_gpu_ctx* c, const LevelLists& L, int level, const KernelOpts& ko, int dynamic,
                             const int* d_large) {
   cudaStream_t st = c->stream;
   c->cur_level = level;
   const int nl = static_cast<int>(L.large.size());
   timed(c, SYMLA_KERNEL_PANEL, 0.0, 0.0, [&] {
-    if (c->use_cluster_panel && cluster_size_for(L.large_max_m, nl, L.panel_width) > 0) {
+    // the single-CTA panel when asked for (cluster size 1) or, by default in
+    // threshold (Bunch-Kaufman) mode, for levels of fewer large fronts than
+    // SMs none taller than kSinglePanelMaxM rows: there the cluster's
+    // barriers on every pivot-by-pivot decision cost more than its spread of
+    // rows saves (static pivoting never leaves the speculative path, so it
+    // keeps the cluster)
+    const bool single = L.cluster_ctas == 1 || (L.cluster_ctas == 0 && ko.mode == SYMLA_MODE_THRESHOLD &&
+                                                nl < kSinglePanelMaxFronts && L.large_max_m <= kSinglePanelMaxM);
+    if (c->use_cluster_panel && !single && cluster_size_for(L.large_max_m, nl, L.panel_width) > 0) {
       CK(launch_cluster_panel(c->d_desc, c->d_state, d_large, nl, L.large_max_m, L.panel_width, ko, c->d_glob, level,
                               dynamic, st, L.cluster_ctas));
     } else {
@@ -2170,20 +2182,25 @@ extern "C" int symla_gpu_level_info(symla_gpu_ctx* c, int level, int* out6) {
 
 extern "C" int symla_gpu_set_level_schedule(symla_gpu_ctx* c, int level, int small_threads, int cluster_ctas) {
   if (!c || level < 0 || level >= c->numLevels) return set_error(SYMLA_ERR_INVALID, "level out of range");
-  if ((small_threads != 0 && small_threads != 128 && small_threads != 256) ||
-      (cluster_ctas != 0 && cluster_ctas != 2 && cluster_ctas != 4 && cluster_ctas != 8 && cluster_ctas != 16))
+  if ((small_threads != 0 && small_threads != 32 && small_threads != 128 && small_threads != 256) ||
+      (cluster_ctas != 0 && cluster_ctas != 1 && cluster_ctas != 2 && cluster_ctas != 4 && cluster_ctas != 8 &&
+       cluster_ctas != 16))
     return set_error(SYMLA_ERR_INVALID,
-                     "symla_gpu_set_level_schedule: small_threads in {0,128,256}, cluster_ctas in {0,2,4,8,16}");
+                     "symla_gpu_set_level_schedule: small_threads in {0,32,128,256}, cluster_ctas in {0,1,2,4,8,16}");
   auto& L = c->levels[level];
-  if (L.small_threads != small_threads || L.cluster_ctas != cluster_ctas) {
+  if (L.small_threads == small_threads && L.cluster_ctas == cluster_ctas) return SYMLA_OK;
+  return guarded([&] {
+    // the single-CTA panel keeps its two working columns in a global buffer
+    // when they do not fit its shared memory
+    if (cluster_ctas == 1 && !L.large.empty() && !panel_fits_shared(L.large_max_m) && !L.d_panel_cols)
+      L.d_panel_cols = dalloc<double>(2 * static_cast<size_t>(L.large_max_m) * L.large.size());
     L.small_threads = small_threads;
     L.cluster_ctas = cluster_ctas;
     if (c->graph_exec) {  // the captured launches used the old shapes
       cudaGraphExecDestroy(c->graph_exec);
       c->graph_exec = nullptr;
     }
-  }
-  return SYMLA_OK;
+  });
 }
 
 extern "C" int symla_gpu_set_level_update_rows(symla_gpu_ctx* c, int level, int rows) {

@@ -186,6 +186,13 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(const FrontDesc* __res
 // (assembly, factorization and write-back in one launch).
 namespace {
 
+// Warp mode of the small-front kernel: fronts of at most kWarpFrontMax rows,
+// kWarpFronts per CTA, each in a fixed slice of kWarpFrontDoubles of the
+// dynamic shared memory (the m x (m | 1) front plus its two index arrays).
+constexpr int kWarpFrontMax = 32;
+constexpr int kWarpFronts = 8;
+constexpr int kWarpFrontDoubles = kWarpFrontMax * (kWarpFrontMax | 1) + kWarpFrontMax;
+
 template <int NT>
 struct SmallFront {
   double* S;
@@ -207,9 +214,9 @@ struct SmallFront {
 // there is one integer division per call instead of one per entry, and no
 // thread idles on the upper half.
 template <int NT, class Fn>
-__device__ __forceinline__ void for_lower(int t, Fn&& fn) {
+__device__ __forceinline__ void for_lower(int t, int tid, Fn&& fn) {
   const int R = t + 1, C = (t + 1) >> 1;
-  int q = threadIdx.x % R, c = threadIdx.x / R;  // position c R + q, advancing by NT
+  int q = tid % R, c = tid / R;  // position c R + q, advancing by NT
   const int dq = NT % R, dc = NT / R;
   while (c < C) {
     if (q >= c && q < t) {
@@ -227,11 +234,36 @@ __device__ __forceinline__ void for_lower(int t, Fn&& fn) {
   }
 }
 
+// The threads that factor one small front: the whole CTA (NT = 128 or 256)
+// or one warp (NT = 32; the CTA then holds kWarpFronts fronts, one per
+// warp, and no block-wide barrier is used).
+template <int NT>
+__device__ __forceinline__ void grp_sync() {
+  if constexpr (NT == 32)
+    __syncwarp();
+  else
+    __syncthreads();
+}
+template <int NT>
+__device__ __forceinline__ ArgMax grp_argmax(ArgMax a, double* sv, int* si) {
+  if constexpr (NT == 32)
+    return warp_argmax(a);
+  else
+    return block_argmax<NT>(a, sv, si);
+}
+template <int NT>
+__device__ __forceinline__ double grp_max(double v, double* sv) {
+  if constexpr (NT == 32)
+    return warp_max(v);
+  else
+    return block_max<NT>(v, sv);
+}
+
 // Symmetric swap of positions i < j in lower storage over the whole front.
 template <int NT>
-__device__ void smem_swap(SmallFront<NT>& F, int* fi, int* lp, int i, int j) {
+__device__ void smem_swap(SmallFront<NT>& F, int* fi, int* lp, int i, int j, int tid) {
   const int m = F.m;
-  for (int t = threadIdx.x; t < m - 1; t += NT) {
+  for (int t = tid; t < m - 1; t += NT) {
     if (t < i) {  // row swap in columns c < i
       const int c = t;
       double a = F.at(i, c);
@@ -253,7 +285,7 @@ __device__ void smem_swap(SmallFront<NT>& F, int* fi, int* lp, int i, int j) {
       F.at(r, j) = a;
     }
   }
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     int a = fi[i];
     fi[i] = fi[j];
     fi[j] = a;
@@ -261,24 +293,29 @@ __device__ void smem_swap(SmallFront<NT>& F, int* fi, int* lp, int i, int j) {
     lp[i] = lp[j];
     lp[j] = a;
   }
-  __syncthreads();
+  grp_sync<NT>();
 }
 
 }  // namespace
 
 template <int NT>
-__global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __restrict__ fronts,
-                                                          const ChildLink* __restrict__ links, FrontState* st,
-                                                          const int* __restrict__ front_list,
-                                                          const int* __restrict__ a_colptr, KernelOpts o,
-                                                          FactorGlobals* g, int level, int dynamic) {
+__global__ void __launch_bounds__(NT == 32 ? 32 * kWarpFronts : NT)
+    factor_small_kernel(const FrontDesc* __restrict__ fronts, const ChildLink* __restrict__ links, FrontState* st,
+                        const int* __restrict__ front_list, int count, const int* __restrict__ a_colptr, KernelOpts o,
+                        FactorGlobals* g, int level, int dynamic) {
   if (level_aborted(g, level, dynamic)) return;
-  extern __shared__ double smem[];
+  extern __shared__ double smem_all[];
   __shared__ double red_v[NT / 32];
   __shared__ int red_i[NT / 32];
-  __shared__ int s_np;
+  // warp mode: warp w of the CTA factors list entry kWarpFronts blockIdx + w
+  // in its own slice of shared memory
+  const int tid = NT == 32 ? static_cast<int>(threadIdx.x & 31) : static_cast<int>(threadIdx.x);
+  const int grp = NT == 32 ? static_cast<int>(threadIdx.x >> 5) : 0;
+  const int entry = NT == 32 ? static_cast<int>(blockIdx.x) * kWarpFronts + grp : static_cast<int>(blockIdx.x);
+  if (entry >= count) return;  // (warp mode only: the whole warp leaves)
+  double* smem = smem_all + (NT == 32 ? static_cast<size_t>(grp) * kWarpFrontDoubles : 0);
 
-  const int s = front_list[blockIdx.x];
+  const int s = front_list[entry];
   const FrontDesc f = fronts[s];
   const int m = f.m;
   SmallFront<NT> F{smem, m | 1, m};
@@ -286,27 +323,27 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
   int* lp = fi + m;  // local pivot permutation
 
   // ---- assembly (multifrontal.hpp:498-535), children summed in fixed order
-  for_lower<NT>(m, [&](int i, int j) {
+  for_lower<NT>(m, tid, [&](int i, int j) {
     F.at(i, j) = gather_children(fronts, links, st, f.ch_begin, f.ch_end, i, j, o.chk);
   });
-  for (int t = threadIdx.x; t < m; t += NT) {
+  for (int t = tid; t < m; t += NT) {
     fi[t] = f.fidx[t];
     lp[t] = t;
   }
-  __syncthreads();
+  grp_sync<NT>();
   {
     const int e0 = a_colptr[f.a_begin], e1 = a_colptr[f.a_begin + f.ncols];
-    for (int e = e0 + threadIdx.x; e < e1; e += NT) {
+    for (int e = e0 + tid; e < e1; e += NT) {
       int j, i, idx;
       if (a_entry(o, f, e, j, i, idx)) F.at(i, j) += o.values[idx];
     }
   }
-  __syncthreads();
+  grp_sync<NT>();
 
   // ---- orig_max over the whole front (dense_kernel.hpp:413, :934)
   double tmax = 0.0;
-  for_lower<NT>(m, [&](int i, int j) { tmax = fmax(tmax, fabs(F.at(i, j))); });
-  double orig_max = block_max<NT>(tmax, red_v);
+  for_lower<NT>(m, tid, [&](int i, int j) { tmax = fmax(tmax, fabs(F.at(i, j))); });
+  double orig_max = grp_max<NT>(tmax, red_v);
   const bool isStatic = (o.mode == 1);
   if (isStatic) {
     if (orig_max < o.static_abs_floor) orig_max = 1.0;
@@ -351,24 +388,24 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
         ++n_neg;
       else
         ++n_zero;
-      __syncthreads();
-      if (threadIdx.x == 0) F.at(k, k) = d;
+      grp_sync<NT>();
+      if (tid == 0) F.at(k, k) = d;
       thread_rmax = fmax(thread_rmax, fabs(d));
-      for (int i = k + 1 + threadIdx.x; i < m; i += NT) {
+      for (int i = k + 1 + tid; i < m; i += NT) {
         const double a = F.at(i, k);
         thread_rmax = fmax(thread_rmax, fabs(a));
         F.at(i, k) = a / d;
       }
-      __syncthreads();
-      for_lower<NT>(m - k - 1, [&](int ii, int jj) {
+      grp_sync<NT>();
+      for_lower<NT>(m - k - 1, tid, [&](int ii, int jj) {
         const int i = k + 1 + ii, j = k + 1 + jj;
         const double v = F.at(i, j) - (F.at(i, k) * d) * F.at(j, k);
         F.at(i, j) = v;
         thread_rmax = fmax(thread_rmax, fabs(v));
       });
-      __syncthreads();
+      grp_sync<NT>();
     }
-    for (int t = threadIdx.x; t < effEnd; t += NT) {
+    for (int t = tid; t < effEnd; t += NT) {
         f.Dd[t] = F.at(t, t);
         f.Do[t] = 0.0;
         f.pk[t] = 0;
@@ -377,11 +414,11 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
     // dense_kernel.hpp:576-793, unblocked
     while (k < effEnd) {
       ArgMax am{0.0, -1};
-      for (int i = k + 1 + threadIdx.x; i < effEnd; i += NT) {
+      for (int i = k + 1 + tid; i < effEnd; i += NT) {
         const double v = fabs(F.at(i, k));
         am = argmax_combine(am, ArgMax{v, i});
       }
-      am = block_argmax<NT>(am, red_v, red_i);
+      am = grp_argmax<NT>(am, red_v, red_i);
       const double lambda = am.v;
       const int r = am.i;
       const double akk = F.at(k, k);
@@ -393,9 +430,9 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
         dec = 0;
       } else {
         double sm = 0.0;
-        for (int i = k + threadIdx.x; i < effEnd; i += NT)
+        for (int i = k + tid; i < effEnd; i += NT)
           if (i != r) sm = fmax(sm, fabs(F.sym(i, r)));
-        const double sigma = block_max<NT>(sm, red_v);
+        const double sigma = grp_max<NT>(sm, red_v);
         if (fabs(akk) * sigma >= kAlpha * lambda * lambda)
           dec = 0;
         else if (fabs(F.at(r, r)) >= kAlpha * sigma)
@@ -404,8 +441,8 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
           dec = 2;
       }
       if (dec == 3) break;
-      __syncthreads();
-      if (dec == 1) smem_swap<NT>(F, fi, lp, k, r);
+      grp_sync<NT>();
+      if (dec == 1) smem_swap<NT>(F, fi, lp, k, r, tid);
       if (dec == 0 || dec == 1) {
         const double d = F.at(k, k);
         if (d > 0)
@@ -415,32 +452,32 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
         else
           ++n_zero;
         thread_rmax = fmax(thread_rmax, fabs(d));
-        for (int i = k + 1 + threadIdx.x; i < m; i += NT) {
+        for (int i = k + 1 + tid; i < m; i += NT) {
           const double a = F.at(i, k);
           thread_rmax = fmax(thread_rmax, fabs(a));
           F.at(i, k) = a / d;
         }
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
           f.Dd[k] = d;
           f.Do[k] = 0.0;
           f.pk[k] = 0;
         }
-        __syncthreads();
-        for_lower<NT>(m - k - 1, [&](int ii, int jj) {
+        grp_sync<NT>();
+        for_lower<NT>(m - k - 1, tid, [&](int ii, int jj) {
           const int i = k + 1 + ii, j = k + 1 + jj;
           const double v = F.at(i, j) - (F.at(i, k) * d) * F.at(j, k);
           F.at(i, j) = v;
           thread_rmax = fmax(thread_rmax, fabs(v));
         });
-        __syncthreads();
+        grp_sync<NT>();
         k += 1;
         continue;
       }
       // 2x2 pivot
-      if (r != k + 1) smem_swap<NT>(F, fi, lp, k + 1, r);
+      if (r != k + 1) smem_swap<NT>(F, fi, lp, k + 1, r, tid);
       const double d11 = F.at(k, k), d21 = F.at(k + 1, k), d22 = F.at(k + 1, k + 1);
       const double det = d11 * d22 - d21 * d21;
-      const double rm = fmax(orig_max, block_max<NT>(thread_rmax, red_v));
+      const double rm = fmax(orig_max, grp_max<NT>(thread_rmax, red_v));
       const double rm1 = fmax(1.0, rm);
       if (fabs(det) <= o.zero_tol * rm1 * rm1) break;
       thread_rmax = fmax(thread_rmax, fmax(fabs(d11), fmax(fabs(d21), fabs(d22))));
@@ -459,13 +496,13 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
         }
       }
       const double inv11 = d22 / det, inv21 = -d21 / det, inv22 = d11 / det;
-      for (int i = k + 2 + threadIdx.x; i < m; i += NT) {
+      for (int i = k + 2 + tid; i < m; i += NT) {
         const double a0 = F.at(i, k), a1 = F.at(i, k + 1);
         thread_rmax = fmax(thread_rmax, fmax(fabs(a0), fabs(a1)));
         F.at(i, k) = a0 * inv11 + a1 * inv21;
         F.at(i, k + 1) = a0 * inv21 + a1 * inv22;
       }
-      if (threadIdx.x == 0) {
+      if (tid == 0) {
         f.Dd[k] = d11;
         f.Dd[k + 1] = d22;
         f.Do[k] = d21;
@@ -473,8 +510,8 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
         f.pk[k] = 1;
         f.pk[k + 1] = 2;
       }
-      __syncthreads();
-      for_lower<NT>(m - k - 2, [&](int ii, int jj) {
+      grp_sync<NT>();
+      for_lower<NT>(m - k - 2, tid, [&](int ii, int jj) {
         const int i = k + 2 + ii, j = k + 2 + jj;
         const double l0i = F.at(i, k), l1i = F.at(i, k + 1);
         const double w0 = l0i * d11 + l1i * d21;
@@ -483,23 +520,21 @@ __global__ void __launch_bounds__(NT) factor_small_kernel(const FrontDesc* __res
         F.at(i, j) = v;
         thread_rmax = fmax(thread_rmax, fabs(v));
       });
-      __syncthreads();
+      grp_sync<NT>();
       k += 2;
     }
   }
 
   // ---- write back (lower triangle of the whole front, permuted indices)
-  __syncthreads();
-  for_lower<NT>(m, [&](int i, int j) { f.F[static_cast<int64_t>(j) * f.ld + i] = F.at(i, j); });
-  for (int t = threadIdx.x; t < m; t += NT) {
+  grp_sync<NT>();
+  for_lower<NT>(m, tid, [&](int i, int j) { f.F[static_cast<int64_t>(j) * f.ld + i] = F.at(i, j); });
+  for (int t = tid; t < m; t += NT) {
     f.fidx[t] = fi[t];
     f.lperm[t] = lp[t];
     f.lpos[lp[t]] = t;
   }
-  const double rmax = block_max<NT>(thread_rmax, red_v);
-  if (threadIdx.x == 0) s_np = k;
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  const double rmax = grp_max<NT>(thread_rmax, red_v);
+    if (tid == 0) {
     FrontState& S = st[s];
     S.npiv = k;
     S.n_pos = n_pos;
@@ -1244,10 +1279,17 @@ void launch_factor_small(const FrontDesc* fronts, const ChildLink* links, FrontS
                          cudaStream_t stream, int threads) {
   if (count <= 0) return;
   const size_t sm = small_front_smem(max_m);
-  if (threads == 128 || (threads == 0 && max_m <= 48)) {
-    factor_small_kernel<128><<<count, 128, sm, stream>>>(fronts, links, st, list, a_colptr, o, g, level, dynamic);
+  if (max_m <= kWarpFrontMax && (threads == 32 || threads == 0)) {
+    // one warp per front, kWarpFronts fronts per CTA
+    const int grid = (count + kWarpFronts - 1) / kWarpFronts;
+    factor_small_kernel<32><<<grid, 32 * kWarpFronts, kWarpFronts * kWarpFrontDoubles * sizeof(double), stream>>>(
+        fronts, links, st, list, count, a_colptr, o, g, level, dynamic);
+  } else if (threads == 128 || (threads != 256 && max_m <= 48)) {
+    factor_small_kernel<128><<<count, 128, sm, stream>>>(fronts, links, st, list, count, a_colptr, o, g, level,
+                                                          dynamic);
   } else {
-    factor_small_kernel<256><<<count, 256, sm, stream>>>(fronts, links, st, list, a_colptr, o, g, level, dynamic);
+    factor_small_kernel<256><<<count, 256, sm, stream>>>(fronts, links, st, list, count, a_colptr, o, g, level,
+                                                          dynamic);
   }
 }
 
@@ -1403,6 +1445,9 @@ void launch_validate_fronts(const FrontDesc* fronts, const ChildLink* links, con
 
 cudaError_t configure_factor_kernels() {
   cudaError_t e;
+  e = cudaFuncSetAttribute(factor_small_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(kWarpFronts * kWarpFrontDoubles * sizeof(double)));
+  if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(factor_small_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(factor_small_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);

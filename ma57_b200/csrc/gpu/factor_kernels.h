@@ -25,7 +25,8 @@ void launch_assemble(const FrontDesc* fronts, const ChildLink* links, FrontState
                      int dynamic, cudaStream_t stream);
 void launch_factor_small(const FrontDesc* fronts, const ChildLink* links, FrontState* st, const int* list, int count,
                          int max_m, const int* a_colptr, const KernelOpts& o, FactorGlobals* g, int level, int dynamic,
-                         cudaStream_t stream, int threads = 0);  // threads: 128, 256, or 0 (by front size)
+                         cudaStream_t stream, int threads = 0);  // threads: 32 (a warp per front, fronts of
+                                                                 // <= 32 rows), 128, 256, or 0 (by front size)
 // Single-CTA panel kernel. Its two working columns (2 m doubles per front)
 // live in shared memory when panel_fits_shared(max_m), else in `cols`
 // (device, 2 max_m doubles per front of the list), which is then required.

@@ -115,3 +115,62 @@ def test_update_tile_rows_keep_results(rows):
     X = s.solve(B)
     assert backward_error(A, X, B) <= 10 * max(backward_error(A, X0, B), 1e-16)
     np.testing.assert_allclose(X, X0, rtol=0, atol=1e-9 * np.abs(X0).max())
+
+
+def _set_all_levels(s, small_threads, cluster_ctas):
+    from ma57_b200 import _lib as L
+    lib = L.load()
+    for lv in range(int(s.plan_stats()["levels"])):
+        assert lib.symla_gpu_set_level_schedule(s._ctx.h, lv, small_threads, cluster_ctas) == L.SYMLA_OK
+
+
+def _factor_arrays(s):
+    nf = s.numericFactor()
+    return [(list(f.rowIndices), f.nPivots, np.asarray(f.L).copy(), np.r_[f.Ddiag, f.Doff]) for f in nf.fronts]
+
+
+@pytest.mark.parametrize("case", ["batched", "kkt"])
+def test_warp_per_front_matches_block_small_kernel_bitwise(case):
+    """Fronts of at most 32 rows run one warp per front (eight per CTA) by
+    default; forcing the 128-thread block kernel on every level gives the
+    same factor bit for bit (same operations, reductions exact), including
+    2 x 2 pivots, interchanges and delayed columns of an indefinite KKT
+    system."""
+    if case == "batched":
+        mats = [M.config4_system(i)[0] for i in range(24)]
+        A = BatchedSolver(mats).A
+        ordering = OrderingType.Natural
+    else:
+        from helpers import random_rect, spd_block
+        A = M.kkt(spd_block(300, 4, 5), spd_block(120, 4, 22), random_rect(120, 300, 3, 36))
+        ordering = OrderingType.AMD
+    runs = []
+    for threads in (0, 128):
+        s = SymLDLT()
+        s.setOrdering(ordering)
+        s.analyzePattern(A)
+        s.factorize(A)
+        _set_all_levels(s, threads, 0)
+        s.factorize(A)
+        runs.append((s.inertia().as_tuple(), _factor_arrays(s)))
+    assert runs[0][0] == runs[1][0]
+    for (r0, p0, l0, d0), (r1, p1, l1, d1) in zip(runs[0][1], runs[1][1]):
+        assert r0 == r1 and p0 == p1
+        np.testing.assert_array_equal(l0, l1)
+        np.testing.assert_array_equal(d0, d1)
+
+
+def test_single_cta_panel_keeps_results():
+    """Panel cluster size 1 (the single-CTA panel kernel on every level)
+    gives the inertia of the cluster kernel and a comparable backward
+    error."""
+    A, b = M.config1(14)
+    s = SymLDLT()
+    s.analyzePattern(A)
+    s.factorize(A)
+    inertia, x0 = s.inertia().as_tuple(), s.solve(b)
+    _set_all_levels(s, 0, 1)
+    s.factorize(A)
+    assert s.inertia().as_tuple() == inertia
+    x = s.solve(b)
+    assert backward_error(A, x, b) <= 10 * max(backward_error(A, x0, b), 1e-16)
