@@ -723,17 +723,6 @@ template <typename F>
 void timed(symla_gpu_ctx* c, int kind, double flops, double bytes, F&& launch);
 void collect_pending(symla_gpu_ctx* c);
 
-// Cluster panels speculate again right after an interchange, a 2x2 or a 1x1
-// by the sigma test when SYMLA_GPU_SPEC_RESUME is 1 (read once); by default
-// only after a plain 1x1 by the first test.
-bool spec_resume_enabled() {
-  static const bool on = [] {
-    const char* e = std::getenv("SYMLA_GPU_SPEC_RESUME");
-    return e && e[0] == '1' && e[1] == '\0';
-  }();
-  return on;
-}
-
 KernelOpts make_kernel_opts(symla_gpu_ctx* c, const symla_factor_opts* o) {
   KernelOpts k;
   std::memset(&k, 0, sizeof k);  // padding too: graph reuse compares the bytes
@@ -752,7 +741,6 @@ KernelOpts make_kernel_opts(symla_gpu_ctx* c, const symla_factor_opts* o) {
   k.a_idx = c->d_a_idx;
   k.nnz = c->nnz;
   k.chk = c->d_check;
-  k.spec_resume = spec_resume_enabled() ? 1 : 0;
   return k;
 }
 

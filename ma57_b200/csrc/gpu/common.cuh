@@ -119,20 +119,6 @@ struct FactorGlobals {
   int spec_restarts;  // speculative runs started after a sequential decision inside a panel
 };
 
-// Chained launch (programmatic dependent launch) of the factorization's level
-// kernels: each is launched with programmatic stream serialization, so its
-// CTAs may be scheduled while the kernel before it in the stream still runs.
-// Such a kernel calls chain_enter() before anything else: griddepcontrol.wait
-// returns once the preceding kernel has completed and its memory operations
-// are visible (at once for an ordinary launch), and launch_dependents then
-// lets the following kernel's CTAs be scheduled. The following kernel can
-// only be scheduled once every CTA of this one has started, so the CTAs that
-// wait never hold resources this kernel still needs.
-__device__ __forceinline__ void chain_enter() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
 // Kernels of a level return at once when an earlier level stopped the
 // planned (static) pass: a delayed pivot (delay_level) or, in a graph
 // launch, a level whose planned panel iterations did not finish it
@@ -158,8 +144,6 @@ struct KernelOpts {
   const int* a_idx;             // A entry: index into values
   long long nnz;                // number of A values
   CheckWord* chk;               // status word of the bounds checks (checked build)
-  int spec_resume;              // cluster panels: speculate again right after any sequential
-                                // decision (1), or only after a plain 1x1 by the first test (0)
 };
 
 }  // namespace symla_gpu

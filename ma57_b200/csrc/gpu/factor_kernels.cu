@@ -18,7 +18,6 @@
 #include <cfloat>
 #include <climits>
 #include <cmath>
-#include <cstdlib>
 
 #include "common.cuh"
 #include "factor_kernels.h"
@@ -86,7 +85,6 @@ __global__ void __launch_bounds__(256, 4) assemble_kernel(const FrontDesc* __res
                                                        FrontState* st, const int* __restrict__ tasks,
                                                        const int* __restrict__ a_colptr, KernelOpts o,
                                                        const FactorGlobals* __restrict__ g, int level, int dynamic) {
-  chain_enter();
   if (level_aborted(g, level, dynamic)) return;
   __shared__ const int* s_inv[kAsmMaxChildren];
   __shared__ const double* s_cb[kAsmMaxChildren];
@@ -305,7 +303,6 @@ __global__ void __launch_bounds__(NT == 32 ? 32 * kWarpFronts : NT)
     factor_small_kernel(const FrontDesc* __restrict__ fronts, const ChildLink* __restrict__ links, FrontState* st,
                         const int* __restrict__ front_list, int count, const int* __restrict__ a_colptr, KernelOpts o,
                         FactorGlobals* g, int level, int dynamic) {
-  chain_enter();
   if (level_aborted(g, level, dynamic)) return;
   extern __shared__ double smem_all[];
   __shared__ double red_v[NT / 32];
@@ -650,7 +647,6 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(const FrontDesc* _
                                                               const int* __restrict__ front_list, int nb, KernelOpts o,
                                                               FactorGlobals* g, int level, int dynamic,
                                                               double* cols, int cols_stride) {
-  chain_enter();
   if (level_aborted(g, level, dynamic)) return;
   constexpr int NT = kPanelThreads;
   extern __shared__ double smem[];
@@ -1066,7 +1062,6 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
                                                                const int* __restrict__ front_list, int count,
                                                                FactorGlobals* g, int level, int dynamic,
                                                                const double* __restrict__ tc_guard) {
-  chain_enter();
   if (level_aborted(g, level, dynamic)) return;
   constexpr int AS = kAS<TM>;
   constexpr int WROWS = TM / 32;       // warps along the tile's rows
@@ -1268,20 +1263,11 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
 // ---------------------------------------------------------------------------
 // Host launchers
 
-bool chained_launch_enabled() {
-  static const bool on = [] {
-    const char* e = std::getenv("SYMLA_GPU_CHAINED_LAUNCH");
-    return e && e[0] == '1' && e[1] == '\0';
-  }();
-  return on;
-}
-
 void launch_assemble(const FrontDesc* fronts, const ChildLink* links, FrontState* st, const int* tasks,
                      int ntasks, const int* a_colptr, const KernelOpts& o, const FactorGlobals* g, int level,
                      int dynamic, cudaStream_t stream) {
   if (ntasks <= 0) return;
-  (void)launch_chained(assemble_kernel, dim3(ntasks), dim3(256), 0, stream, 0, fronts, links, st, tasks, a_colptr, o,
-                       g, level, dynamic);
+  assemble_kernel<<<ntasks, 256, 0, stream>>>(fronts, links, st, tasks, a_colptr, o, g, level, dynamic);
 }
 
 size_t small_front_smem(int m) {
@@ -1296,15 +1282,14 @@ void launch_factor_small(const FrontDesc* fronts, const ChildLink* links, FrontS
   if (max_m <= kWarpFrontMax && (threads == 32 || threads == 0)) {
     // one warp per front, kWarpFronts fronts per CTA
     const int grid = (count + kWarpFronts - 1) / kWarpFronts;
-    (void)launch_chained(factor_small_kernel<32>, dim3(grid), dim3(32 * kWarpFronts),
-                         kWarpFronts * kWarpFrontDoubles * sizeof(double), stream, 0, fronts, links, st, list, count,
-                         a_colptr, o, g, level, dynamic);
+    factor_small_kernel<32><<<grid, 32 * kWarpFronts, kWarpFronts * kWarpFrontDoubles * sizeof(double), stream>>>(
+        fronts, links, st, list, count, a_colptr, o, g, level, dynamic);
   } else if (threads == 128 || (threads != 256 && max_m <= 48)) {
-    (void)launch_chained(factor_small_kernel<128>, dim3(count), dim3(128), sm, stream, 0, fronts, links, st, list,
-                         count, a_colptr, o, g, level, dynamic);
+    factor_small_kernel<128><<<count, 128, sm, stream>>>(fronts, links, st, list, count, a_colptr, o, g, level,
+                                                          dynamic);
   } else {
-    (void)launch_chained(factor_small_kernel<256>, dim3(count), dim3(256), sm, stream, 0, fronts, links, st, list,
-                         count, a_colptr, o, g, level, dynamic);
+    factor_small_kernel<256><<<count, 256, sm, stream>>>(fronts, links, st, list, count, a_colptr, o, g, level,
+                                                          dynamic);
   }
 }
 
@@ -1319,8 +1304,8 @@ cudaError_t launch_panel(const FrontDesc* fronts, FrontState* st, const int* lis
   if (count <= 0) return cudaSuccess;
   if (!panel_fits_shared(max_m) && !cols) return cudaErrorInvalidValue;
   const size_t sm = cols ? 0 : 2 * static_cast<size_t>(max_m) * sizeof(double);
-  return launch_chained(panel_kernel, dim3(count), dim3(kPanelThreads), sm, stream, 0, fronts, st, list, nb, o, g,
-                        level, dynamic, cols, max_m);
+  panel_kernel<<<count, kPanelThreads, sm, stream>>>(fronts, st, list, nb, o, g, level, dynamic, cols, max_m);
+  return cudaGetLastError();
 }
 
 
@@ -1342,7 +1327,6 @@ void launch_count_unfinished(const FrontState* st, const int* list, int count, i
 // iterations marks itself, so the later levels of the graph return at once.
 __global__ void mark_unfinished_kernel(const FrontState* __restrict__ st, const int* __restrict__ list, int count,
                                        FactorGlobals* g, int level) {
-  chain_enter();
   if (level_skipped(g, level, 0)) return;
   int c = 0;
   for (int t = threadIdx.x; t < count; t += blockDim.x)
@@ -1354,7 +1338,7 @@ __global__ void mark_unfinished_kernel(const FrontState* __restrict__ st, const 
 void launch_mark_unfinished(const FrontState* st, const int* list, int count, FactorGlobals* g, int level,
                             cudaStream_t stream) {
   if (count <= 0) return;
-  (void)launch_chained(mark_unfinished_kernel, dim3(1), dim3(256), 0, stream, 0, st, list, count, g, level);
+  mark_unfinished_kernel<<<1, 256, 0, stream>>>(st, list, count, g, level);
 }
 
 namespace {
@@ -1363,9 +1347,8 @@ void launch_update_t(const FrontDesc* fronts, FrontState* st, const int* list, i
                      FactorGlobals* g, int level, int dynamic, cudaStream_t stream, const double* tc_guard) {
   for (int b = 0; b < count; b += kMaxUpdateFronts) {
     const int cnt = count - b < kMaxUpdateFronts ? count - b : kMaxUpdateFronts;
-    (void)launch_chained(update_mma_kernel<MODE, TM>, dim3(grid_x), dim3(kMThreads), mma_smem<TM>(), stream, 0,
-                         fronts, st, list + b, cnt, g, level, dynamic,
-                         (MODE == 1 && tc_guard) ? tc_guard + 2 * b : nullptr);
+    update_mma_kernel<MODE, TM><<<grid_x, kMThreads, mma_smem<TM>(), stream>>>(
+        fronts, st, list + b, cnt, g, level, dynamic, (MODE == 1 && tc_guard) ? tc_guard + 2 * b : nullptr);
   }
 }
 }  // namespace

@@ -19,38 +19,6 @@ constexpr int kAsmRows = 1024;
 cudaError_t configure_factor_kernels();
 size_t small_front_smem(int m);
 
-// Whether the factorization's level kernels are chained (programmatic
-// dependent launch, see chain_enter): when the environment variable
-// SYMLA_GPU_CHAINED_LAUNCH is 1 as the library first launches one.
-bool chained_launch_enabled();
-
-// Launch one of those kernels with the programmatic-serialization attribute
-// (when enabled), plus a cluster dimension when cluster_x > 0.
-template <typename... P, typename... A>
-cudaError_t launch_chained(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
-                           int cluster_x, A&&... args) {
-  cudaLaunchAttribute attr[2];
-  unsigned n = 0;
-  attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[n].val.programmaticStreamSerializationAllowed = chained_launch_enabled() ? 1 : 0;
-  ++n;
-  if (cluster_x > 0) {
-    attr[n].id = cudaLaunchAttributeClusterDimension;
-    attr[n].val.clusterDim.x = static_cast<unsigned>(cluster_x);
-    attr[n].val.clusterDim.y = 1;
-    attr[n].val.clusterDim.z = 1;
-    ++n;
-  }
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = stream;
-  cfg.attrs = attr;
-  cfg.numAttrs = n;
-  return cudaLaunchKernelEx(&cfg, kernel, static_cast<A&&>(args)...);
-}
-
 // tasks: (front, first column, first row, end row or -1 for the front's m)
 void launch_assemble(const FrontDesc* fronts, const ChildLink* links, FrontState* st, const int* tasks,
                      int ntasks, const int* a_colptr, const KernelOpts& o, const FactorGlobals* g, int level,

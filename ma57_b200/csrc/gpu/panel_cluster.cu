@@ -135,7 +135,6 @@ template <int CS>
 __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __restrict__ fronts, FrontState* st,
                                                             const int* __restrict__ front_list, int nb, int R,
                                                             KernelOpts o, FactorGlobals* g, int level, int dynamic) {
-  chain_enter();
   if (level_skipped(g, level, dynamic)) return;
   cg::cluster_group cluster = cg::this_cluster();
   const int q = static_cast<int>(cluster.block_rank());
@@ -837,7 +836,7 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
       __syncthreads();
       k += 1;
       // a plain 1x1 at k by the first test: the next pivots likely are too
-      try_spec = dec_kind == 0 || o.spec_resume;
+      try_spec = dec_kind == 0;
       continue;
     }
     pf_col = -1;  // an interchange invalidates the prefetched column
@@ -918,10 +917,6 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
       __threadfence();
       cluster.sync();
     }
-    // (a restart needs no more state than the next sequential pivot: L of
-    // the panel's pivots in Lr, D in sh, and w of row k for a restart that
-    // fails at its first pivot)
-    if (o.spec_resume) try_spec = true;
   }
 
   // ---- finish: running max by a global atomic (monotone), state by rank 0
@@ -1033,21 +1028,27 @@ cudaError_t launch_cluster_panel(const FrontDesc* fronts, FrontState* st, const 
   const int cs = cluster_size_fits(max_m, cs_choice, nb) ? cs_choice : cluster_size_for(max_m, count, nb);
   if (cs == 0) return cudaErrorInvalidValue;
   const int R = cluster_rows(max_m, cs);
-  const dim3 grid(cs * count), block(kCT);
-  const size_t sm = cluster_panel_smem(max_m, nb, cs);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cs * count);
+  cfg.blockDim = dim3(kCT);
+  cfg.dynamicSmemBytes = cluster_panel_smem(max_m, nb, cs);
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
   switch (cs) {
     case 16:
-      return launch_chained(cluster_panel_kernel<16>, grid, block, sm, stream, cs, fronts, st, list, nb, R, o, g,
-                            level, dynamic);
+      return cudaLaunchKernelEx(&cfg, cluster_panel_kernel<16>, fronts, st, list, nb, R, o, g, level, dynamic);
     case 8:
-      return launch_chained(cluster_panel_kernel<8>, grid, block, sm, stream, cs, fronts, st, list, nb, R, o, g,
-                            level, dynamic);
+      return cudaLaunchKernelEx(&cfg, cluster_panel_kernel<8>, fronts, st, list, nb, R, o, g, level, dynamic);
     case 4:
-      return launch_chained(cluster_panel_kernel<4>, grid, block, sm, stream, cs, fronts, st, list, nb, R, o, g,
-                            level, dynamic);
+      return cudaLaunchKernelEx(&cfg, cluster_panel_kernel<4>, fronts, st, list, nb, R, o, g, level, dynamic);
     default:
-      return launch_chained(cluster_panel_kernel<2>, grid, block, sm, stream, cs, fronts, st, list, nb, R, o, g,
-                            level, dynamic);
+      return cudaLaunchKernelEx(&cfg, cluster_panel_kernel<2>, fronts, st, list, nb, R, o, g, level, dynamic);
   }
 }
 
