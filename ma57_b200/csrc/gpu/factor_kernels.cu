@@ -1179,6 +1179,24 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
             acc[rt][ct][2 * v + h] = (gj < c1 && gi < m && gi >= gj) ? colp[gi] : 0.0;
           }
       }
+    // D of this thread's pivot of a chunk (pivot q = threadIdx.x / 16 of the
+    // chunk; W row q, columns (threadIdx.x % 16) + 16 j): loaded one chunk
+    // ahead into registers, so no global load waits between a chunk's
+    // staging and its barrier
+    const int wq = threadIdx.x >> 4, wr0 = threadIdx.x & 15;
+    int dk = 0;
+    double dd = 0.0, dn = 0.0, dp = 0.0;
+    auto load_d = [&](int kc, int kn) {
+      if (wq < kn) {
+        const FrontDesc& fd = fronts[s];
+        const int pq = kc + wq;
+        dk = fd.pk[pq];
+        dd = fd.Dd[pq];
+        dn = fd.Do[pq];
+        dp = pq > 0 ? fd.Do[pq - 1] : 0.0;
+      }
+    };
+    load_d(q0, min(kKM, q1 - q0));
     for (int c = 0; c < nchunks; ++c, ++u) {
       const int kc = q0 + c * kKM, kn = min(kKM, q1 - kc);
       const unsigned b = u % kMStages;
@@ -1197,23 +1215,22 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
       const int kn8 = (kn + 7) & ~7;
       for (int t = threadIdx.x; t < (kn8 - kn) * AS; t += kMThreads) As[kn * AS + t] = 0.0;
       // W(j, q) = -(L D)(j, q)
-      {
-        const FrontDesc& fd = fronts[s];
-        for (int t = threadIdx.x; t < kn8 * kTJ; t += kMThreads) {
-          const int q = t / kTJ, r = t % kTJ;
+      if (wq < kn8) {
+#pragma unroll
+        for (int j = 0; j < kTJ / 16; ++j) {
+          const int r = wr0 + 16 * j;
           double w = 0.0;
-          if (q < kn) {
-            const int pq = kc + q;
-            const double* col = Bs + (q + 1) * kBS + r;
-            const int8_t kind = fd.pk[pq];
-            w = fd.Dd[pq] * col[0];
-            if (kind == 1) w += fd.Do[pq] * col[kBS];
-            if (kind == 2) w += fd.Do[pq - 1] * col[-kBS];
+          if (wq < kn) {
+            const double* col = Bs + (wq + 1) * kBS + r;
+            w = dd * col[0];
+            if (dk == 1) w += dn * col[kBS];
+            if (dk == 2) w += dp * col[-kBS];
           }
-          Ws[q * kBS + r] = -w;
+          Ws[wq * kBS + r] = -w;
         }
       }
       __syncthreads();  // W and the zeroed columns ready; every thread is past chunk c - 1
+      if (c + 1 < nchunks) load_d(kc + kKM, min(kKM, q1 - kc - kKM));
       if (warp == 0 && c + 2 < nchunks) {
         const int kc2 = kc + 2 * kKM;
         const unsigned b2 = (u + 2) % kMStages;
