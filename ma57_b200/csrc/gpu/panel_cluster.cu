@@ -414,6 +414,9 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
       // 16-byte pairs (the extra slot before r0 and after rend is spare)
       const int s0 = r0 & ~1, e0 = (rend + 1) & ~1;
       const bool have_rows = r0 < rend;
+      // static pivoting: expected sign of block row `lane`, loaded now so the
+      // diagonal-block chain below reads it from a register
+      const int lane_sign = (o.mode == 1 && o.sign_final && warp == 0 && lane < np) ? o.sign_final[f.fidx[k0 + lane]] : 0;
       if (warp == 0) {
         for (int j = 0; j < np; ++j)
           for (int i = j + lane; i < np; i += 32) cp_async8(&sh.db[i][j], F + static_cast<int64_t>(k0 + j) * ld + k0 + i);
@@ -509,7 +512,7 @@ __global__ void __launch_bounds__(kCT) cluster_panel_kernel(const FrontDesc* __r
           double d = akk, applied = 0.0;
           if (o.mode == 1) {
             // static pivoting (dense_kernel.hpp:982-1034), as in the sequential path
-            const int sign = o.sign_final ? o.sign_final[f.fidx[k0 + c]] : 0;
+            const int sign = __shfl_sync(0xffffffffu, lane_sign, c);
             bool need;
             if (sign > 0)
               need = akk < floorv;
