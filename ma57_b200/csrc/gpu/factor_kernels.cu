@@ -362,9 +362,13 @@ __global__ void __launch_bounds__(NT == 32 ? 32 * kWarpFronts : NT)
     // dense_kernel.hpp:919-1059, unblocked (panel_size 1 for small fronts)
     delta = o.front_delta ? o.front_delta[s] : (o.static_delta > 0.0 ? o.static_delta : 1.4901161193847656e-08 * orig_max);
     const double floorv = fmax(o.static_abs_floor, o.static_rel_floor * orig_max);
+    // expected sign of the next pivot, loaded one pivot ahead (static
+    // pivoting never reorders fi)
+    int sign_next = (o.sign_final && effEnd > 0) ? o.sign_final[fi[0]] : 0;
     for (k = 0; k < effEnd; ++k) {
       const double akk = F.at(k, k);
-      const int sign = o.sign_final ? o.sign_final[fi[k]] : 0;
+      const int sign = sign_next;
+      if (o.sign_final && k + 1 < effEnd) sign_next = o.sign_final[fi[k + 1]];
       bool need;
       if (sign > 0)
         need = akk < floorv;

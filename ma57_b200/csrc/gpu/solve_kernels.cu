@@ -179,6 +179,11 @@ __device__ bool forward_block(const FrontDesc* __restrict__ fronts, const ChildL
   const int jend = min(rb, nbp);
   const bool hasDiag = r0 < np;
   const int ntiles = jend + (hasDiag ? 1 : 0);
+  // pivot kinds the steps below need, loaded before any wait: a 2x2 pivot
+  // ending at row r0 - 1 (its d21 slot sits in the last earlier tile) and
+  // one starting at this thread's row of the diagonal block
+  const bool pair_before = r0 > 0 && r0 - 1 < np && f.pk[r0 - 1] == 1;
+  const bool own_pair = hasDiag && threadIdx.x + 1 < min(r1, np) - r0 && f.pk[r0 + threadIdx.x] == 1;
   // tile tt: pivot block tt (tt < jend) or the diagonal block
   auto stage = [&](int tt) {
     double* T = Lb0 + (tt & 1) * kRB * kTileStride;
@@ -234,7 +239,7 @@ __device__ bool forward_block(const FrontDesc* __restrict__ fronts, const ChildL
       __syncthreads();
       // a 2x2 pivot straddling the block boundary: its d21 slot in L is not
       // an L entry
-      if (threadIdx.x == 0 && j == rb - 1 && r0 - 1 >= j0 && f.pk[r0 - 1] == 1) T[r0 - 1 - j0] = 0.0;
+      if (threadIdx.x == 0 && j == rb - 1 && r0 - 1 >= j0 && pair_before) T[r0 - 1 - j0] = 0.0;
       __syncthreads();
       if (row < nr) {
         double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
@@ -261,8 +266,7 @@ __device__ bool forward_block(const FrontDesc* __restrict__ fronts, const ChildL
       scp_wait<0>();
       __syncthreads();
       const int npv = min(r1, np) - r0;
-      if (threadIdx.x < npv - 1 && f.pk[r0 + threadIdx.x] == 1)
-        T[(threadIdx.x + 1) * kTileStride + threadIdx.x] = 0.0;  // d21 slot of a 2x2 pivot
+      if (own_pair) T[(threadIdx.x + 1) * kTileStride + threadIdx.x] = 0.0;  // d21 slot of a 2x2 pivot
       __syncthreads();
       // a warp takes right-hand sides c and c + 8 together: the two
       // substitution chains interleave (each step is a shuffle and an FMA)
@@ -358,6 +362,13 @@ __device__ bool backward_block(const FrontDesc* __restrict__ fronts, const Front
   const int nanc = a1 - a0;
   const int nlater = helper ? 0 : nbp - 1 - cb;
   const int ntiles = nanc + nlater + (helper ? 0 : 1);
+  // loaded before any wait: the 2x2 pivot kinds the steps below need and
+  // the rows the block's solution is written to
+  static_assert(kST % kRB == 0, "a thread keeps one tile row in the gathers");
+  __shared__ int s_row[kRB];
+  const bool pair_at_end = nq > 0 && f.pk[q1 - 1] == 1;
+  const bool own_pair = threadIdx.x + 1 < nq && f.pk[q0 + threadIdx.x] == 1;
+  if (!helper && threadIdx.x < nq) s_row[threadIdx.x] = f.fidx[q0 + threadIdx.x];
   auto tile_rows = [&](int tt, int& i0, int& i1) {
     if (tt < nanc) {
       i0 = np + (a0 + tt) * kRB;
@@ -412,6 +423,10 @@ __device__ bool backward_block(const FrontDesc* __restrict__ fronts, const Front
       // 2. minus L(rows of the tile, block)^T x(rows of the tile): the
       //    ancestor rows are final from earlier levels; later pivot blocks of
       //    this front are waited for
+      const int ni = i1 - i0;
+      // this thread's tile row (the same for every t below), before the wait
+      const int my_ii = threadIdx.x % kRB;
+      const int my_gi = my_ii < ni ? f.fidx[i0 + my_ii] : 0;
       if (tt >= nanc) {
         const int j = nbp - 1 - (tt - nanc);
         if (!wait_flag(flags, flag_base[s] + j, epoch, err, wait_ns)) {
@@ -419,12 +434,11 @@ __device__ bool backward_block(const FrontDesc* __restrict__ fronts, const Front
           return false;
         }
       }
-      const int ni = i1 - i0;
       for (int t = threadIdx.x; t < kRB * nc; t += kST) {
         const int ii = t % kRB, c = t / kRB;
         double xv = 0.0;
         if (ii < ni) {
-          const int gi = f.fidx[i0 + ii];
+          const int gi = my_gi;
           if (solve_index_ok(in_range(gi, 0, n), err)) xv = X[gi + static_cast<int64_t>(c0 + c) * n];
         }
         xb[ii * kAccStride + c] = xv;
@@ -435,7 +449,7 @@ __device__ bool backward_block(const FrontDesc* __restrict__ fronts, const Front
         scp_wait<0>();
       __syncthreads();
       // a 2x2 pivot straddling the block boundary: d21 is not an L entry
-      if (threadIdx.x == 0 && i0 == q1 && nq > 0 && f.pk[q1 - 1] == 1) T[nq - 1] = 0.0;
+      if (threadIdx.x == 0 && i0 == q1 && pair_at_end) T[nq - 1] = 0.0;
       __syncthreads();
       if (col < nq) {
         double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
@@ -473,8 +487,7 @@ __device__ bool backward_block(const FrontDesc* __restrict__ fronts, const Front
       // 3. transposed unit-lower solve on the diagonal block
       scp_wait<0>();
       __syncthreads();
-      if (threadIdx.x < nq - 1 && f.pk[q0 + threadIdx.x] == 1)
-        T[(threadIdx.x + 1) * kTileStride + threadIdx.x] = 0.0;  // d21 slot of a 2x2 pivot
+      if (own_pair) T[(threadIdx.x + 1) * kTileStride + threadIdx.x] = 0.0;  // d21 slot of a 2x2 pivot
       __syncthreads();
       // right-hand sides c and c + NW together (interleaved chains)
       for (int c = warp; c < nc; c += 2 * NW) {
@@ -518,7 +531,7 @@ __device__ bool backward_block(const FrontDesc* __restrict__ fronts, const Front
   } else {
     for (int t = threadIdx.x; t < nq * nc; t += kST) {
       const int qq = t % nq, c = t / nq;
-      const int gi = f.fidx[q0 + qq];
+      const int gi = s_row[qq];
       if (solve_index_ok(in_range(gi, 0, n), err)) X[gi + static_cast<int64_t>(c0 + c) * n] = acc[qq * kAccStride + c];
     }
     publish(flags, flag_base[s] + cb, epoch);
