@@ -1118,6 +1118,51 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
   // column tile's first tile (tj_first, counted within the entry) only move
   // forward: each is advanced from where the previous tile left it
   int fi = 0, tj = 0, tj_first = 0;
+  // rows of a tile's copies, from the even row at or before its first row,
+  // rounded up to whole 16-byte pairs (the extra row of an odd m is the
+  // padding row of the front's even leading dimension); warp 0
+  auto set_copy_rows = [&](int ti0, int tj0, int tm) {
+    if (lane == 0) {
+      copy_rows.ra = ti0 & ~1;
+      copy_rows.na = ((min(ti0 + TM, tm) + 1) & ~1) - copy_rows.ra;
+      copy_rows.rb = tj0 & ~1;
+      copy_rows.nb = ((min(tj0 + kTJ, tm) + 1) & ~1) - copy_rows.rb;
+    }
+    __syncwarp();
+  };
+  // the CTA's next tile nt: its first (up to two) chunks into stages
+  // (u + 1) % 3 and (u + 2) % 3, issued by warp 0 after the barrier of this
+  // tile's last chunk u (every warp is past the chunks that used those
+  // stages). The walk runs on copies: the tile loop repeats it at nt.
+  auto issue_next = [&](int nt) {
+    int nfi = fi, ntj = tj, ntjf = tj_first;
+    while (nt >= tile_end[nfi]) {
+      ++nfi;
+      ntj = 0;
+      ntjf = 0;
+    }
+    const int ns = front_list[nfi % count];
+    const int nm = fronts[ns].m;
+    int nc0, nc1, nq0, nq1;
+    update_range(st[ns], nm, entry_far(nfi), nc0, nc1, nq0, nq1);
+    const int nrel = nt - (nfi > 0 ? tile_end[nfi - 1] : 0);
+    for (;;) {
+      const int nr = (nm - (nc0 + ntj * kTJ) + TM - 1) / TM;
+      if (nrel < ntjf + nr) break;
+      ntjf += nr;
+      ++ntj;
+    }
+    const int nj0 = nc0 + ntj * kTJ, ni0 = nj0 + (nrel - ntjf) * TM;
+    set_copy_rows(ni0, nj0, nm);
+    const int nn = (nq1 - nq0 + kKM - 1) / kKM;
+    for (int cc = 0; cc < 2 && cc < nn; ++cc) {
+      const int kc = nq0 + cc * kKM;
+      const unsigned b = (u + 1 + cc) % kMStages;
+      u_issue<TM>(fronts[ns].F, fronts[ns].ld, nq0, nq1, kc, min(kKM, nq1 - kc), copy_rows, As_of(b), Bs_of(b),
+                  &full[b], lane);
+    }
+  };
+  bool ahead = false;  // warp 0 issued this tile's first chunks during the previous tile
   for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
     while (tile >= tile_end[fi]) {
       ++fi;
@@ -1147,24 +1192,16 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
     }
     const int j0 = c0 + tj * kTJ, i0 = j0 + (rel - tj_first) * TM;
     const int sa = i0 & 1, sb = j0 & 1;  // parity offsets of the staged rows
-    __syncthreads();  // previous tile done with every stage
-    if (warp == 0) {
-      // rows from the even row at or before the tile's first row, rounded up
-      // to whole 16-byte pairs (the extra row of an odd m is the padding row
-      // of the front's even leading dimension)
-      if (lane == 0) {
-        copy_rows.ra = i0 & ~1;
-        copy_rows.na = ((min(i0 + TM, m) + 1) & ~1) - copy_rows.ra;
-        copy_rows.rb = j0 & ~1;
-        copy_rows.nb = ((min(j0 + kTJ, m) + 1) & ~1) - copy_rows.rb;
-      }
-      __syncwarp();
+    __syncthreads();  // previous tile done with every stage and with W
+    if (warp == 0 && !ahead) {
+      set_copy_rows(i0, j0, m);
       for (int c = 0; c < 2 && c < nchunks; ++c) {
         const int kc = q0 + c * kKM;
         const unsigned b = (u + c) % kMStages;
         u_issue<TM>(Fp, ld, q0, q1, kc, min(kKM, q1 - kc), copy_rows, As_of(b), Bs_of(b), &full[b], lane);
       }
     }
+    ahead = false;
     // C tile into the accumulators (lane holds rows gi0 + 16 rt + 8 v,
     // columns gj0 + 8 ct + h as acc[rt][ct][2 v + h])
     const int gi0 = i0 + wr * 32 + lg, gj0 = j0 + wc * WN + 2 * lt;
@@ -1239,6 +1276,9 @@ __global__ void __launch_bounds__(kMThreads, 2) update_mma_kernel(const FrontDes
         const int kc2 = kc + 2 * kKM;
         const unsigned b2 = (u + 2) % kMStages;
         u_issue<TM>(Fp, ld, q0, q1, kc2, min(kKM, q1 - kc2), copy_rows, As_of(b2), Bs_of(b2), &full[b2], lane);
+      } else if (warp == 0 && c == nchunks - 1 && tile + static_cast<int>(gridDim.x) < total) {
+        issue_next(tile + static_cast<int>(gridDim.x));
+        ahead = true;
       }
       const double* Aq = As + sa;
       for (int k0 = 0; k0 < kn8; k0 += 8) {
