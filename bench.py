@@ -46,6 +46,31 @@ PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 UPDATE_DRAM_BYTES_PER_FLOP = 1.2578e9 / 25.8151e9
 
 
+def replica_group(world: int, backend: str = "nccl"):
+    """torch.distributed for N > 1 replicas launched by torchrun (RANK,
+    WORLD_SIZE, MASTER_* from the environment), or None for one process. The
+    replicas exchange nothing on the data path: only barriers around the
+    timed region and the max-over-ranks reductions below. The short timeout
+    ends a wait for a rank that died with an error instead of a hang."""
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    """The slowest replica's figure; every rank calls this in the same order."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def load_peaks():
     try:
         with open(PEAKS_PATH) as f:
@@ -634,11 +659,7 @@ def run_ours(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dist = replica_group(world)
 
     lib = L.load()
     A, B = build_problem(args.k, args.nrhs)
@@ -698,6 +719,8 @@ def run_ours(args):
     lib.symla_gpu_reset_kernel_stats(h)
     clk = clocks_start(local)
     ms = timed_steps(args.steps)
+    if dist:
+        dist.barrier()
     clocks = clocks_stop(clk)
     launches = int(lib.symla_gpu_launch_count(h)) // max(1, args.steps)
     inertia = [info.n_pos, info.n_neg, info.n_zero]
@@ -710,7 +733,7 @@ def run_ours(args):
         opts.precision = other
         for _ in range(args.warmup):
             step()
-        ms_other = timed_steps(args.steps)
+        ms_other = max_over_ranks(timed_steps(args.steps), dist, dev)
         name = "mixed" if other == L.PREC_MIXED else "fp64"
         comparison = {f"{name}_s": ms_other / 1e3, f"{args.precision}_s": ms / 1e3,
                       "mixed_over_fp64": (ms_other / ms) if other == L.PREC_MIXED else (ms / ms_other),
@@ -731,10 +754,7 @@ def run_ours(args):
         step()
     torch.cuda.synchronize()
     lib.symla_gpu_set_profiling(h, 0)
-    if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, dev)
     kstats = {}
     buf = (C.c_double * 4)()
     for kind, name in enumerate(L.KERNEL_KINDS):
@@ -764,11 +784,7 @@ def run_ours(args):
         check(lib.symla_gpu_solve_refine(h, L.ptr_d(vals_h), L.ptr_d(Bh), n, nrhs, L.ptr_d(Xh), n, 0, 10, 1e-12,
                                          C.byref(rinfo)))
         e2e_times.append(time.perf_counter() - t0)
-    e2e = statistics.median(e2e_times)
-    if dist:
-        t = torch.tensor([e2e], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e = float(t.item())
+    e2e = max_over_ranks(statistics.median(e2e_times), dist, dev)
 
     # independent check of the backward error of the host-path result
     import scipy.sparse as sp
